@@ -1,0 +1,395 @@
+"""Benchmark: LeCo-fix bulk decode GB/s and batched random access on B200.
+
+Workload (one GPU): 200M sorted uint64 keys from a piecewise-linear trend
+(segment lengths geometric, mean 50k; slopes log-uniform in [1, 2^20]) plus
+round(N(0, 2^12)) noise, LeCo-fix linear codec with 4096-value blocks
+(48,829 blocks).  A step is one bulk decode of the whole column (inputs and
+outputs are larger than L2) followed by one batch of 2^24 uniform random
+lookups.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  --impl reference times the reference's own CPU
+codec (the compiled reference headers, oracle/_ref) on the host cores on the
+same workload.  Under torchrun each rank decodes its own 200M-key column
+(weak scaling, no data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LeCo-fix decode GB/s and batched random-access Mlookups/s, p50/p99, 1 B200"
+N_DEFAULT = 200_000_000
+BS = 4096
+RA_BATCH = 1 << 24
+DECODE_KERNEL = "decode_kernel"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="leco", choices=["leco", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the decode kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "decode_kernel_leco_u64_200M.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return int(float(line.split(":", 1)[1].strip().split()[0]))
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_decode(x: np.ndarray, bs: int, threads: int, budget_s: float = 10.0):
+    """Times the compiled reference headers (oracle/_ref): Leco_int<uint64_t>
+    encodeArray8_int per block once, then decodeArray8 over all blocks with
+    `threads` host threads, repeated until `budget_s` elapses.  Returns
+    (GB/s of decoded bytes, kind, sample description, ratio)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if os.path.exists(oracle.REF_SO):
+        R, kind = oracle.Reference(), "reference"
+    else:
+        R, kind = None, "port"
+    s = x.dtype.itemsize
+    if R is not None:
+        pay, off = R.encode_column(0, x, bs)
+    else:
+        O = oracle.Oracle()
+        pay, off = O.encode_column(0, x, bs)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        if R is not None:
+            y = R.decode_column(0, pay, off, len(x), s, bs, threads=threads)
+        else:
+            y = oracle.Oracle().decode_column(0, pay, off, len(x), s, bs)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or reps >= 50:
+            break
+    assert np.array_equal(y, x), "reference decode mismatch"
+    gbs = reps * len(x) * s / el / 1e9
+    sample = f"{len(x)/1e6:.0f}M keys of the same generator, {reps} full decodes in {el:.1f}s"
+    return gbs, kind, sample, len(pay) / (len(x) * s), pay, off
+
+
+def cpu_reference_random(pay, off, x, bs, threads, m=4_000_000):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    R = oracle.Reference()
+    rng = np.random.default_rng(7)
+    idx = rng.integers(0, len(x), m).astype(np.uint64)
+    t0 = time.perf_counter()
+    y = R.random_column(0, pay, off, 8, bs, idx, threads=threads)
+    el = time.perf_counter() - t0
+    assert np.array_equal(y, x[idx])
+    return m / el / 1e6
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's CPU codec on the host cores."""
+    if rank != 0:
+        return
+    from leco_b200 import workloads
+
+    threads = os.cpu_count() or 1
+    n = min(args.n, 50_000_000)  # bounded sample of the same workload
+    x = workloads.piecewise_linear_u64(n, seed=2).numpy().view(np.uint64)
+    times = []
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not os.path.exists(oracle.REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libleco_ref.so was not built"}))
+        return
+    R = oracle.Reference()
+    pay, off = R.encode_column(0, x, BS)
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        y = R.decode_column(0, pay, off, n, 8, BS, threads=threads)
+        el = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(el)
+    assert np.array_equal(y, x)
+    ms = float(np.mean(times)) * 1e3
+    gbs = n * 8 / (ms / 1e3) / 1e9
+    ra = cpu_reference_random(pay, off, x, BS, threads)
+    sample = f"{n/1e6:.0f}M keys of the 200M-key generator (bounded sample), {threads} threads"
+    out = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+           "config": {"workload": "leco_fix u64 piecewise-linear sorted keys, 4096-value blocks", "keys": n,
+                      "block_size": BS, "threads": threads},
+           "ra_mlookups_s": round(ra, 2),
+           "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    n = args.n
+    x = workloads.piecewise_linear_u64(n, seed=2 + rank, device=dev)
+    stream = torch.cuda.current_stream()
+    t_enc = {}
+    cols = {}
+    for mode, name in ((lc.FIT_REFERENCE, "reference"), (lc.FIT_EXACT, "exact")):
+        col = lc.encode(x, lc.LINEAR, BS, mode)  # warm-up + correctness
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record(stream)
+        for _ in range(reps):
+            col = lc.encode(x, lc.LINEAR, BS, mode, payload=col.payload)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_enc[name] = e0.elapsed_time(e1) / reps
+        cols[name] = col
+    col = cols["reference"]
+    lc.check()
+    y = col.decode()
+    assert torch.equal(y, x), "decode mismatch"
+    gidx = torch.randint(0, n, (RA_BATCH,), device=dev, dtype=torch.int64)
+    assert torch.equal(col.gather(gidx), x[gidx]), "random access mismatch"
+    assert col.sum() == int(x.sum().item()) & 0xFFFFFFFFFFFFFFFF, "sum mismatch"
+    del cols
+    torch.cuda.synchronize()
+
+    out = torch.empty_like(x)
+    ra_out = torch.empty(RA_BATCH, dtype=torch.int64, device=dev)
+    idx_sets = [torch.randint(0, n, (RA_BATCH,), device=dev, dtype=torch.int64) for _ in range(4)]
+    for i in range(args.warmup):
+        col.decode(out=out)
+        col.gather(idx_sets[i % 4], out=ra_out)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(args.steps):
+            a, b, c = ev[i]
+            a.record(stream)
+            col.decode(out=out)
+            b.record(stream)
+            col.gather(idx_sets[i % 4], out=ra_out)
+            c.record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t_start.elapsed_time(t_end)
+    dec_ms = [a.elapsed_time(b) for a, b, _ in ev]
+    ra_ms = [b.elapsed_time(c) for _, b, c in ev]
+    lc.check()
+    assert torch.equal(out, x)
+
+    if pg:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms, float(np.mean(dec_ms)), float(np.mean(ra_ms))], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, dec_mean, ra_mean = t.tolist()
+    else:
+        dec_mean, ra_mean = float(np.mean(dec_ms)), float(np.mean(ra_ms))
+
+    comp = col.nbytes
+    dec_bytes = n * 8
+    value = world * dec_bytes / (dec_mean / 1e3) / 1e9
+    ra_rate = world * RA_BATCH / (ra_mean / 1e3) / 1e6
+    peak, peak_kind = peaks()
+    alg_bytes = comp + (col.nblocks + 1) * 8 + dec_bytes  # payload + offsets read, values written
+    achieved = alg_bytes / (dec_mean / 1e3) / 1e9
+
+    # end-to-end through the public host-buffer API: pinned compressed bytes in,
+    # pinned decoded values out, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        pay_h, off_h = col.to_host()
+        pay_pin = torch.empty(len(pay_h) + 64, dtype=torch.uint8).pin_memory()
+        pay_pin[: len(pay_h)].copy_(torch.from_numpy(pay_h))
+        off_pin = torch.from_numpy(off_h.view(np.int64)).pin_memory()
+        out_pin = torch.empty(n, dtype=torch.int64).pin_memory()
+        L = lc.lib()
+        import ctypes
+
+        P = ctypes.c_void_p
+        args_e2e = (0, 8, P(pay_pin.data_ptr()), P(off_pin.data_ptr()), n, BS, P(out_pin.data_ptr()))
+        for _ in range(2):
+            lc._check(L.leco_decode_host(*args_e2e))
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            lc._check(L.leco_decode_host(*args_e2e))
+        e2e_s = (time.perf_counter() - t0) / reps
+        assert torch.equal(out_pin, x.cpu())
+        e2e = {"value": round(world * dec_bytes / e2e_s / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(comp + off_h.nbytes), "d2h_bytes_per_step": int(dec_bytes),
+               "api": "leco_decode_host (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        xs = x[: min(n, 20_000_000)].cpu().numpy().view(np.uint64)
+        threads = os.cpu_count() or 1
+        gbs, kind, sample, ref_ratio, rpay, roff = cpu_reference_decode(xs, BS, threads, budget_s=10.0)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample,
+               "ratio_on_sample": round(ref_ratio, 5)}
+        # the GPU stream of the same sample is byte-identical to the reference's
+        gcol = lc.encode(x[: len(xs)].contiguous(), lc.LINEAR, BS, lc.FIT_REFERENCE)
+        gp, go = gcol.to_host()
+        cpu["gpu_stream_identical_on_sample"] = bool(np.array_equal(gp, rpay) and np.array_equal(go, roff))
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "leco_fix u64 200M piecewise-linear sorted keys, 4096-value blocks, "
+                                   "bulk decode + 2^24 uniform random lookups per step",
+                       "keys_per_gpu": n, "block_size": BS, "blocks": col.nblocks, "ra_batch": RA_BATCH,
+                       "l2": "inputs and outputs larger than L2 (no flush needed)", "parallelism": f"shard{world}"},
+            "decode_ms": round(dec_mean, 4),
+            "ra_mlookups_s": round(ra_rate, 1),
+            "ra_batch_p50_us": round(float(np.percentile(ra_ms, 50)) * 1e3, 1),
+            "ra_batch_p99_us": round(float(np.percentile(ra_ms, 99)) * 1e3, 1),
+            "decode_p50_ms": round(float(np.percentile(dec_ms, 50)), 4),
+            "decode_p99_ms": round(float(np.percentile(dec_ms, 99)), 4),
+            "encode_gbs": {"fit_reference": round(dec_bytes / (t_enc['reference'] / 1e3) / 1e9, 2),
+                           "fit_exact": round(dec_bytes / (t_enc['exact'] / 1e3) / 1e9, 2)},
+            "compressed_ratio": round(comp / dec_bytes, 5),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "kernel": DECODE_KERNEL, "algorithmic_bytes_per_launch": int(alg_bytes)},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps * 2,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+/*
+ * leco.h -- C ABI of the B200 (sm_100a) LeCo integer codec.
+ *
+ * Drop-in boundary for the reference's per-block codec classes
+ * (yhliu918/Learn-to-Compress):
+ *   Leco_int<T>             headers/piecewise_fix_integer_template.h:14-338
+ *   FOR_int<T>              headers/FOR_integer_template.h:14-249
+ *   Delta_int<T>            headers/delta_integer_template.h:14-158
+ *   Leco_int_poly<T,2>      headers/poly_fix_integer_template.h:15-292
+ *   Leco_cost_merge_double_wo_round<uint64_t> (variable-length segments)
+ *                           headers/piecewise_cost_merge_integer_template_double_wo_round.h:18-700
+ * each with init / encodeArray8_int / decodeArray8 / randomdecodeArray8.
+ *
+ * The reference encodes a column as independent per-block byte strings held by
+ * its driver (experiments/leco_int_fix_template.cpp:108-127).  Here a column is
+ *   payload  : the reference block images concatenated, byte for byte,
+ *   offsets  : uint64 byte offset of block b in payload, offsets[nblocks] = total,
+ * so block b is exactly what the reference's encodeArray8_int writes for values
+ * [b*block_size, min(n, (b+1)*block_size)).  Payload buffers must be 8-byte
+ * aligned and extend LECO_PAYLOAD_SLACK bytes past the last block (kernels read
+ * whole 8-byte words).
+ *
+ * Conventions: all pointers named d_* are device pointers, h_* host pointers;
+ * every call is asynchronous on `stream` unless documented otherwise; status 0 =
+ * success, negative = error (leco_last_error() describes the last one on the
+ * calling thread).  No call allocates device memory unless its comment says so.
+ */
+#ifndef LECO_B200_H_
+#define LECO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *leco_stream_t; /* == cudaStream_t */
+
+enum leco_codec {
+  LECO_CODEC_LINEAR = 0, /* Leco_int<T>: OLS line + midpoint shift, signed residuals */
+  LECO_CODEC_FOR = 1,    /* FOR_int<T>: frame of reference, unsigned offsets        */
+  LECO_CODEC_DELTA = 2,  /* Delta_int<T>: signed first differences                  */
+  LECO_CODEC_POLY2 = 3,  /* Leco_int_poly<T,2>: degree-2 normal-equation fit        */
+  LECO_CODEC_VARLEN = 4  /* Leco_cost_merge_double_wo_round<uint64_t> segments      */
+};
+
+/* Value type = bytes per value. */
+enum leco_dtype { LECO_U32 = 4, LECO_U64 = 8 };
+
+/* How the encoder fits the block model.
+ * LECO_FIT_REFERENCE: the reference's sequential FP64 moment sums
+ *   (headers/lr.h:66-85, headers/polynomial_regression_internals.hpp:111-137),
+ *   so every block image is byte-identical to the reference encoder's.
+ * LECO_FIT_EXACT: exact 128-bit integer moment sums (parallel reduction), one
+ *   rounding to FP64, then the reference's formula.  Deterministic for any
+ *   launch shape; the stored model is what the reference decoder recomputes, so
+ *   the streams still decode bit-exactly in the reference's own decoder. */
+enum leco_fit_mode { LECO_FIT_REFERENCE = 0, LECO_FIT_EXACT = 1 };
+
+enum leco_status {
+  LECO_OK = 0,
+  LECO_ERR_ARG = -1,         /* bad argument (null pointer, size, codec/dtype)      */
+  LECO_ERR_CUDA = -2,        /* a CUDA runtime call failed                           */
+  LECO_ERR_CORRUPT = -3,     /* a block header or offset is not a valid stream       */
+  LECO_ERR_NOMEM = -4,       /* device or host allocation failed / admission refused */
+  LECO_ERR_TIMEOUT = -5,     /* a bounded device wait gave up (error word set)       */
+  LECO_ERR_UNSUPPORTED = -6, /* codec/dtype combination not provided                 */
+  LECO_ERR_CAPACITY = -7     /* output buffer smaller than the encoded size          */
+};
+
+#define LECO_PAYLOAD_SLACK 64u
+#define LECO_MAX_BLOCK 16384u
+
+/* Directory entry derived from a block header (32 bytes), kept device-resident
+ * so random access reads one L2-resident sector of metadata per lookup:
+ *   word0 = absolute bit address of field 0 | (l << 56) | (kind << 48)
+ *   a0,a1,a2 = model (theta0/theta1, poly coefficients, FOR base or Delta base
+ *   as raw 64-bit patterns). */
+typedef struct leco_dir_entry {
+  uint64_t word0;
+  double a0, a1, a2;
+} leco_dir_entry;
+
+/* ---- sizing (host, no device work) ------------------------------------ */
+
+/* Number of blocks of a column. */
+uint64_t leco_num_blocks(uint64_t n, uint32_t block_size);
+/* Upper bound on payload bytes (including LECO_PAYLOAD_SLACK). */
+uint64_t leco_max_payload_bytes(int codec, int dtype, uint64_t n, uint32_t block_size);
+/* Bytes of device workspace leco_encode needs (caller allocates). */
+uint64_t leco_encode_workspace_bytes(int codec, int dtype, uint64_t n, uint32_t block_size, int fit_mode);
+/* Exact byte size of one reference block image with l-bit fields
+ * (headers/bit_write.h:257-323 and :326-390 padding rules). */
+uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues);
+
+/* ---- column encode / decode / random access (device buffers) ---------- */
+
+/* Encodes n values (d_values, dtype) in blocks of block_size with `codec`
+ * (LINEAR, FOR, DELTA, POLY2).  Writes the concatenated reference block images
+ * to d_payload (capacity payload_cap bytes, see leco_max_payload_bytes),
+ * d_offsets[nblocks+1] and, when d_dir != NULL, the directory (nblocks
+ * entries).  Replaces the driver loop over <Codec>::encodeArray8_int
+ * (experiments/leco_int_fix_template.cpp:111-127).  One single-pass kernel
+ * (plus a sequential-fit kernel for LECO_FIT_REFERENCE columns whose FP64 sums
+ * round), a block-size prefix sum by decoupled look-back through d_workspace. */
+int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
+                uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
+                void *d_workspace, uint64_t workspace_bytes, leco_stream_t stream);
+
+/* Decodes a whole column into d_out[n].  Replaces <Codec>::decodeArray8 per block
+ * (piecewise_fix_integer_template.h:142-204, FOR_integer_template.h:83-112,
+ * delta_integer_template.h:89-127, poly_fix_integer_template.h:93-158).  A block
+ * is raw iff l == 8*sizeof(T) (the reference's random-access rule; its bulk
+ * decoders also treat l == 8*sizeof(T)-1 as raw, which mis-decodes such blocks). */
+int leco_decode(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                uint32_t block_size, void *d_out, leco_stream_t stream);
+
+/* Decodes values [first, first+count) of a column into d_out[count]
+ * (range scan: only the touched blocks are read). */
+int leco_decode_range(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                      uint32_t block_size, uint64_t first, uint64_t count, void *d_out, leco_stream_t stream);
+
+/* Builds the device directory from the block headers (after an import). */
+int leco_build_directory(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                         uint32_t block_size, leco_dir_entry *d_dir, leco_stream_t stream);
+
+/* Random access: d_out[i] = value d_idx[i] of the column, for i < m.  Replaces
+ * the per-index randomdecodeArray8 loop (experiments/leco_int_fix_template.cpp:189-207;
+ * piecewise_fix_integer_template.h:305-337, FOR_integer_template.h:218-245,
+ * delta_integer_template.h:132-154, poly_fix_integer_template.h:259-291).
+ * d_dir may be NULL (headers are then parsed from the payload). Indices >= n
+ * yield 0 and set the column error word (see leco_check). */
+int leco_gather(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets,
+                const leco_dir_entry *d_dir, uint64_t n, uint32_t block_size, const uint64_t *d_idx, uint64_t m,
+                void *d_out, leco_stream_t stream);
+
+/* Sum of all decoded values mod 2^64, written to *d_sum, without
+ * materialising the values (compressed-domain summation; the reference has
+ * one only for its legacy u32 codec, piecewise_fix_op.h:187-282).
+ * d_partials: device scratch of leco_sum_workspace_bytes() bytes. */
+uint64_t leco_sum_workspace_bytes(uint64_t n, uint32_t block_size);
+int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+             uint32_t block_size, uint64_t *d_sum, void *d_partials, leco_stream_t stream);
+
+/* ---- host-buffer entry points (synchronous; allocate device memory) ----
+ * These are the reference-facing calls: host in, host out, the same
+ * arguments as the reference's per-column driver loops. */
+
+/* Encodes h_values[n]; writes payload bytes and offsets[nblocks+1] to host
+ * buffers; *out_bytes = compressed size. */
+int leco_encode_host(int codec, int dtype, const void *h_values, uint64_t n, uint32_t block_size, int fit_mode,
+                     uint8_t *h_payload, uint64_t payload_cap, uint64_t *h_offsets, uint64_t *out_bytes);
+/* Decodes a host column into h_out[n]; copies are pipelined with the kernels. */
+int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
+                     uint32_t block_size, void *h_out);
+/* Random access from host indices into host output. */
+int leco_gather_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
+                     uint32_t block_size, const uint64_t *h_idx, uint64_t m, void *h_out);
+
+/* ---- per-block drop-in (one reference block, host buffers) ------------
+ * Byte-for-byte the reference methods' contracts; used by include/leco_codecs.hpp. */
+
+/* <Codec>::encodeArray8_int(data, length, res, nvalue): returns bytes written
+ * to h_out (which must hold leco_block_bytes(..., 8*dtype, length)), or a
+ * negative status. */
+int64_t leco_block_encode(int codec, int dtype, const void *h_values, uint32_t length, int fit_mode, uint8_t *h_out);
+/* <Codec>::decodeArray8(in, length, out, nvalue). in_bytes = image size. */
+int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length, void *h_out);
+/* <Codec>::randomdecodeArray8(in, to_find, NULL, 0) into *h_value. */
+int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
+                      uint32_t to_find, void *h_value);
+
+/* ---- validation / errors ------------------------------------------------ */
+
+/* Host-side validation of an imported column before any launch: offsets
+ * monotone and within payload_bytes, each header's l legal for the codec and
+ * each image size equal to leco_block_bytes(). Returns LECO_OK or
+ * LECO_ERR_CORRUPT (first bad block in *bad_block). */
+int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t payload_bytes,
+                       const uint64_t *h_offsets, uint64_t n, uint32_t block_size, uint64_t *bad_block);
+/* Reads and clears the device error word (bad index, bad header, bounded-wait
+ * timeout). Synchronous. Returns LECO_OK, LECO_ERR_CORRUPT or LECO_ERR_TIMEOUT. */
+int leco_check(leco_stream_t stream);
+/* Message of the last error on this thread ("" if none). */
+const char *leco_last_error(void);
+/* Library version string. */
+const char *leco_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LECO_B200_H_ */

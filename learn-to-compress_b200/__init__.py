@@ -1,0 +1,355 @@
+"""LeCo integer codec on B200 (sm_100a): Python host API over the C ABI.
+
+The product is the CUDA library ``lib/libleco_b200.so`` (sources in ``csrc/``,
+ABI in ``include/leco.h``).  This module binds it with ctypes and offers:
+
+* ``Leco_int``, ``FOR_int``, ``Delta_int``, ``Leco_int_poly`` -- per-block
+  mirrors of the reference classes (yhliu918/Learn-to-Compress
+  headers/piecewise_fix_integer_template.h:14-338, FOR_integer_template.h:14-249,
+  delta_integer_template.h:14-158, poly_fix_integer_template.h:15-292) with the
+  same ``init / encodeArray8_int / decodeArray8 / randomdecodeArray8`` methods on
+  host numpy buffers;
+* ``encode`` / ``Column`` -- whole columns resident in device memory (torch
+  tensors are used only as device allocations and for the stream handle):
+  decode, range decode, random access, compressed-domain sum.
+
+There is no CPU fallback: every call goes to the CUDA library, and importing
+the library fails loudly if it was not built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+
+LINEAR, FOR, DELTA, POLY2, VARLEN = 0, 1, 2, 3, 4
+U32, U64 = 4, 8
+FIT_REFERENCE, FIT_EXACT = 0, 1
+PAYLOAD_SLACK = 64
+MAX_BLOCK = 16384
+CODEC_NAMES = {LINEAR: "leco_fix", FOR: "for_fix", DELTA: "delta_fix", POLY2: "leco_poly2", VARLEN: "leco_varlen"}
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_U32 = ctypes.c_uint32
+_I = ctypes.c_int
+
+ERRORS = {
+    -1: "LECO_ERR_ARG", -2: "LECO_ERR_CUDA", -3: "LECO_ERR_CORRUPT", -4: "LECO_ERR_NOMEM",
+    -5: "LECO_ERR_TIMEOUT", -6: "LECO_ERR_UNSUPPORTED", -7: "LECO_ERR_CAPACITY",
+}
+
+
+class LecoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+# (name, restype, argtypes) of every entry point declared in include/leco.h
+SIGNATURES = [
+    ("leco_num_blocks", _U64, [_U64, _U32]),
+    ("leco_max_payload_bytes", _U64, [_I, _I, _U64, _U32]),
+    ("leco_encode_workspace_bytes", _U64, [_I, _I, _U64, _U32, _I]),
+    ("leco_block_bytes", _U64, [_I, _I, _U32, _U32]),
+    ("leco_encode", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P, _P, _U64, _P]),
+    ("leco_decode", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P]),
+    ("leco_decode_range", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _U64, _P, _P]),
+    ("leco_build_directory", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P]),
+    ("leco_gather", _I, [_I, _I, _P, _P, _P, _U64, _U32, _P, _U64, _P, _P]),
+    ("leco_sum_workspace_bytes", _U64, [_U64, _U32]),
+    ("leco_sum", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P, _P]),
+    ("leco_encode_host", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P]),
+    ("leco_decode_host", _I, [_I, _I, _P, _P, _U64, _U32, _P]),
+    ("leco_gather_host", _I, [_I, _I, _P, _P, _U64, _U32, _P, _U64, _P]),
+    ("leco_block_encode", ctypes.c_int64, [_I, _I, _P, _U32, _I, _P]),
+    ("leco_block_decode", _I, [_I, _I, _P, _U64, _U32, _P]),
+    ("leco_block_random", _I, [_I, _I, _P, _U64, _U32, _U32, _P]),
+    ("leco_validate_host", _I, [_I, _I, _P, _U64, _P, _U64, _U32, _P]),
+    ("leco_check", _I, [_P]),
+    ("leco_last_error", ctypes.c_char_p, []),
+    ("leco_version", ctypes.c_char_p, []),
+]
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib(build_if_missing: bool = True):
+    """The loaded CUDA library.  Raises if it is missing and cannot be built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise FileNotFoundError(f"{path} is not built (run learn-to-compress_b200/build.py)")
+        _build.build()
+    L = ctypes.CDLL(path)
+    for name, res, args in SIGNATURES:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _check(rc: int, what: str = "") -> int:
+    if rc < 0:
+        msg = lib().leco_last_error().decode()
+        raise LecoError(rc, f"{what}: {msg}" if what else msg)
+    return rc
+
+
+def _np_ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _dtype_of(arr) -> int:
+    s = arr.dtype.itemsize
+    if s not in (4, 8):
+        raise ValueError("values must be 32- or 64-bit unsigned integers")
+    return s
+
+
+def _np_dtype(s: int):
+    return np.uint64 if s == 8 else np.uint32
+
+
+# ---------------------------------------------------------------------------
+# Per-block mirrors of the reference classes (host buffers).
+# ---------------------------------------------------------------------------
+
+class _BlockCodec:
+    """Common part of the reference codec classes' per-block surface.
+
+    ``encodeArray8_int(data, length, res, nvalue)`` writes the reference block
+    image of ``data[:length]`` into the uint8 array ``res`` and returns the
+    number of bytes written (the reference returns the end pointer).
+    ``decodeArray8(in_, length, out, nvalue)`` decodes ``length`` values into
+    ``out`` and returns it.  ``randomdecodeArray8(in_, to_find, out, nvalue)``
+    returns value ``to_find`` of the block.  ``nvalue`` (the block id) and the
+    unused ``out`` argument are accepted for signature parity only.
+    """
+
+    CODEC = LINEAR
+
+    def __init__(self, dtype=np.uint64, fit_mode: int = FIT_REFERENCE):
+        self.dtype = np.dtype(dtype)
+        self.fit_mode = fit_mode
+        self.blocks = 0
+        self.block_size = 0
+
+    def init(self, block: int, block_s: int) -> None:
+        self.blocks = block
+        self.block_size = block_s
+
+    def encodeArray8_int(self, data, length: int, res: np.ndarray, nvalue: int = 0) -> int:
+        data = np.ascontiguousarray(np.asarray(data, dtype=self.dtype)[:length])
+        s = self.dtype.itemsize
+        need = lib().leco_block_bytes(self.CODEC, s, 8 * s, length) + 64
+        tmp = np.zeros(max(need, 64), np.uint8)
+        nbytes = _check(lib().leco_block_encode(self.CODEC, s, _np_ptr(data), length, self.fit_mode, _np_ptr(tmp)),
+                        "encodeArray8_int")
+        res[:nbytes] = tmp[:nbytes]
+        return nbytes
+
+    def decodeArray8(self, in_, length: int, out: Optional[np.ndarray] = None, nvalue: int = 0) -> np.ndarray:
+        buf = np.frombuffer(bytes(in_), np.uint8).copy()
+        s = self.dtype.itemsize
+        if out is None:
+            out = np.zeros(length, self.dtype)
+        o = np.zeros(length, self.dtype)
+        _check(lib().leco_block_decode(self.CODEC, s, _np_ptr(buf), len(buf), length, _np_ptr(o)), "decodeArray8")
+        out[:length] = o
+        return out
+
+    def randomdecodeArray8(self, in_, to_find: int, out=None, nvalue: int = 0, length: Optional[int] = None) -> int:
+        buf = np.frombuffer(bytes(in_), np.uint8).copy()
+        s = self.dtype.itemsize
+        n = length if length is not None else (self.block_size or to_find + 1)
+        v = np.zeros(1, self.dtype)
+        _check(lib().leco_block_random(self.CODEC, s, _np_ptr(buf), len(buf), n, to_find, _np_ptr(v)), "randomdecodeArray8")
+        return int(v[0])
+
+
+class Leco_int(_BlockCodec):
+    """Mirror of ``Codecset::Leco_int<T>`` (piecewise_fix_integer_template.h:14-338)."""
+    CODEC = LINEAR
+
+
+class FOR_int(_BlockCodec):
+    """Mirror of ``Codecset::FOR_int<T>`` (FOR_integer_template.h:14-249)."""
+    CODEC = FOR
+
+
+class Delta_int(_BlockCodec):
+    """Mirror of ``Codecset::Delta_int<T>`` (delta_integer_template.h:14-158)."""
+    CODEC = DELTA
+
+
+class Leco_int_poly(_BlockCodec):
+    """Mirror of ``Codecset::Leco_int_poly<T, 2>`` (poly_fix_integer_template.h:15-292)."""
+    CODEC = POLY2
+
+
+# ---------------------------------------------------------------------------
+# Device-resident columns.
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch  # plumbing only: device allocations and stream handles
+    return torch
+
+
+def _stream_ptr(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return _P(s.cuda_stream)
+
+
+def _tptr(t):
+    return _P(t.data_ptr()) if t is not None else None
+
+
+_TORCH_INT = {4: "int32", 8: "int64"}
+
+
+@dataclass
+class Column:
+    """An encoded column in device memory.
+
+    ``payload`` holds the reference block images back to back (plus
+    PAYLOAD_SLACK bytes), ``offsets[b]`` the byte offset of block b
+    (``offsets[nblocks]`` = compressed bytes), ``dir`` the 32-byte per-block
+    directory used by random access.
+    """
+    codec: int
+    dtype: int
+    n: int
+    block_size: int
+    payload: object
+    offsets: object
+    dir: object = None
+    _nbytes: Optional[int] = field(default=None, repr=False)
+
+    @property
+    def nblocks(self) -> int:
+        return (self.n + self.block_size - 1) // self.block_size
+
+    @property
+    def nbytes(self) -> int:
+        """Compressed bytes: the sum of the reference block image sizes."""
+        if self._nbytes is None:
+            self._nbytes = int(self.offsets[-1].item())
+        return self._nbytes
+
+    @property
+    def ratio(self) -> float:
+        return self.nbytes / (self.n * self.dtype)
+
+    def decode(self, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.n, dtype=getattr(torch, _TORCH_INT[self.dtype]), device=self.payload.device)
+        _check(lib().leco_decode(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n, self.block_size,
+                                 _tptr(out), _stream_ptr(stream)), "leco_decode")
+        return out
+
+    def decode_range(self, first: int, count: int, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(count, dtype=getattr(torch, _TORCH_INT[self.dtype]), device=self.payload.device)
+        _check(lib().leco_decode_range(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n,
+                                       self.block_size, first, count, _tptr(out), _stream_ptr(stream)), "leco_decode_range")
+        return out
+
+    def gather(self, idx, out=None, stream=None, use_dir: bool = True):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(idx.numel(), dtype=getattr(torch, _TORCH_INT[self.dtype]), device=self.payload.device)
+        _check(lib().leco_gather(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets),
+                                 _tptr(self.dir) if use_dir else None, self.n, self.block_size, _tptr(idx), idx.numel(),
+                                 _tptr(out), _stream_ptr(stream)), "leco_gather")
+        return out
+
+    def sum(self, out=None, stream=None) -> int:
+        torch = _torch()
+        if out is None:
+            out = torch.empty(1, dtype=torch.int64, device=self.payload.device)
+        _check(lib().leco_sum(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n, self.block_size,
+                              _tptr(out), None, _stream_ptr(stream)), "leco_sum")
+        return int(out.item()) & 0xFFFFFFFFFFFFFFFF
+
+    def build_directory(self, stream=None):
+        torch = _torch()
+        if self.dir is None:
+            self.dir = torch.empty(self.nblocks * 32, dtype=torch.uint8, device=self.payload.device)
+        _check(lib().leco_build_directory(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n,
+                                          self.block_size, _tptr(self.dir), _stream_ptr(stream)), "leco_build_directory")
+        return self.dir
+
+    def to_host(self):
+        """(payload bytes as uint8 numpy, offsets as uint64 numpy)."""
+        off = self.offsets.cpu().numpy().view(np.uint64)
+        pay = self.payload[: int(off[-1])].cpu().numpy()
+        return pay, off
+
+    @classmethod
+    def from_host(cls, codec: int, dtype: int, n: int, block_size: int, payload: np.ndarray, offsets: np.ndarray,
+                  device="cuda", validate: bool = True) -> "Column":
+        """Imports reference block images (e.g. from the reference encoder)."""
+        torch = _torch()
+        payload = np.ascontiguousarray(payload, np.uint8)
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        if validate:
+            bad = np.zeros(1, np.uint64)
+            _check(lib().leco_validate_host(codec, dtype, _np_ptr(payload), len(payload), _np_ptr(offsets), n, block_size,
+                                            _np_ptr(bad)), "leco_validate_host")
+        buf = np.zeros(len(payload) + PAYLOAD_SLACK, np.uint8)
+        buf[: len(payload)] = payload
+        col = cls(codec, dtype, n, block_size, torch.from_numpy(buf).to(device),
+                  torch.from_numpy(offsets.view(np.int64)).to(device))
+        col.build_directory()
+        return col
+
+
+def check(stream=None) -> None:
+    """Raises if a kernel set the device error word (bad index, header, timeout)."""
+    _check(lib().leco_check(_stream_ptr(stream)), "leco_check")
+
+
+def encode(values, codec: int = LINEAR, block_size: int = 4096, fit_mode: int = FIT_REFERENCE, stream=None,
+           with_dir: bool = True, workspace=None, payload=None) -> Column:
+    """Encodes a 1-D CUDA tensor of 32/64-bit integers (viewed as unsigned)."""
+    torch = _torch()
+    if not values.is_cuda:
+        raise ValueError("values must be a CUDA tensor")
+    s = values.element_size()
+    n = values.numel()
+    L = lib()
+    nb = L.leco_num_blocks(n, block_size)
+    cap = L.leco_max_payload_bytes(codec, s, n, block_size)
+    wsb = L.leco_encode_workspace_bytes(codec, s, n, block_size, fit_mode)
+    dev = values.device
+    if payload is None or payload.numel() < cap:
+        payload = torch.empty(cap, dtype=torch.uint8, device=dev)
+    offsets = torch.empty(nb + 1, dtype=torch.int64, device=dev)
+    d = torch.empty(nb * 32, dtype=torch.uint8, device=dev) if with_dir else None
+    if workspace is None or workspace.numel() < wsb:
+        workspace = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    _check(L.leco_encode(codec, s, _tptr(values), n, block_size, fit_mode, _tptr(payload), cap, _tptr(offsets), _tptr(d),
+                         _tptr(workspace), wsb, _stream_ptr(stream)), "leco_encode")
+    return Column(codec, s, n, block_size, payload, offsets, d)
+
+
+def version() -> str:
+    return lib().leco_version().decode()

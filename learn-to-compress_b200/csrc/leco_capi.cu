@@ -1,0 +1,472 @@
+// leco_capi.cu -- the C ABI (include/leco.h): argument checks, workspace
+// layout, launches, host-buffer pipelines and the per-block drop-in calls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "leco_device.cuh"
+#include "leco_internal.h"
+
+namespace leco {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+static int cuda_fail(cudaError_t e, const char *where) {
+  return fail(LECO_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define LECO_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+// Library-wide device error word: a file-scope __device__ variable, so no
+// allocation is needed.  Host code obtains its device address once per device.
+__device__ uint32_t g_error_word;
+static uint32_t *g_error_ptr[64];
+
+static int error_ptr(uint32_t **p) {
+  int dev = 0;
+  LECO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(LECO_ERR_ARG, "device ordinal out of range");
+  if (!g_error_ptr[dev]) LECO_CUDA(cudaGetSymbolAddress((void **)&g_error_ptr[dev], g_error_word));
+  *p = g_error_ptr[dev];
+  return LECO_OK;
+}
+
+static bool codec_ok(int codec) { return codec >= kLinear && codec <= kPoly2; }
+static bool dtype_ok(int dtype) { return dtype == LECO_U32 || dtype == LECO_U64; }
+
+void poly2_x_sums(uint32_t N, double X[5]) {
+  for (int k = 0; k < 5; ++k) {
+    double acc = 0;
+    for (uint32_t j = 0; j < N; ++j) {
+      double xr = 1.0, xj = (double)j;
+      if (k >= 1) xr = xj;
+      for (int d = 2; d <= k; ++d) xr = xr * xj;
+      acc += xr;
+    }
+    X[k] = acc;
+  }
+}
+
+// Workspace layout of leco_encode.
+struct EncWs {
+  uint64_t status_off, ticket_off, models_off, total;
+};
+static EncWs enc_ws(uint64_t nb, bool seq) {
+  EncWs w;
+  w.status_off = 0;
+  w.ticket_off = (nb * 8 + 255) / 256 * 256;
+  w.models_off = w.ticket_off + 256;
+  w.total = w.models_off + (seq ? (nb * 24 + 255) / 256 * 256 : 0);
+  return w;
+}
+// Whether LECO_FIT_REFERENCE needs the sequential fit kernel: for u32 linear
+// blocks of at most 2048 values every partial FP64 sum of lr.h:72-77 is an
+// exact integer, so the exact in-kernel moments reproduce it bit for bit.
+static bool needs_seq_fit(int codec, int dtype, uint32_t bs, int fit_mode) {
+  if (fit_mode != LECO_FIT_REFERENCE) return false;
+  if (codec == kLinear) return !(dtype == LECO_U32 && bs <= 2048);
+  return codec == kPoly2;
+}
+
+}  // namespace leco
+
+using namespace leco;
+
+extern "C" {
+
+const char *leco_last_error(void) { return g_last_error.c_str(); }
+const char *leco_version(void) { return "leco-b200 0.1 (sm_100a)"; }
+
+uint64_t leco_num_blocks(uint64_t n, uint32_t block_size) { return block_size ? (n + block_size - 1) / block_size : 0; }
+
+uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues) {
+  if (dtype == LECO_U32) {
+    switch (codec) {
+      case kLinear: return block_bytes<kLinear, 4>(l, nvalues);
+      case kFor: return block_bytes<kFor, 4>(l, nvalues);
+      case kDelta: return block_bytes<kDelta, 4>(l, nvalues);
+      case kPoly2: return block_bytes<kPoly2, 4>(l, nvalues);
+    }
+  } else if (dtype == LECO_U64) {
+    switch (codec) {
+      case kLinear: return block_bytes<kLinear, 8>(l, nvalues);
+      case kFor: return block_bytes<kFor, 8>(l, nvalues);
+      case kDelta: return block_bytes<kDelta, 8>(l, nvalues);
+      case kPoly2: return block_bytes<kPoly2, 8>(l, nvalues);
+    }
+  }
+  return 0;
+}
+
+uint64_t leco_max_payload_bytes(int codec, int dtype, uint64_t n, uint32_t block_size) {
+  if (!codec_ok(codec) || !dtype_ok(dtype) || !block_size) return 0;
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  // Worst block: raw (1 + n*s) or the widest packed image; the packed image
+  // with l = 8s-1 never exceeds raw + header + 16 bytes.
+  return n * (uint64_t)dtype + nb * 48 + LECO_PAYLOAD_SLACK;
+}
+
+uint64_t leco_encode_workspace_bytes(int codec, int dtype, uint64_t n, uint32_t block_size, int fit_mode) {
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  return enc_ws(nb, needs_seq_fit(codec, dtype, block_size, fit_mode)).total;
+}
+
+int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
+                uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
+                void *d_workspace, uint64_t workspace_bytes, leco_stream_t stream) {
+  if (!codec_ok(codec)) return fail(LECO_ERR_UNSUPPORTED, "leco_encode: codec must be LINEAR, FOR, DELTA or POLY2");
+  if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, "leco_encode: dtype must be LECO_U32 or LECO_U64");
+  if (!block_size || block_size > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, "leco_encode: block_size must be in 1..16384");
+  if (n == 0) return fail(LECO_ERR_ARG, "leco_encode: n must be > 0");
+  if (!d_values || !d_payload || !d_offsets || !d_workspace) return fail(LECO_ERR_ARG, "leco_encode: null pointer");
+  if ((reinterpret_cast<uintptr_t>(d_payload) & 7) || (reinterpret_cast<uintptr_t>(d_values) & (dtype - 1)))
+    return fail(LECO_ERR_ARG, "leco_encode: payload must be 8-byte aligned and values aligned to their size");
+  if (fit_mode != LECO_FIT_REFERENCE && fit_mode != LECO_FIT_EXACT) return fail(LECO_ERR_ARG, "leco_encode: bad fit_mode");
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  if (nb > 0xffffffffull) return fail(LECO_ERR_ARG, "leco_encode: too many blocks");
+  const bool seq = needs_seq_fit(codec, dtype, block_size, fit_mode);
+  const EncWs w = enc_ws(nb, seq);
+  if (workspace_bytes < w.total) return fail(LECO_ERR_ARG, "leco_encode: workspace too small");
+  uint32_t *err = nullptr;
+  int rc = error_ptr(&err);
+  if (rc) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  uint8_t *ws = static_cast<uint8_t *>(d_workspace);
+  LECO_CUDA(cudaMemsetAsync(ws, 0, w.models_off, st));  // status words + ticket
+  EncodeLaunch L;
+  L.values = d_values; L.n = n; L.bs = block_size; L.nb = nb;
+  L.payload = d_payload; L.payload_cap = payload_cap; L.offsets = d_offsets; L.dir = d_dir;
+  L.seq_models = seq ? reinterpret_cast<double *>(ws + w.models_off) : nullptr;
+  L.status = reinterpret_cast<uint64_t *>(ws + w.status_off);
+  L.ticket = reinterpret_cast<uint32_t *>(ws + w.ticket_off);
+  L.error = err;
+  for (int i = 0; i < 10; ++i) L.polyX[i] = 0;
+  if (codec == kPoly2) {
+    poly2_x_sums(std::min<uint64_t>(n, block_size), L.polyX);
+    const uint64_t tail = n - (nb - 1) * block_size;
+    poly2_x_sums((uint32_t)tail, L.polyX + 5);
+  }
+  if (launch_encode(codec, dtype, L, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_encode: no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+static int check_column(const char *fn, int codec, int dtype, const void *payload, const void *offsets, uint32_t bs) {
+  if (!codec_ok(codec)) return fail(LECO_ERR_UNSUPPORTED, std::string(fn) + ": codec must be LINEAR, FOR, DELTA or POLY2");
+  if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, std::string(fn) + ": dtype must be LECO_U32 or LECO_U64");
+  if (!bs || bs > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, std::string(fn) + ": block_size must be in 1..16384");
+  if (!payload || !offsets) return fail(LECO_ERR_ARG, std::string(fn) + ": null pointer");
+  if (reinterpret_cast<uintptr_t>(payload) & 7) return fail(LECO_ERR_ARG, std::string(fn) + ": payload must be 8-byte aligned");
+  return LECO_OK;
+}
+
+int leco_decode(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                uint32_t block_size, void *d_out, leco_stream_t stream) {
+  return leco_decode_range(codec, dtype, d_payload, d_offsets, n, block_size, 0, n, d_out, stream);
+}
+
+int leco_decode_range(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                      uint32_t block_size, uint64_t first, uint64_t count, void *d_out, leco_stream_t stream) {
+  int rc = check_column("leco_decode", codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (!d_out || (reinterpret_cast<uintptr_t>(d_out) & (dtype - 1))) return fail(LECO_ERR_ARG, "leco_decode: out null or misaligned");
+  if (first > n || count > n - first) return fail(LECO_ERR_ARG, "leco_decode: range outside the column");
+  if (!count) return LECO_OK;
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  DecodeLaunch L{d_payload, d_offsets, n, block_size, first, count, d_out, err};
+  if (launch_decode(codec, dtype, L, reinterpret_cast<cudaStream_t>(stream))) return fail(LECO_ERR_UNSUPPORTED, "no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+int leco_build_directory(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                         uint32_t block_size, leco_dir_entry *d_dir, leco_stream_t stream) {
+  int rc = check_column("leco_build_directory", codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (!d_dir) return fail(LECO_ERR_ARG, "leco_build_directory: null directory");
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  if (launch_build_dir(codec, dtype, d_payload, d_offsets, n, block_size, d_dir, err, reinterpret_cast<cudaStream_t>(stream)))
+    return fail(LECO_ERR_UNSUPPORTED, "no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+int leco_gather(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets,
+                const leco_dir_entry *d_dir, uint64_t n, uint32_t block_size, const uint64_t *d_idx, uint64_t m,
+                void *d_out, leco_stream_t stream) {
+  int rc = check_column("leco_gather", codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (m && (!d_idx || !d_out)) return fail(LECO_ERR_ARG, "leco_gather: null pointer");
+  if (!m) return LECO_OK;
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  GatherLaunch L{d_payload, d_offsets, d_dir, n, block_size, d_idx, m, d_out, err};
+  if (launch_gather(codec, dtype, L, reinterpret_cast<cudaStream_t>(stream))) return fail(LECO_ERR_UNSUPPORTED, "no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+uint64_t leco_sum_workspace_bytes(uint64_t n, uint32_t block_size) {
+  (void)n;
+  (void)block_size;
+  return 0;
+}
+
+int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+             uint32_t block_size, uint64_t *d_sum, void *d_partials, leco_stream_t stream) {
+  (void)d_partials;
+  int rc = check_column("leco_sum", codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (!d_sum) return fail(LECO_ERR_ARG, "leco_sum: null output");
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  LECO_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(uint64_t), st));
+  DecodeLaunch L{d_payload, d_offsets, n, block_size, 0, n, nullptr, err};
+  if (launch_sum(codec, dtype, L, d_sum, st)) return fail(LECO_ERR_UNSUPPORTED, "no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+int leco_check(leco_stream_t stream) {
+  uint32_t *err = nullptr;
+  int rc = error_ptr(&err);
+  if (rc) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  uint32_t h = 0;
+  LECO_CUDA(cudaMemcpyAsync(&h, err, 4, cudaMemcpyDeviceToHost, st));
+  LECO_CUDA(cudaStreamSynchronize(st));
+  if (h) LECO_CUDA(cudaMemsetAsync(err, 0, 4, st));
+  LECO_CUDA(cudaStreamSynchronize(st));
+  if (h & kErrTimeout) return fail(LECO_ERR_TIMEOUT, "device wait gave up (look-back or queue)");
+  if (h & kErrCapacity) return fail(LECO_ERR_CAPACITY, "payload buffer smaller than the encoded column");
+  if (h & kErrBadHeader) return fail(LECO_ERR_CORRUPT, "invalid block header");
+  if (h & kErrBadIndex) return fail(LECO_ERR_CORRUPT, "index outside the column");
+  return LECO_OK;
+}
+
+// ---- host-side validation ------------------------------------------------------------
+
+int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t payload_bytes,
+                       const uint64_t *h_offsets, uint64_t n, uint32_t block_size, uint64_t *bad_block) {
+  int rc = check_column("leco_validate_host", codec, dtype, h_payload, h_offsets, block_size);
+  if (rc) return rc;
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  const uint32_t tb = 8u * (uint32_t)dtype;
+  for (uint64_t b = 0; b < nb; ++b) {
+    const uint64_t o = h_offsets[b], e = h_offsets[b + 1];
+    const uint32_t len = (uint32_t)std::min<uint64_t>(block_size, n - b * block_size);
+    bool ok = o < e && e <= payload_bytes;
+    if (ok) {
+      const uint32_t l = h_payload[o];
+      bool sentinel = (l == 126 || l == 127) && codec != kFor;
+      if (sentinel) ok = e - o >= 1 + (uint64_t)dtype * (l == 127 ? 1 : 2);
+      else ok = l <= tb && (e - o) == leco_block_bytes(codec, dtype, l, len);
+      if (ok && codec == kFor && l > 0 && l < tb) {
+        // FOR: header max - min must need exactly l bits (FOR_integer_template.h:43-49)
+        uint64_t mn = 0, mx = 0;
+        memcpy(&mn, h_payload + o + 1, dtype);
+        memcpy(&mx, h_payload + o + 1 + dtype, dtype);
+        ok = mx >= mn;
+      }
+    }
+    if (!ok) {
+      if (bad_block) *bad_block = b;
+      return fail(LECO_ERR_CORRUPT, "leco_validate_host: block " + std::to_string(b) + " is not a valid image");
+    }
+  }
+  return LECO_OK;
+}
+
+// ---- host-buffer pipelines -------------------------------------------------------------
+
+struct DevBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  cudaError_t alloc(size_t bytes, cudaStream_t s) {
+    st = s;
+    return cudaMallocAsync(&p, bytes ? bytes : 1, s);
+  }
+};
+
+int leco_encode_host(int codec, int dtype, const void *h_values, uint64_t n, uint32_t block_size, int fit_mode,
+                     uint8_t *h_payload, uint64_t payload_cap, uint64_t *h_offsets, uint64_t *out_bytes) {
+  if (!h_values || !h_payload || !h_offsets) return fail(LECO_ERR_ARG, "leco_encode_host: null pointer");
+  if (!codec_ok(codec) || !dtype_ok(dtype) || !block_size || block_size > LECO_MAX_BLOCK || !n)
+    return fail(LECO_ERR_ARG, "leco_encode_host: bad codec/dtype/block_size/n");
+  cudaStream_t st;
+  LECO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int rc = LECO_OK;
+  {
+    const uint64_t nb = leco_num_blocks(n, block_size);
+    const uint64_t cap = leco_max_payload_bytes(codec, dtype, n, block_size);
+    const uint64_t wsb = leco_encode_workspace_bytes(codec, dtype, n, block_size, fit_mode);
+    DevBuf dv, dp, doff, dws;
+    if (dv.alloc(n * dtype, st) || dp.alloc(cap, st) || doff.alloc((nb + 1) * 8, st) || dws.alloc(wsb, st)) {
+      rc = fail(LECO_ERR_NOMEM, "leco_encode_host: device allocation failed");
+    } else {
+      cudaMemcpyAsync(dv.p, h_values, n * dtype, cudaMemcpyHostToDevice, st);
+      rc = leco_encode(codec, dtype, dv.p, n, block_size, fit_mode, (uint8_t *)dp.p, cap, (uint64_t *)doff.p, nullptr,
+                       dws.p, wsb, reinterpret_cast<leco_stream_t>(st));
+      if (!rc) {
+        cudaMemcpyAsync(h_offsets, doff.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        rc = leco_check(reinterpret_cast<leco_stream_t>(st));
+      }
+      if (!rc) {
+        const uint64_t total = h_offsets[nb];
+        if (out_bytes) *out_bytes = total;
+        if (total > payload_cap) rc = fail(LECO_ERR_CAPACITY, "leco_encode_host: payload_cap too small");
+        else cudaMemcpyAsync(h_payload, dp.p, total, cudaMemcpyDeviceToHost, st);
+      }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(e, "leco_encode_host");
+  return rc;
+}
+
+// Decodes a host column in chunks of whole blocks on two streams, so the
+// host->device copy of one chunk, the decode of another and the device->host
+// copy of a third overlap.
+int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
+                     uint32_t block_size, void *h_out) {
+  int rc = check_column("leco_decode_host", codec, dtype, h_payload, h_offsets, block_size);
+  if (rc) return rc;
+  if (!h_out) return fail(LECO_ERR_ARG, "leco_decode_host: null output");
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  if (!nb) return LECO_OK;
+  const uint64_t total = h_offsets[nb];
+  // chunk = ~64 MiB of decoded values, whole blocks
+  uint64_t bpc = std::max<uint64_t>(1, (64ull << 20) / ((uint64_t)block_size * dtype));
+  bpc = std::min(bpc, nb);
+  const int NS = 2;
+  cudaStream_t st[NS];
+  for (int i = 0; i < NS; ++i) LECO_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
+  DevBuf pay[NS], off[NS], out[NS];
+  uint64_t max_chunk_bytes = 0;
+  for (uint64_t b0 = 0; b0 < nb; b0 += bpc) {
+    uint64_t b1 = std::min(nb, b0 + bpc);
+    max_chunk_bytes = std::max(max_chunk_bytes, h_offsets[b1] - h_offsets[b0]);
+  }
+  for (int i = 0; i < NS && !rc; ++i) {
+    if (pay[i].alloc(max_chunk_bytes + LECO_PAYLOAD_SLACK + 8, st[i]) || off[i].alloc((bpc + 1) * 8, st[i]) ||
+        out[i].alloc(bpc * block_size * (uint64_t)dtype, st[i]))
+      rc = fail(LECO_ERR_NOMEM, "leco_decode_host: device allocation failed");
+  }
+  std::vector<std::vector<uint64_t>> rel(NS, std::vector<uint64_t>(bpc + 1));
+  uint64_t chunk = 0;
+  for (uint64_t b0 = 0; b0 < nb && !rc; b0 += bpc, ++chunk) {
+    const int i = (int)(chunk % NS);
+    cudaStream_t s = st[i];
+    const uint64_t b1 = std::min(nb, b0 + bpc), cb = b1 - b0;
+    const uint64_t pbase = h_offsets[b0] & ~7ull;  // keep the 8-byte word alignment of bit addresses
+    cudaStreamSynchronize(s);                       // rel[i] and the buffers are reused
+    for (uint64_t b = 0; b <= cb; ++b) rel[i][b] = h_offsets[b0 + b] - pbase;
+    const uint64_t nbytes = h_offsets[b1] - pbase;
+    cudaMemcpyAsync(pay[i].p, h_payload + pbase, std::min<uint64_t>(nbytes + 8, total - pbase), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(off[i].p, rel[i].data(), (cb + 1) * 8, cudaMemcpyHostToDevice, s);
+    const uint64_t v0 = b0 * block_size, nv = std::min<uint64_t>(n, b1 * block_size) - v0;
+    rc = leco_decode(codec, dtype, (const uint8_t *)pay[i].p, (const uint64_t *)off[i].p, nv, block_size, out[i].p,
+                     reinterpret_cast<leco_stream_t>(s));
+    cudaMemcpyAsync(static_cast<uint8_t *>(h_out) + v0 * dtype, out[i].p, nv * dtype, cudaMemcpyDeviceToHost, s);
+  }
+  for (int i = 0; i < NS; ++i) {
+    cudaError_t e = cudaStreamSynchronize(st[i]);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "leco_decode_host");
+  }
+  if (!rc) rc = leco_check(reinterpret_cast<leco_stream_t>(st[0]));
+  for (int i = 0; i < NS; ++i) {
+    pay[i].~DevBuf(); pay[i].p = nullptr;
+    off[i].~DevBuf(); off[i].p = nullptr;
+    out[i].~DevBuf(); out[i].p = nullptr;
+    cudaStreamSynchronize(st[i]);
+    cudaStreamDestroy(st[i]);
+  }
+  return rc;
+}
+
+int leco_gather_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
+                     uint32_t block_size, const uint64_t *h_idx, uint64_t m, void *h_out) {
+  int rc = check_column("leco_gather_host", codec, dtype, h_payload, h_offsets, block_size);
+  if (rc) return rc;
+  if (m && (!h_idx || !h_out)) return fail(LECO_ERR_ARG, "leco_gather_host: null pointer");
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  cudaStream_t st;
+  LECO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  {
+    const uint64_t total = h_offsets[nb];
+    DevBuf dp, doff, ddir, didx, dout;
+    if (dp.alloc(total + LECO_PAYLOAD_SLACK, st) || doff.alloc((nb + 1) * 8, st) || ddir.alloc(nb * sizeof(leco_dir_entry), st) ||
+        didx.alloc(m * 8, st) || dout.alloc(m * dtype, st)) {
+      rc = fail(LECO_ERR_NOMEM, "leco_gather_host: device allocation failed");
+    } else {
+      cudaMemsetAsync((uint8_t *)dp.p + total, 0, LECO_PAYLOAD_SLACK, st);
+      cudaMemcpyAsync(dp.p, h_payload, total, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(doff.p, h_offsets, (nb + 1) * 8, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(didx.p, h_idx, m * 8, cudaMemcpyHostToDevice, st);
+      leco_stream_t ls = reinterpret_cast<leco_stream_t>(st);
+      rc = leco_build_directory(codec, dtype, (const uint8_t *)dp.p, (const uint64_t *)doff.p, n, block_size,
+                                (leco_dir_entry *)ddir.p, ls);
+      if (!rc)
+        rc = leco_gather(codec, dtype, (const uint8_t *)dp.p, (const uint64_t *)doff.p, (const leco_dir_entry *)ddir.p, n,
+                         block_size, (const uint64_t *)didx.p, m, dout.p, ls);
+      if (!rc) cudaMemcpyAsync(h_out, dout.p, m * dtype, cudaMemcpyDeviceToHost, st);
+      if (!rc) rc = leco_check(ls);
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(e, "leco_gather_host");
+  return rc;
+}
+
+// ---- per-block drop-in -----------------------------------------------------------------
+
+int64_t leco_block_encode(int codec, int dtype, const void *h_values, uint32_t length, int fit_mode, uint8_t *h_out) {
+  if (!length || length > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, "leco_block_encode: length must be in 1..16384");
+  const uint64_t cap = leco_max_payload_bytes(codec, dtype, length, length);
+  std::vector<uint8_t> tmp(cap);
+  uint64_t off[2], bytes = 0;
+  int rc = leco_encode_host(codec, dtype, h_values, length, length, fit_mode, tmp.data(), cap, off, &bytes);
+  if (rc) return rc;
+  memcpy(h_out, tmp.data(), bytes);
+  return (int64_t)bytes;
+}
+
+int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length, void *h_out) {
+  if (!h_in || !h_out || !length) return fail(LECO_ERR_ARG, "leco_block_decode: bad argument");
+  std::vector<uint8_t> tmp(in_bytes + LECO_PAYLOAD_SLACK, 0);
+  memcpy(tmp.data(), h_in, in_bytes);
+  uint64_t off[2] = {0, in_bytes};
+  return leco_decode_host(codec, dtype, tmp.data(), off, length, length, h_out);
+}
+
+int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
+                      uint32_t to_find, void *h_value) {
+  if (!h_in || !h_value || to_find >= length) return fail(LECO_ERR_ARG, "leco_block_random: bad argument");
+  std::vector<uint8_t> tmp(in_bytes + LECO_PAYLOAD_SLACK, 0);
+  memcpy(tmp.data(), h_in, in_bytes);
+  uint64_t off[2] = {0, in_bytes};
+  uint64_t idx = to_find;
+  return leco_gather_host(codec, dtype, tmp.data(), off, length, length, &idx, 1, h_value);
+}
+
+}  // extern "C"

@@ -1,0 +1,379 @@
+// leco_decode.cu -- bulk decode, range decode, compressed-domain sum, random
+// access and directory build for the LeCo fixed-block codecs.
+//
+// Bulk decode replaces <Codec>::decodeArray8 per block:
+//   Leco_int     piecewise_fix_integer_template.h:142-204 + read_all_bit_fix (bit_read.h:222-275)
+//   FOR_int      FOR_integer_template.h:83-112 + read_all_bit_FOR (bit_read.h:1373-1414)
+//   Delta_int    delta_integer_template.h:89-127 + read_all_bit_Delta (bit_read.h:1319-1370)
+//   Leco_int_poly poly_fix_integer_template.h:93-158 + read_all_bit_fix_poly (bit_read.h:277-330)
+// Random access replaces randomdecodeArray8 (piecewise_fix_integer_template.h:305-337,
+// FOR_integer_template.h:218-245, delta_integer_template.h:132-154,
+// poly_fix_integer_template.h:259-291).
+//
+// A block is raw iff l == 8*sizeof(T) everywhere (the reference's random-access
+// rule).  The reference's bulk decoders also call l == 8*sizeof(T)-1 raw, which
+// mis-decodes such packed blocks; this decoder reads them correctly.
+#include "leco_device.cuh"
+#include "leco_internal.h"
+
+namespace leco {
+
+// Block model parsed from a header (or a directory entry).
+struct BlockHdr {
+  uint64_t body_bit;  // absolute bit address of field 0 (raw: of value 0)
+  uint32_t l;         // field width; 8*S = raw; 126/127 = 2/1-value sentinels
+  double a0, a1, a2;  // model
+  uint64_t base;      // FOR minimum / Delta first value
+};
+
+template <int CODEC, int S>
+__device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ payload, uint64_t off) {
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
+  BlockHdr h;
+  uint64_t w0 = load_u64_at(words, off);
+  h.l = (uint32_t)(w0 & 0xff);
+  h.a0 = h.a1 = h.a2 = 0;
+  h.base = 0;
+  if (h.l == 8u * S || h.l == 126 || h.l == 127) {
+    h.body_bit = (off + 1) * 8;
+    return h;
+  }
+  if (CODEC == kLinear || CODEC == kPoly2) {
+    h.a0 = __longlong_as_double((long long)load_u64_at(words, off + 1));
+    h.a1 = __longlong_as_double((long long)load_u64_at(words, off + 9));
+    if (CODEC == kPoly2) h.a2 = __longlong_as_double((long long)load_u64_at(words, off + 17));
+  } else {
+    uint64_t v = load_u64_at(words, off + 1);
+    h.base = S == 8 ? v : (v & 0xffffffffull);
+  }
+  h.body_bit = (off + Hdr<CODEC, S>::bytes) * 8;
+  return h;
+}
+
+template <int CODEC, int S>
+__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b) {
+  const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
+  ulonglong2 q0 = __ldg(p), q1 = __ldg(p + 1);
+  BlockHdr h;
+  h.body_bit = q0.x & ((1ull << 48) - 1);
+  h.l = (uint32_t)(q0.x >> 56);
+  h.a0 = __longlong_as_double((long long)q0.y);
+  h.a1 = __longlong_as_double((long long)q1.x);
+  h.a2 = __longlong_as_double((long long)q1.y);
+  h.base = S == 8 ? q0.y : (q0.y & 0xffffffffull);
+  return h;
+}
+
+// Value k of a non-raw, non-Delta block given its field f (bulk decode rules).
+template <int CODEC, int S>
+__device__ __forceinline__ uint64_t value_from_field(const BlockHdr &h, uint32_t k, uint64_t f) {
+  if (CODEC == kFor) return h.base + f;
+  int64_t pred;
+  if (CODEC == kLinear) pred = f2i_x86(pred_linear(h.a0, h.a1, k));
+  else pred = f2i_x86(pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k)));
+  return h.l ? apply_signed((uint64_t)pred, f, h.l) : (uint64_t)pred;
+}
+
+// Delta running sum split over the CTA: each thread owns a contiguous chunk
+// [k0, k1) of values; a block-wide exclusive scan of the chunks' delta sums
+// gives each thread the value at k0.  Must be called by all threads.
+struct DeltaChunk {
+  uint32_t k0, k1;
+  uint64_t run;  // decoded value k0 (mod 2^64)
+};
+__device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len) {
+  __shared__ uint64_t wsum[32];
+  const uint32_t nt = blockDim.x, tid = threadIdx.x;
+  const uint32_t chunk = (len + nt - 1) / nt;
+  DeltaChunk c;
+  c.k0 = min(len, tid * chunk);
+  c.k1 = min(len, c.k0 + chunk);
+  uint64_t local = 0;  // fields k0 .. k1-1 feed values k0+1 .. k1; field len-1 is not a delta
+  if (h.l)
+    for (uint32_t k = c.k0; k < c.k1 && k + 1 < len; ++k)
+      local += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+  const int lane = tid & 31, warp = tid >> 5;
+  uint64_t incl = local;
+  for (int d = 1; d < 32; d <<= 1) {
+    uint64_t y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (nt + 31) >> 5;
+    uint64_t x = lane < nw ? wsum[lane] : 0, xi = x;
+    for (int d = 1; d < 32; d <<= 1) {
+      uint64_t y = __shfl_up_sync(0xffffffffu, xi, d);
+      if (lane >= d) xi += y;
+    }
+    if (lane < nw) wsum[lane] = xi - x;
+  }
+  __syncthreads();
+  c.run = h.base + wsum[warp] + (incl - local);
+  return c;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v, int cnt, bool full);
+
+// ---- bulk / range decode ----------------------------------------------------
+// One CTA per block.  Each thread decodes VEC = 16/sizeof(T) consecutive values
+// per step from a three-word window of the packed body and writes them with one
+// 16-byte store.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  constexpr int VEC = 16 / S;
+  const uint64_t bfirst = a.first / a.bs;
+  const uint64_t b = bfirst + blockIdx.x;
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  // values of this block inside [first, first+count)
+  const uint64_t r0 = a.first > base ? a.first : base, r1 = umin64(a.first + a.count, base + len);
+  if (r0 >= r1) return;
+  const uint32_t lo = (uint32_t)(r0 - base), hi = (uint32_t)(r1 - base);
+  T *out = reinterpret_cast<T *>(a.out);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+  const uint64_t obase = base - a.first;  // out index of block value 0
+
+  if (h.l == 126 || h.l == 127) {  // sentinel blocks (…_integer_template.h:152-170)
+    if (CODEC == kFor) { if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader); return; }
+    if (threadIdx.x == 0) {
+      const uint32_t cnt = h.l == 127 ? 1 : 2;
+      for (uint32_t k = lo; k < cnt && k < hi; ++k)
+        out[obase + k] = (T)load_field(words, h.body_bit + (uint64_t)k * TB, TB);
+    }
+    return;
+  }
+  if (h.l > TB) {
+    if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader);
+    return;
+  }
+  const bool raw = h.l == TB;
+
+  if (CODEC == kDelta && !raw) {
+    // Running sum: value k = x0 + sum_{i<k} signed(field_i) (mod 2^(8S)).
+    const DeltaChunk c = delta_chunk_start(words, h, len);
+    uint64_t run = c.run;
+    for (uint32_t k = c.k0; k < c.k1; ++k) {
+      if (k >= lo && k < hi) out[obase + k] = (T)run;
+      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+    }
+    return;
+  }
+
+  const uint32_t l = raw ? TB : h.l;
+  // First vector start so that out[obase + kv] is 16-byte aligned (out must be
+  // sizeof(T)-aligned); kv may start up to VEC-1 values before lo.
+  const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + obase + lo);
+  const int32_t kstart = (int32_t)lo - (int32_t)((oaddr & 15) / S);
+  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
+    uint64_t v[VEC];
+    const uint32_t kw = kv < (int32_t)lo ? lo : (uint32_t)kv;  // first value actually needed
+    if (l) {
+      const uint64_t bit0 = h.body_bit + (uint64_t)kw * l;
+      const uint64_t w = bit0 >> 6;
+      const uint64_t W0 = __ldg(words + w), W1 = __ldg(words + w + 1), W2 = __ldg(words + w + 2);
+      const uint32_t sh0 = (uint32_t)(bit0 & 63);
+#pragma unroll
+      for (int j = 0; j < VEC; ++j) {
+        const int32_t k = kv + j;
+        const uint32_t rel = sh0 + (uint32_t)(k - (int32_t)kw) * l;  // unused when k < kw
+        const uint32_t sh = rel & 63;
+        const uint64_t lo64 = rel < 64 ? W0 : (rel < 128 ? W1 : W2);
+        const uint64_t hi64 = rel < 64 ? W1 : W2;
+        const uint64_t f = funnel64(lo64, hi64, sh) & lowmask(l);
+        v[j] = raw ? f : value_from_field<CODEC, S>(h, (uint32_t)k, f);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; ++j) v[j] = value_from_field<CODEC, S>(h, (uint32_t)(kv + j), 0);
+    }
+    const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
+    store_vals<T>(out, obase + kv, v, VEC, full);
+    if (!full) {
+#pragma unroll
+      for (int j = 0; j < VEC; ++j)
+        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
+    }
+  }
+}
+
+template <>
+__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
+  if (full) __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
+}
+template <>
+__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
+  if (full) __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
+}
+
+// ---- compressed-domain sum ----------------------------------------------------
+// Sum of decoded values mod 2^64 without writing them: reads only the payload.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_sum) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  __shared__ u128 red[33];
+  const uint64_t b = blockIdx.x;
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+  const uint64_t tmask = S == 8 ? ~0ull : 0xffffffffull;
+  uint64_t acc = 0;
+  if (h.l == 126 || h.l == 127 || h.l > TB) {
+    if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader);
+    return;
+  }
+  const bool raw = h.l == TB;
+  if (CODEC == kDelta && !raw) {
+    const DeltaChunk c = delta_chunk_start(words, h, len);
+    uint64_t run = c.run;
+    for (uint32_t k = c.k0; k < c.k1; ++k) {
+      acc += run & tmask;
+      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+    }
+  } else {
+    const uint32_t l = raw ? TB : h.l;
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+      uint64_t f = l ? load_field(words, h.body_bit + (uint64_t)k * l, l) : 0;
+      acc += (raw ? f : value_from_field<CODEC, S>(h, k, f)) & tmask;
+    }
+  }
+  acc = (uint64_t)block_reduce<5>((u128)acc, red);
+  if (threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long *>(d_sum), (unsigned long long)acc);
+}
+
+// ---- random access --------------------------------------------------------------
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) gather_kernel(GatherLaunch a) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  T *out = reinterpret_cast<T *>(a.out);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = __ldg(a.idx + i);
+    if (g >= a.n) {
+      out[i] = 0;
+      atomicOr(a.error, kErrBadIndex);
+      continue;
+    }
+    uint64_t b;
+    uint32_t k;
+    if (a.n <= 0xffffffffull) {
+      b = (uint32_t)g / a.bs;
+      k = (uint32_t)g - (uint32_t)b * a.bs;
+    } else {
+      b = g / a.bs;
+      k = (uint32_t)(g - b * a.bs);
+    }
+    const BlockHdr h = a.dir ? from_dir<CODEC, S>(a.dir, b) : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+    uint64_t v;
+    if (h.l == TB) {
+      v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);  // raw (…_integer_template.h:313-317)
+    } else if (h.l > TB) {
+      v = 0;  // sentinel / corrupt header: the reference's random access has no such case
+      atomicOr(a.error, kErrBadHeader);
+    } else if (CODEC == kLinear) {
+      const double p = pred_linear(h.a0, h.a1, k);
+      if (h.l) v = apply_signed((uint64_t)f2i_x86(p), load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+      else v = f2T_x86<S>(p);  // (T)(theta0 + k*theta1) directly (:334)
+    } else if (CODEC == kPoly2) {
+      const double p = pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
+      if (h.l) v = apply_signed((uint64_t)f2i_x86(p), load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+      else v = f2T_x86<S>(p);  // poly_fix_integer_template.h:288
+    } else if (CODEC == kFor) {
+      v = h.l ? h.base + load_field(words, h.body_bit + (uint64_t)k * h.l, h.l) : h.base;
+    } else {  // Delta: prefix walk over fields 0..k-1 (bit_read.h:1292-1317)
+      v = h.base;
+      if (h.l)
+        for (uint32_t j = 0; j < k; ++j) v += apply_signed(0, load_field(words, h.body_bit + (uint64_t)j * h.l, h.l), h.l);
+    }
+    out[i] = (T)v;
+  }
+}
+
+// ---- directory ---------------------------------------------------------------------
+template <typename T, int CODEC>
+__global__ void build_dir_kernel(const uint8_t *payload, const uint64_t *offsets, uint64_t nb, leco_dir_entry *dir) {
+  constexpr int S = sizeof(T);
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const BlockHdr h = parse_header<CODEC, S>(payload, __ldg(offsets + b));
+  leco_dir_entry e;
+  e.word0 = h.body_bit | ((uint64_t)h.l << 56) | ((uint64_t)CODEC << 48);
+  if (CODEC == kLinear || CODEC == kPoly2) {
+    e.a0 = h.a0; e.a1 = h.a1; e.a2 = h.a2;
+  } else {
+    e.a0 = __longlong_as_double((long long)h.base); e.a1 = 0; e.a2 = 0;
+  }
+  dir[b] = e;
+}
+
+// ---- launchers ------------------------------------------------------------------------
+
+#define LECO_DISPATCH(codec, s, FN, ...)                                   \
+  do {                                                                     \
+    if ((s) == 4) {                                                        \
+      switch (codec) {                                                     \
+        case kLinear: FN<uint32_t, kLinear>(__VA_ARGS__); return 0;         \
+        case kFor: FN<uint32_t, kFor>(__VA_ARGS__); return 0;               \
+        case kDelta: FN<uint32_t, kDelta>(__VA_ARGS__); return 0;           \
+        case kPoly2: FN<uint32_t, kPoly2>(__VA_ARGS__); return 0;           \
+      }                                                                    \
+    } else {                                                               \
+      switch (codec) {                                                     \
+        case kLinear: FN<uint64_t, kLinear>(__VA_ARGS__); return 0;         \
+        case kFor: FN<uint64_t, kFor>(__VA_ARGS__); return 0;               \
+        case kDelta: FN<uint64_t, kDelta>(__VA_ARGS__); return 0;           \
+        case kPoly2: FN<uint64_t, kPoly2>(__VA_ARGS__); return 0;           \
+      }                                                                    \
+    }                                                                      \
+    return -1;                                                             \
+  } while (0)
+
+template <typename T, int CODEC>
+static void run_decode(const DecodeLaunch &L, cudaStream_t st) {
+  if (!L.count) return;
+  const uint64_t b0 = L.first / L.bs, b1 = (L.first + L.count - 1) / L.bs;
+  decode_kernel<T, CODEC><<<(unsigned)(b1 - b0 + 1), 256, 0, st>>>(L);
+}
+int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st) { LECO_DISPATCH(codec, s, run_decode, L, st); }
+
+template <typename T, int CODEC>
+static void run_sum(const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st) {
+  const uint64_t nb = (L.n + L.bs - 1) / L.bs;
+  if (nb) sum_kernel<T, CODEC><<<(unsigned)nb, 256, 0, st>>>(L, d_sum);
+}
+int launch_sum(int codec, int s, const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st) {
+  LECO_DISPATCH(codec, s, run_sum, L, d_sum, st);
+}
+
+template <typename T, int CODEC>
+static void run_gather(const GatherLaunch &L, cudaStream_t st) {
+  if (!L.m) return;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t need = (L.m + 255) / 256;
+  const unsigned grid = (unsigned)umin64(need, (uint64_t)sms * 16);
+  gather_kernel<T, CODEC><<<grid, 256, 0, st>>>(L);
+}
+int launch_gather(int codec, int s, const GatherLaunch &L, cudaStream_t st) { LECO_DISPATCH(codec, s, run_gather, L, st); }
+
+template <typename T, int CODEC>
+static void run_dir(const uint8_t *payload, const uint64_t *offsets, uint64_t nb, leco_dir_entry *dir, cudaStream_t st) {
+  if (nb) build_dir_kernel<T, CODEC><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(payload, offsets, nb, dir);
+}
+int launch_build_dir(int codec, int s, const uint8_t *payload, const uint64_t *offsets, uint64_t n, uint32_t bs,
+                     leco_dir_entry *dir, uint32_t *error, cudaStream_t st) {
+  (void)error;
+  const uint64_t nb = (n + bs - 1) / bs;
+  LECO_DISPATCH(codec, s, run_dir, payload, offsets, nb, dir, st);
+}
+
+}  // namespace leco

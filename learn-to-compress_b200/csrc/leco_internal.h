@@ -1,0 +1,61 @@
+// leco_internal.h -- declarations shared by the library's translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/leco.h"
+
+namespace leco {
+
+struct EncodeLaunch {
+  const void *values;
+  uint64_t n;
+  uint32_t bs;
+  uint64_t nb;
+  uint8_t *payload;
+  uint64_t payload_cap;
+  uint64_t *offsets;
+  leco_dir_entry *dir;
+  double *seq_models;  // non-null: run the sequential reference fit first
+  double polyX[10];    // X sums (full block, tail block) for the degree-2 fit
+  uint64_t *status;
+  uint32_t *ticket;
+  uint32_t *error;
+};
+
+struct DecodeLaunch {
+  const uint8_t *payload;
+  const uint64_t *offsets;
+  uint64_t n;
+  uint32_t bs;
+  uint64_t first, count;
+  void *out;
+  uint32_t *error;
+};
+
+struct GatherLaunch {
+  const uint8_t *payload;
+  const uint64_t *offsets;
+  const leco_dir_entry *dir;
+  uint64_t n;
+  uint32_t bs;
+  const uint64_t *idx;
+  uint64_t m;
+  void *out;
+  uint32_t *error;
+};
+
+int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st);
+int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st);
+int launch_gather(int codec, int s, const GatherLaunch &L, cudaStream_t st);
+int launch_sum(int codec, int s, const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st);
+int launch_build_dir(int codec, int s, const uint8_t *payload, const uint64_t *offsets, uint64_t n, uint32_t bs,
+                     leco_dir_entry *dir, uint32_t *error, cudaStream_t st);
+
+// Reference X sums of polynomial_regression_iter: X[k] = sum_{j<N} j^k as a
+// sequential FP64 loop (polynomial_regression_internals.hpp:111-116), x^k built
+// by repeated multiplication (:80-99).  Host code, compiled with
+// -ffp-contract=off.
+void poly2_x_sums(uint32_t N, double X[5]);
+
+}  // namespace leco

@@ -1,0 +1,250 @@
+"""Test infrastructure only: ctypes bindings for the oracle libraries.
+
+* ``Oracle`` -- the plain-C restatement ``oracle/leco_oracle.c``
+  (``oracle/_build/liboracle.so``).
+* ``Reference`` -- the unmodified reference codec headers compiled by
+  ``oracle/Makefile`` into ``oracle/_ref/libleco_ref.so`` (present only when it
+  was built where the reference sources exist; the built file travels with the
+  repository snapshot).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs use this
+module; the product never imports it.
+
+Codec ids follow the product's C ABI: 0 LeCo linear, 1 FOR, 2 Delta, 3 LeCo
+degree-2 polynomial.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libleco_ref.so")
+
+LECO, FOR, DELTA, POLY2 = 0, 1, 2, 3
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+
+
+def build(force: bool = False) -> None:
+    """Compiles the oracle libraries with oracle/Makefile (gcc only)."""
+    if force or not os.path.exists(ORACLE_SO):
+        subprocess.check_call(["make", "-s", "-C", HERE, "_build/liboracle.so"])
+    if os.path.isdir("/root/reference/headers"):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _dtype(s: int):
+    return np.uint64 if s == 8 else np.uint32
+
+
+def worst_case_bytes(n: int, s: int, bs: int) -> int:
+    nb = (n + bs - 1) // bs
+    return n * s + nb * 64 + 64
+
+
+class Oracle:
+    """The plain-C restatement of the reference algorithm."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        self.L = L
+        for name in ("oracle_leco_encode", "oracle_for_encode", "oracle_delta_encode", "oracle_poly2_encode"):
+            getattr(L, name).restype = _SZ
+            getattr(L, name).argtypes = [_P, ctypes.c_int, _SZ, _P]
+        for name in ("oracle_leco_decode", "oracle_for_decode", "oracle_delta_decode", "oracle_poly2_decode"):
+            getattr(L, name).restype = _SZ
+            getattr(L, name).argtypes = [_P, ctypes.c_int, _SZ, _P, ctypes.c_int]
+        for name in ("oracle_leco_random", "oracle_for_random", "oracle_delta_random", "oracle_poly2_random"):
+            getattr(L, name).restype = ctypes.c_uint64
+            getattr(L, name).argtypes = [_P, ctypes.c_int, ctypes.c_int]
+        L.oracle_column_encode.restype = _SZ
+        L.oracle_column_encode.argtypes = [ctypes.c_int, _P, ctypes.c_int, _SZ, ctypes.c_uint32, _P, _P]
+        L.oracle_column_decode.restype = None
+        L.oracle_column_decode.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, _P]
+        L.oracle_column_random.restype = None
+        L.oracle_column_random.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, _P, _SZ, _P]
+        L.oracle_column_sum.restype = ctypes.c_uint64
+        L.oracle_column_sum.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, _P]
+        L.oracle_varseg_encode.restype = _SZ
+        L.oracle_varseg_encode.argtypes = [_P, ctypes.c_uint32, ctypes.c_uint32, _P]
+        L.oracle_varseg_decode.restype = _SZ
+        L.oracle_varseg_decode.argtypes = [_P, _SZ, _P]
+        L.oracle_varseg_random.restype = ctypes.c_uint64
+        L.oracle_varseg_random.argtypes = [_P, ctypes.c_uint64]
+        L.oracle_lr_fit.restype = None
+        L.oracle_lr_fit.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, _P]
+        L.oracle_poly2_fit.restype = None
+        L.oracle_poly2_fit.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
+
+    _ENC = ("oracle_leco_encode", "oracle_for_encode", "oracle_delta_encode", "oracle_poly2_encode")
+    _DEC = ("oracle_leco_decode", "oracle_for_decode", "oracle_delta_decode", "oracle_poly2_decode")
+    _RA = ("oracle_leco_random", "oracle_for_random", "oracle_delta_random", "oracle_poly2_random")
+
+    # -- one block --------------------------------------------------------
+    def encode_block(self, codec: int, data: np.ndarray) -> bytes:
+        data = np.ascontiguousarray(data)
+        s = data.dtype.itemsize
+        out = np.zeros(len(data) * s + 128, np.uint8)
+        nbytes = getattr(self.L, self._ENC[codec])(_ptr(data), s, len(data), _ptr(out))
+        return out[:nbytes].tobytes()
+
+    def decode_block(self, codec: int, block: bytes, n: int, s: int, strict_raw: int = 1) -> np.ndarray:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(max(n, 2), _dtype(s))
+        getattr(self.L, self._DEC[codec])(_ptr(buf), s, n, _ptr(out), strict_raw)
+        return out[:n]
+
+    def random_block(self, codec: int, block: bytes, k: int, s: int) -> int:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        return int(getattr(self.L, self._RA[codec])(_ptr(buf), s, k))
+
+    def lr_fit(self, data: np.ndarray):
+        t = np.zeros(2, np.float64)
+        self.L.oracle_lr_fit(_ptr(data), data.dtype.itemsize, len(data), _ptr(t[:1]), _P(t.ctypes.data + 8))
+        return float(t[0]), float(t[1])
+
+    def poly2_fit(self, data: np.ndarray):
+        a = np.zeros(3, np.float64)
+        self.L.oracle_poly2_fit(_ptr(data), data.dtype.itemsize, len(data), _ptr(a))
+        return a
+
+    # -- whole column -----------------------------------------------------
+    def encode_column(self, codec: int, data: np.ndarray, bs: int):
+        data = np.ascontiguousarray(data)
+        s, n = data.dtype.itemsize, len(data)
+        nb = (n + bs - 1) // bs
+        out = np.zeros(worst_case_bytes(n, s, bs), np.uint8)
+        off = np.zeros(nb + 1, np.uint64)
+        total = self.L.oracle_column_encode(codec, _ptr(data), s, n, bs, _ptr(out), _ptr(off))
+        return out[:total].copy(), off
+
+    def decode_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int):
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        out = np.zeros(n, _dtype(s))
+        self.L.oracle_column_decode(codec, _ptr(pay), _ptr(offsets), s, n, bs, _ptr(out))
+        return out
+
+    def random_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, s: int, bs: int, idx: np.ndarray):
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        idx = np.ascontiguousarray(idx, np.uint64)
+        out = np.zeros(len(idx), _dtype(s))
+        self.L.oracle_column_random(codec, _ptr(pay), _ptr(offsets), s, bs, _ptr(idx), len(idx), _ptr(out))
+        return out
+
+    # -- variable-length segments ----------------------------------------
+    def varseg_encode(self, array: np.ndarray, start: int, end: int) -> bytes:
+        out = np.zeros((end - start + 1) * 8 + 64, np.uint8)
+        nbytes = self.L.oracle_varseg_encode(_ptr(array), start, end, _ptr(out))
+        return out[:nbytes].tobytes()
+
+    def varseg_decode(self, seg: bytes, length: int) -> np.ndarray:
+        buf = np.frombuffer(seg + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(max(length, 2), np.uint64)
+        self.L.oracle_varseg_decode(_ptr(buf), length, _ptr(out))
+        return out[:length]
+
+    def varseg_random(self, seg: bytes, g: int) -> int:
+        buf = np.frombuffer(seg + b"\0" * 32, np.uint8).copy()
+        return int(self.L.oracle_varseg_random(_ptr(buf), g))
+
+
+class Reference:
+    """The reference's own codec classes (compiled headers), via ref_wrap.cpp."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(path)
+        self.L = L
+        for t, ct in (("u32", ctypes.c_uint32), ("u64", ctypes.c_uint64)):
+            f = getattr(L, f"ref_encode_block_{t}"); f.restype = _SZ; f.argtypes = [ctypes.c_int, _P, _SZ, _P]
+            f = getattr(L, f"ref_decode_block_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _SZ, _P]
+            f = getattr(L, f"ref_random_{t}"); f.restype = ct; f.argtypes = [ctypes.c_int, _P, ctypes.c_int]
+            f = getattr(L, f"ref_column_encode_{t}"); f.restype = _SZ; f.argtypes = [ctypes.c_int, _P, _SZ, ctypes.c_uint32, _P, _P]
+            f = getattr(L, f"ref_column_decode_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _P, _SZ, ctypes.c_uint32, _P, ctypes.c_int]
+            f = getattr(L, f"ref_column_random_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _P, ctypes.c_uint32, _P, _SZ, _P, ctypes.c_int]
+        L.ref_varlen_encode_u64.restype = _P
+        L.ref_varlen_encode_u64.argtypes = [_P, _SZ, ctypes.c_int, ctypes.c_int64]
+        L.ref_varlen_segments.restype = _SZ
+        L.ref_varlen_segments.argtypes = [_P]
+        L.ref_varlen_export.restype = _SZ
+        L.ref_varlen_export.argtypes = [_P, _P, _P, _P]
+        L.ref_varlen_decode.restype = None
+        L.ref_varlen_decode.argtypes = [_P, _SZ, _P]
+        L.ref_varlen_random.restype = None
+        L.ref_varlen_random.argtypes = [_P, _P, _SZ, _P]
+        L.ref_varlen_free.restype = None
+        L.ref_varlen_free.argtypes = [_P]
+
+    @staticmethod
+    def _t(s):
+        return "u64" if s == 8 else "u32"
+
+    def encode_block(self, codec: int, data: np.ndarray) -> bytes:
+        data = np.ascontiguousarray(data)
+        s = data.dtype.itemsize
+        out = np.zeros(len(data) * s * 4 + 128, np.uint8)
+        nbytes = getattr(self.L, f"ref_encode_block_{self._t(s)}")(codec, _ptr(data), len(data), _ptr(out))
+        return out[:nbytes].tobytes()
+
+    def decode_block(self, codec: int, block: bytes, n: int, s: int) -> np.ndarray:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(max(n, 2) + 64, _dtype(s))
+        getattr(self.L, f"ref_decode_block_{self._t(s)}")(codec, _ptr(buf), n, _ptr(out))
+        return out[:n]
+
+    def random_block(self, codec: int, block: bytes, k: int, s: int) -> int:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        return int(getattr(self.L, f"ref_random_{self._t(s)}")(codec, _ptr(buf), k))
+
+    def encode_column(self, codec: int, data: np.ndarray, bs: int):
+        data = np.ascontiguousarray(data)
+        s, n = data.dtype.itemsize, len(data)
+        nb = (n + bs - 1) // bs
+        out = np.zeros(worst_case_bytes(n, s, bs) + n * s, np.uint8)
+        off = np.zeros(nb + 1, np.uint64)
+        total = getattr(self.L, f"ref_column_encode_{self._t(s)}")(codec, _ptr(data), n, bs, _ptr(out), _ptr(off))
+        return out[:total].copy(), off
+
+    def decode_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int, threads: int = 1):
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        out = np.zeros(n + 64, _dtype(s))
+        getattr(self.L, f"ref_column_decode_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), n, bs, _ptr(out), threads)
+        return out[:n]
+
+    def random_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, s: int, bs: int, idx: np.ndarray, threads: int = 1):
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        idx = np.ascontiguousarray(idx, np.uint64)
+        out = np.zeros(len(idx), _dtype(s))
+        getattr(self.L, f"ref_column_random_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), bs, _ptr(idx), len(idx), _ptr(out), threads)
+        return out
+
+    # -- variable-length (u64) ---------------------------------------------
+    def varlen_encode(self, data: np.ndarray, blocks: int, delta: int):
+        """Runs the reference partitioner + segment writer; returns
+        (starts[u32], byte_offsets[u64, ns+1], payload[u8])."""
+        data = np.ascontiguousarray(data, np.uint64)
+        h = self.L.ref_varlen_encode_u64(_ptr(data), len(data), blocks, delta)
+        try:
+            ns = self.L.ref_varlen_segments(h)
+            starts = np.zeros(ns, np.uint32)
+            off = np.zeros(ns + 1, np.uint64)
+            total = self.L.ref_varlen_export(h, None, None, None)
+            pay = np.zeros(total + 64, np.uint8)
+            self.L.ref_varlen_export(h, _ptr(starts), _ptr(off), _ptr(pay))
+            dec = np.zeros(len(data) + 64, np.uint64)
+            self.L.ref_varlen_decode(h, len(data), _ptr(dec))
+        finally:
+            self.L.ref_varlen_free(h)
+        return starts, off, pay[:total].copy(), dec[: len(data)]

@@ -1,0 +1,183 @@
+// Test infrastructure only: a C-ABI wrapper around the UNMODIFIED reference codec
+// headers (yhliu918/Learn-to-Compress, headers/*_integer_template.h), compiled
+// from where they lie by oracle/Makefile into oracle/_ref/libleco_ref.so.  It is
+// the checker that pins the plain-C restatement (oracle/leco_oracle.c) and the
+// reference arm of bench.py; nothing in the product links it.
+//
+// Every function forwards to the reference class method named in its comment and
+// adds only the per-block loop of the reference drivers
+// (experiments/leco_int_fix_template.cpp:108-127 encode, :142-153 decode,
+// :189-207 random access).
+#include "piecewise_fix_integer_template.h"
+#include "FOR_integer_template.h"
+#include "delta_integer_template.h"
+#include "poly_fix_integer_template.h"
+#include "piecewise_cost_merge_integer_template_double_wo_round.h"
+
+#include <atomic>
+#include <thread>
+#include <vector>
+
+using namespace Codecset;
+
+namespace {
+
+enum { C_LECO = 0, C_FOR = 1, C_DELTA = 2, C_POLY2 = 3 };
+
+template <typename T>
+size_t enc_block(int codec, const T *data, size_t len, uint8_t *out, size_t block_id) {
+  uint8_t *end = out;
+  switch (codec) {
+    case C_LECO: { Leco_int<T> c; end = c.encodeArray8_int(data, len, out, block_id); break; }
+    case C_FOR: { FOR_int<T> c; end = c.encodeArray8_int(data, len, out, block_id); break; }
+    case C_DELTA: { Delta_int<T> c; end = c.encodeArray8_int(const_cast<T *>(data), len, out, block_id); break; }
+    case C_POLY2: { Leco_int_poly<T, 2> c; end = c.encodeArray8_int(data, len, out, block_id); break; }
+    default: return 0;
+  }
+  return (size_t)(end - out);
+}
+
+template <typename T>
+void dec_block(int codec, const uint8_t *in, size_t len, T *out, size_t block_id) {
+  switch (codec) {
+    case C_LECO: { Leco_int<T> c; c.decodeArray8(in, len, out, block_id); break; }
+    case C_FOR: { FOR_int<T> c; c.decodeArray8(in, len, out, block_id); break; }
+    case C_DELTA: { Delta_int<T> c; c.decodeArray8(const_cast<uint8_t *>(in), len, out, block_id); break; }
+    case C_POLY2: { Leco_int_poly<T, 2> c; c.decodeArray8(in, len, out, block_id); break; }
+    default: break;
+  }
+}
+
+template <typename T>
+T ra_block(int codec, const uint8_t *in, int k) {
+  switch (codec) {
+    case C_LECO: { Leco_int<T> c; return c.randomdecodeArray8(in, k, nullptr, 0); }
+    case C_FOR: { FOR_int<T> c; return c.randomdecodeArray8(in, k, nullptr, 0); }
+    case C_DELTA: { Delta_int<T> c; return c.randomdecodeArray8(const_cast<uint8_t *>(in), k, nullptr, 0); }
+    case C_POLY2: { Leco_int_poly<T, 2> c; return c.randomdecodeArray8(in, k, nullptr, 0); }
+    default: return 0;
+  }
+}
+
+// Runs fn(lo, hi) over [0, n) split into `threads` contiguous ranges.
+template <typename F>
+void parallel_ranges(size_t n, int threads, F fn) {
+  if (threads <= 1 || n < 2) { fn((size_t)0, n); return; }
+  std::vector<std::thread> pool;
+  size_t per = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    size_t lo = (size_t)t * per, hi = std::min(n, lo + per);
+    if (lo >= hi) break;
+    pool.emplace_back([=] { fn(lo, hi); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+template <typename T>
+size_t col_encode(int codec, const T *data, size_t n, uint32_t bs, uint8_t *out, uint64_t *offsets) {
+  size_t nb = (n + bs - 1) / bs, pos = 0;
+  for (size_t b = 0; b < nb; ++b) {
+    size_t len = std::min<size_t>(bs, n - b * bs);
+    offsets[b] = pos;
+    pos += enc_block<T>(codec, data + b * bs, len, out + pos, b);
+  }
+  offsets[nb] = pos;
+  return pos;
+}
+
+template <typename T>
+void col_decode(int codec, const uint8_t *payload, const uint64_t *offsets, size_t n, uint32_t bs, T *out, int threads) {
+  size_t nb = (n + bs - 1) / bs;
+  parallel_ranges(nb, threads, [&](size_t lo, size_t hi) {
+    for (size_t b = lo; b < hi; ++b) {
+      size_t len = std::min<size_t>(bs, n - b * bs);
+      dec_block<T>(codec, payload + offsets[b], len, out + b * bs, b);
+    }
+  });
+}
+
+template <typename T>
+void col_random(int codec, const uint8_t *payload, const uint64_t *offsets, uint32_t bs, const uint64_t *idx, size_t m, T *out, int threads) {
+  parallel_ranges(m, threads, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) {
+      uint64_t g = idx[i];
+      out[i] = ra_block<T>(codec, payload + offsets[g / bs], (int)(g % bs));
+    }
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+// One block through <Codec>::encodeArray8_int; returns the bytes written.
+size_t ref_encode_block_u32(int codec, const uint32_t *d, size_t len, uint8_t *out) { return enc_block<uint32_t>(codec, d, len, out, 0); }
+size_t ref_encode_block_u64(int codec, const uint64_t *d, size_t len, uint8_t *out) { return enc_block<uint64_t>(codec, d, len, out, 0); }
+// One block through <Codec>::decodeArray8.
+void ref_decode_block_u32(int codec, const uint8_t *in, size_t len, uint32_t *out) { dec_block<uint32_t>(codec, in, len, out, 0); }
+void ref_decode_block_u64(int codec, const uint8_t *in, size_t len, uint64_t *out) { dec_block<uint64_t>(codec, in, len, out, 0); }
+// One value through <Codec>::randomdecodeArray8.
+uint32_t ref_random_u32(int codec, const uint8_t *in, int k) { return ra_block<uint32_t>(codec, in, k); }
+uint64_t ref_random_u64(int codec, const uint8_t *in, int k) { return ra_block<uint64_t>(codec, in, k); }
+
+// Whole column, blocks of `bs` values, concatenated block images + byte offsets[nb+1].
+size_t ref_column_encode_u32(int codec, const uint32_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off) { return col_encode<uint32_t>(codec, d, n, bs, out, off); }
+size_t ref_column_encode_u64(int codec, const uint64_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off) { return col_encode<uint64_t>(codec, d, n, bs, out, off); }
+void ref_column_decode_u32(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint32_t *out, int threads) { col_decode<uint32_t>(codec, p, off, n, bs, out, threads); }
+void ref_column_decode_u64(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint64_t *out, int threads) { col_decode<uint64_t>(codec, p, off, n, bs, out, threads); }
+void ref_column_random_u32(int codec, const uint8_t *p, const uint64_t *off, uint32_t bs, const uint64_t *idx, size_t m, uint32_t *out, int threads) { col_random<uint32_t>(codec, p, off, bs, idx, m, out, threads); }
+void ref_column_random_u64(int codec, const uint8_t *p, const uint64_t *off, uint32_t bs, const uint64_t *idx, size_t m, uint64_t *out, int threads) { col_random<uint64_t>(codec, p, off, bs, idx, m, out, threads); }
+
+// ---- Variable-length cost-merge codec, u64 (Leco_cost_merge_double_wo_round) ----
+// Drives the class the way experiments/leco_double_int_template_wo_round.cpp does:
+// init(blocks, block_size, delta), encodeArray8_int per coarse block over the whole
+// array, then hands out the segment images.  The handle owns the codec object.
+void *ref_varlen_encode_u64(const uint64_t *d, size_t n, int blocks, int64_t delta) {
+  auto *c = new Leco_cost_merge_double_wo_round<uint64_t>();
+  int block_size = (int)(n / (size_t)blocks);
+  int nb = (int)(n / (size_t)block_size);
+  if ((size_t)nb * block_size < n) nb++;
+  c->init(nb, block_size, (uint64_t)delta);
+  std::vector<uint8_t> scratch(n * sizeof(uint64_t) * 4 + 64);
+  for (int i = 0; i < nb; ++i) {
+    size_t len = (size_t)block_size;
+    if (i == nb - 1) len = n - (size_t)(nb - 1) * block_size;
+    c->encodeArray8_int(const_cast<uint64_t *>(d), len, scratch.data(), (size_t)i);
+  }
+  return c;
+}
+size_t ref_varlen_segments(void *h) { return ((Leco_cost_merge_double_wo_round<uint64_t> *)h)->block_start_vec_total.size(); }
+// Copies segment starts (value index), byte sizes and the concatenated images.
+size_t ref_varlen_export(void *h, uint32_t *starts, uint64_t *byte_off, uint8_t *payload) {
+  auto *c = (Leco_cost_merge_double_wo_round<uint64_t> *)h;
+  size_t ns = c->block_start_vec_total.size(), pos = 0;
+  for (size_t i = 0; i < ns; ++i) {
+    if (starts) starts[i] = c->segment_index_total[i];
+    if (byte_off) byte_off[i] = pos;
+    if (payload) memcpy(payload + pos, c->block_start_vec_total[i], c->segment_length_total[i]);
+    pos += c->segment_length_total[i];
+  }
+  if (byte_off) byte_off[ns] = pos;
+  return pos;
+}
+// Leco_cost_merge_double_wo_round::decodeArray8 over all segments.
+void ref_varlen_decode(void *h, size_t n, uint64_t *out) {
+  auto *c = (Leco_cost_merge_double_wo_round<uint64_t> *)h;
+  c->decodeArray8(n, out, n);
+  c->segment_index_total.pop_back();  // decodeArray8 appends n; undo so the handle stays reusable
+}
+// get_segment_id (ALEX upper_bound) + randomdecodeArray8 for each index.
+void ref_varlen_random(void *h, const uint64_t *idx, size_t m, uint64_t *out) {
+  auto *c = (Leco_cost_merge_double_wo_round<uint64_t> *)h;
+  for (size_t i = 0; i < m; ++i) {
+    int sid = c->get_segment_id((int)idx[i]);
+    out[i] = c->randomdecodeArray8(sid, c->block_start_vec_total[sid], (int)idx[i], nullptr, 0);
+  }
+}
+void ref_varlen_free(void *h) {
+  auto *c = (Leco_cost_merge_double_wo_round<uint64_t> *)h;
+  for (auto *p : c->block_start_vec_total) free(p);
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,2 @@
+/* Empty stand-in: the LeCo integer hot path does not use this library. */
+#pragma once
