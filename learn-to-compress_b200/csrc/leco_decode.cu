@@ -116,6 +116,72 @@ __device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restri
 
 template <typename T>
 __device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v, int cnt, bool full);
+template <>
+__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
+  if (full) __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
+}
+template <>
+__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
+  if (full) __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
+}
+
+
+// True when every prediction of the block is a finite double inside
+// (-2^63, 2^63), so the x86 out-of-range rule of f2i_x86 can never apply:
+// |a0| + |a1|*(len-1) + |a2|*(len-1)^2 < 2^62 bounds them (rounding moves a
+// prediction by a few ulps only).  NaN/inf models fail the comparison.
+template <int CODEC>
+__device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
+  const double L = __uint2double_rn(len ? len - 1 : 0);
+  double b = fabs(h.a0) + fabs(h.a1) * L;
+  if (CODEC == kPoly2) b += fabs(h.a2) * L * L;
+  return b < 4611686018427387904.0;
+}
+
+// Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
+// (raw u32 blocks included).  Each thread produces VEC consecutive values per
+// step and writes them with one 16-byte store.
+template <typename T, int CODEC, bool FAST>
+__device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint8_t *__restrict__ payload, T *out,
+                                              uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
+  constexpr int S = sizeof(T);
+  constexpr int VEC = 16 / S;
+  const uint32_t l = raw ? 32u : h.l;
+  const uint32_t *bp = reinterpret_cast<const uint32_t *>(payload) + (h.body_bit >> 5);
+  const uint32_t bsh = (uint32_t)(h.body_bit & 31);
+  const uint32_t mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
+  const uint32_t sb = l ? l - 1 : 0, m1 = mask >> 1;
+  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
+    uint64_t v[VEC];
+#pragma unroll
+    for (int j = 0; j < VEC; ++j) {
+      const int32_t k = kv + j;
+      const uint32_t kk = k < (int32_t)lo ? lo : (uint32_t)k;  // values before lo are not stored
+      const uint32_t r = bsh + kk * l;
+      const uint32_t *p = bp + (r >> 5);
+      const uint32_t f = l ? (__funnelshift_r(__ldg(p), __ldg(p + 1), r) & mask) : 0u;
+      if (raw) {
+        v[j] = f;
+      } else if (CODEC == kFor) {
+        v[j] = h.base + f;
+      } else {
+        const double pd = CODEC == kLinear ? pred_linear(h.a0, h.a1, kk)
+                                           : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
+        const int64_t pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
+        const uint32_t mag = f & m1;
+        const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
+        v[j] = (uint64_t)(pred + d);
+      }
+    }
+    const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
+    store_vals<T>(out, obase + kv, v, VEC, full);
+    if (!full) {
+#pragma unroll
+      for (int j = 0; j < VEC; ++j)
+        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
+    }
+  }
+}
 
 // ---- bulk / range decode ----------------------------------------------------
 // One CTA per block.  Each thread decodes VEC = 16/sizeof(T) consecutive values
@@ -165,32 +231,36 @@ __global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
     return;
   }
 
-  const uint32_t l = raw ? TB : h.l;
   // First vector start so that out[obase + kv] is 16-byte aligned (out must be
   // sizeof(T)-aligned); kv may start up to VEC-1 values before lo.
   const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + obase + lo);
   const int32_t kstart = (int32_t)lo - (int32_t)((oaddr & 15) / S);
+  const uint32_t l = raw ? TB : h.l;
+  if (l <= 32) {
+    // Narrow fields (every u32 block, u64 blocks with l <= 32): 32-bit field
+    // extraction; predictions converted without range checks when the block's
+    // model keeps every prediction inside int64 (decided once per block).
+    const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
+    if (fast) decode_narrow<T, CODEC, true>(h, raw, a.payload, out, obase, lo, hi, kstart);
+    else decode_narrow<T, CODEC, false>(h, raw, a.payload, out, obase, lo, hi, kstart);
+    return;
+  }
   for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
     uint64_t v[VEC];
     const uint32_t kw = kv < (int32_t)lo ? lo : (uint32_t)kv;  // first value actually needed
-    if (l) {
-      const uint64_t bit0 = h.body_bit + (uint64_t)kw * l;
-      const uint64_t w = bit0 >> 6;
-      const uint64_t W0 = __ldg(words + w), W1 = __ldg(words + w + 1), W2 = __ldg(words + w + 2);
-      const uint32_t sh0 = (uint32_t)(bit0 & 63);
+    const uint64_t bit0 = h.body_bit + (uint64_t)kw * l;
+    const uint64_t w = bit0 >> 6;
+    const uint64_t W0 = __ldg(words + w), W1 = __ldg(words + w + 1), W2 = __ldg(words + w + 2);
+    const uint32_t sh0 = (uint32_t)(bit0 & 63);
 #pragma unroll
-      for (int j = 0; j < VEC; ++j) {
-        const int32_t k = kv + j;
-        const uint32_t rel = sh0 + (uint32_t)(k - (int32_t)kw) * l;  // unused when k < kw
-        const uint32_t sh = rel & 63;
-        const uint64_t lo64 = rel < 64 ? W0 : (rel < 128 ? W1 : W2);
-        const uint64_t hi64 = rel < 64 ? W1 : W2;
-        const uint64_t f = funnel64(lo64, hi64, sh) & lowmask(l);
-        v[j] = raw ? f : value_from_field<CODEC, S>(h, (uint32_t)k, f);
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < VEC; ++j) v[j] = value_from_field<CODEC, S>(h, (uint32_t)(kv + j), 0);
+    for (int j = 0; j < VEC; ++j) {
+      const int32_t k = kv + j;
+      const uint32_t rel = sh0 + (uint32_t)(k - (int32_t)kw) * l;  // unused when k < kw
+      const uint32_t sh = rel & 63;
+      const uint64_t lo64 = rel < 64 ? W0 : (rel < 128 ? W1 : W2);
+      const uint64_t hi64 = rel < 64 ? W1 : W2;
+      const uint64_t f = funnel64(lo64, hi64, sh) & lowmask(l);
+      v[j] = raw ? f : value_from_field<CODEC, S>(h, (uint32_t)k, f);
     }
     const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
     store_vals<T>(out, obase + kv, v, VEC, full);
@@ -200,15 +270,6 @@ __global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
         if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
     }
   }
-}
-
-template <>
-__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
-}
-template <>
-__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
 }
 
 // ---- compressed-domain sum ----------------------------------------------------
