@@ -16,6 +16,8 @@
 #include "leco_device.cuh"
 #include "leco_internal.h"
 
+#include <cstdlib>
+
 namespace leco {
 
 // Block model parsed from a header (or a directory entry).
@@ -141,13 +143,14 @@ __device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
 // Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
 // (raw u32 blocks included).  Each thread produces VEC consecutive values per
 // step and writes them with one 16-byte store.
-template <typename T, int CODEC, bool FAST>
-__device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint8_t *__restrict__ payload, T *out,
+template <typename T, int CODEC, bool FAST, bool SMEM = false>
+__device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32, T *out,
                                               uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
   constexpr int S = sizeof(T);
   constexpr int VEC = 16 / S;
   const uint32_t l = raw ? 32u : h.l;
-  const uint32_t *bp = reinterpret_cast<const uint32_t *>(payload) + (h.body_bit >> 5);
+  // words32 + body_bit/32: the body's first word (global payload or a staged copy in shared memory)
+  const uint32_t *bp = words32 + (h.body_bit >> 5);
   const uint32_t bsh = (uint32_t)(h.body_bit & 31);
   const uint32_t mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
   const uint32_t sb = l ? l - 1 : 0, m1 = mask >> 1;
@@ -159,7 +162,8 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
       const uint32_t kk = k < (int32_t)lo ? lo : (uint32_t)k;  // values before lo are not stored
       const uint32_t r = bsh + kk * l;
       const uint32_t *p = bp + (r >> 5);
-      const uint32_t f = l ? (__funnelshift_r(__ldg(p), __ldg(p + 1), r) & mask) : 0u;
+      const uint32_t w0 = SMEM ? p[0] : __ldg(p), w1 = SMEM ? p[1] : __ldg(p + 1);
+      const uint32_t f = l ? (__funnelshift_r(w0, w1, r) & mask) : 0u;
       if (raw) {
         v[j] = f;
       } else if (CODEC == kFor) {
@@ -188,12 +192,10 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
 // per step from a three-word window of the packed body and writes them with one
 // 16-byte store.
 template <typename T, int CODEC>
-__global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
+__device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) {
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   constexpr int VEC = 16 / S;
-  const uint64_t bfirst = a.first / a.bs;
-  const uint64_t b = bfirst + blockIdx.x;
   const uint64_t base = b * a.bs;
   const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
   // values of this block inside [first, first+count)
@@ -241,8 +243,9 @@ __global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
     // extraction; predictions converted without range checks when the block's
     // model keeps every prediction inside int64 (decided once per block).
     const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
-    if (fast) decode_narrow<T, CODEC, true>(h, raw, a.payload, out, obase, lo, hi, kstart);
-    else decode_narrow<T, CODEC, false>(h, raw, a.payload, out, obase, lo, hi, kstart);
+    const uint32_t *w32 = reinterpret_cast<const uint32_t *>(a.payload);
+    if (fast) decode_narrow<T, CODEC, true>(h, raw, w32, out, obase, lo, hi, kstart);
+    else decode_narrow<T, CODEC, false>(h, raw, w32, out, obase, lo, hi, kstart);
     return;
   }
   for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
@@ -269,6 +272,152 @@ __global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
       for (int j = 0; j < VEC; ++j)
         if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
     }
+  }
+}
+
+// Direct decode: one CTA per block of the range, everything read from global memory.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
+  decode_block<T, CODEC>(a, a.first / a.bs + blockIdx.x);
+}
+
+// ---- TMA-staged persistent decode --------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t tx) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(tx) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bulk (non-tensor) TMA copy global -> this CTA's shared memory, completion
+// counted on `bar`.  dst/src 16-byte aligned, bytes a multiple of 16.  No
+// multicast: the source is always this GPU's own payload.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Bounded wait on a staging barrier (about a second at most).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t spins = 0; spins < (1u << 24); ++spins)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+struct StageMeta {
+  uint64_t gbase;   // 16-byte aligned global byte address of the staged copy
+  uint32_t hoff;    // block header offset inside the staged copy
+  uint32_t direct;  // 1: block too large for the buffer, decode from global
+};
+
+// Persistent decode of a whole column.  Each CTA walks blocks blockIdx.x,
+// blockIdx.x + gridDim.x, ...; thread 0 stages the next block's image (header +
+// packed body) into the other half of a double buffer with one cp.async.bulk
+// while the CTA decodes the current one out of shared memory.  Blocks that do
+// not fit the buffer, wide (l > 32) and Delta blocks take the direct path.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint32_t bufcap) {
+  constexpr int S = sizeof(T);
+  extern __shared__ __align__(128) uint8_t stage[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ StageMeta meta[2];
+  const uint32_t tid = threadIdx.x;
+  const uint64_t nblk = (a.n + a.bs - 1) / a.bs;
+  uint8_t *buf0 = stage, *buf1 = stage + bufcap;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](uint64_t b, int which) {  // thread 0 only
+    const uint64_t o0 = __ldg(a.offsets + b), o1 = __ldg(a.offsets + b + 1);
+    const uint64_t g0 = o0 & ~15ull, g1 = (o1 + 8 + 15) & ~15ull;  // +8: the field reads touch one word past the body
+    const uint64_t bytes = g1 - g0;
+    StageMeta m;
+    m.gbase = g0;
+    m.hoff = (uint32_t)(o0 - g0);
+    m.direct = bytes > bufcap;
+    meta[which] = m;
+    if (!m.direct) {
+      mbar_arrive_tx(&bar[which], (uint32_t)bytes);
+      bulk_g2s(which ? buf1 : buf0, a.payload + g0, (uint32_t)bytes, &bar[which]);
+    } else {
+      mbar_arrive(&bar[which]);
+    }
+  };
+  uint64_t blk = blockIdx.x;
+  if (tid == 0 && blk < nblk) issue(blk, 0);
+  uint32_t ph0 = 0, ph1 = 0;
+  T *out = reinterpret_cast<T *>(a.out);
+  for (int it = 0; blk < nblk; blk += gridDim.x, ++it) {
+    const int cur = it & 1;
+    const bool has_next = blk + gridDim.x < nblk;
+    if (tid == 0 && has_next) issue(blk + gridDim.x, cur ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
+    if (cur) ph1 ^= 1; else ph0 ^= 1;
+    if (!ok) {
+      if (tid == 0) {
+        atomicOr(a.error, kErrTimeout);
+        if (has_next) mbar_wait_bounded(&bar[cur ^ 1], cur ? ph0 : ph1);  // let our own copy in flight land
+      }
+      return;
+    }
+    const StageMeta m = meta[cur];
+    const uint8_t *sb = (cur ? buf1 : buf0);
+    const uint32_t l = sb[m.hoff];
+    const uint64_t base = blk * a.bs;
+    const uint32_t len = (uint32_t)umin64(a.bs, a.n - base);
+    const bool raw = l == 8u * S;
+    const bool narrow = (CODEC != kDelta) && (l <= 32) && (!raw || S == 4);
+    if (m.direct || !narrow) {
+      decode_block<T, CODEC>(a, blk);
+    } else {
+      BlockHdr h;
+      h.l = l;
+      h.a0 = h.a1 = h.a2 = 0;
+      h.base = 0;
+      const uint8_t *hb = sb + m.hoff + 1;
+      if (!raw) {
+        uint64_t w[3] = {0, 0, 0};
+        const int nw = CODEC == kPoly2 ? 3 : (CODEC == kLinear ? 2 : 1);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          if (q < nw)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) w[q] |= (uint64_t)hb[8 * q + j] << (8 * j);
+        if (CODEC == kLinear || CODEC == kPoly2) {
+          h.a0 = __longlong_as_double((long long)w[0]);
+          h.a1 = __longlong_as_double((long long)w[1]);
+          h.a2 = __longlong_as_double((long long)w[2]);
+        } else {
+          h.base = S == 8 ? w[0] : (w[0] & 0xffffffffull);
+        }
+      }
+      h.body_bit = (uint64_t)(m.hoff + (raw ? 1u : Hdr<CODEC, S>::bytes)) * 8;
+      const uint32_t *w32 = reinterpret_cast<const uint32_t *>(sb);
+      const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + base);
+      const int32_t kstart = -(int32_t)((oaddr & 15) / S);
+      const bool fast = (CODEC == kFor) || raw || pred_in_range<CODEC>(h, len);
+      if (fast) decode_narrow<T, CODEC, true, true>(h, raw, w32, out, base, 0, len, kstart);
+      else decode_narrow<T, CODEC, false, true>(h, raw, w32, out, base, 0, len, kstart);
+    }
+    __syncthreads();  // everyone is done with this buffer before it is refilled
   }
 }
 
@@ -377,6 +526,16 @@ __global__ void build_dir_kernel(const uint8_t *payload, const uint64_t *offsets
 
 // ---- launchers ------------------------------------------------------------------------
 
+// LECO_DECODE_STAGED=0 selects the direct (one CTA per block) decode kernel.
+static bool staged_decode_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("LECO_DECODE_STAGED");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 #define LECO_DISPATCH(codec, s, FN, ...)                                   \
   do {                                                                     \
     if ((s) == 4) {                                                        \
@@ -397,11 +556,29 @@ __global__ void build_dir_kernel(const uint8_t *payload, const uint64_t *offsets
     return -1;                                                             \
   } while (0)
 
+// Staging buffer per half: enough for 4096-value blocks with fields of up to
+// 31 bits (u64) -- larger images are decoded straight from global memory.
+constexpr uint32_t kStageBuf = 16640;
+
 template <typename T, int CODEC>
 static void run_decode(const DecodeLaunch &L, cudaStream_t st) {
   if (!L.count) return;
   const uint64_t b0 = L.first / L.bs, b1 = (L.first + L.count - 1) / L.bs;
-  decode_kernel<T, CODEC><<<(unsigned)(b1 - b0 + 1), 256, 0, st>>>(L);
+  const uint64_t nblk = b1 - b0 + 1;
+  const bool staged = L.first == 0 && L.count == L.n && (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 &&
+                      CODEC != kDelta && nblk >= 1024 && staged_decode_enabled();
+  if (!staged) {
+    decode_kernel<T, CODEC><<<(unsigned)nblk, 256, 0, st>>>(L);
+    return;
+  }
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = 2 * kStageBuf + 64;  // +64: field reads may run a few bytes past a full buffer
+  cudaFuncSetAttribute(decode_staged_kernel<T, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_staged_kernel<T, CODEC>, 256, smem);
+  const uint64_t grid = umin64(nblk, (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1));
+  decode_staged_kernel<T, CODEC><<<(unsigned)grid, 256, smem, st>>>(L, kStageBuf);
 }
 int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st) { LECO_DISPATCH(codec, s, run_decode, L, st); }
 

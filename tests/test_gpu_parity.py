@@ -186,3 +186,35 @@ def test_corrupt_header_sets_error_word(lc, orc, dev):
     with pytest.raises(lc.LecoError):
         lc.check()
     lc.check()  # cleared
+
+
+@pytest.mark.parametrize("s", [4, 8])
+def test_staged_decode_large_mixed(lc, orc, dev, s):
+    """Columns of >= 1024 blocks take the persistent TMA-staged decoder; mix
+    narrow blocks (staged), blocks wider than 32 bits and raw blocks (decoded
+    from global memory) in one column."""
+    import torch
+    rng = np.random.default_rng(99 + s)
+    dt = np.uint64 if s == 8 else np.uint32
+    top = 2 ** (8 * s)
+    n = 2_100_003
+    i = np.arange(n, dtype=np.float64)
+    x = np.clip(1e6 + i * 3.5 + rng.normal(0, 300, n), 0, top / 4)
+    seg = (np.arange(n) // 50_000) % 4
+    wide = rng.integers(0, 2 ** (8 * s - 20), n, dtype=np.uint64).astype(np.float64)
+    x = np.where(seg == 1, x + wide, x)                      # wide residuals (l > 32 for u64)
+    x = x.astype(np.uint64)
+    unif = rng.integers(0, top, n, dtype=np.uint64)
+    x = np.where(seg == 2, unif, x).astype(dt)                # raw blocks
+    for codec in (0, 1, 3):
+        for bs in (1000, 2048):
+            col = lc.encode(to_dev(x, dev), codec, bs, lc.FIT_EXACT)
+            assert col.nblocks >= 1024
+            y = to_np(col.decode(), s)
+            assert np.array_equal(y, x), (codec, bs)
+            assert col.sum() == int(x.astype(np.uint64).sum(dtype=np.uint64)), (codec, bs)
+        # and a reference-encoded copy of a slice decodes the same way
+        pay, off = orc.encode_column(codec, x[:1_100_000], 1000)
+        c2 = lc.Column.from_host(codec, s, 1_100_000, 1000, pay, off)
+        assert np.array_equal(to_np(c2.decode(), s), x[:1_100_000]), codec
+    lc.check()
