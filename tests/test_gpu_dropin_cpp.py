@@ -1,0 +1,57 @@
+"""GPU tier: the C++ drop-in header (include/leco_codecs.hpp) driven by a
+reference-style experiment loop (tests/cpp/dropin_driver.cpp), its block
+images compared byte for byte with the oracle's."""
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from gpu_helpers import mask_delta_last_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _keys():
+    N = 200000
+    k32 = np.zeros(N, np.uint32)
+    k64 = np.zeros(N, np.uint64)
+    state = 7
+    M = (1 << 64) - 1
+    for i in range(N):
+        state = (state * 6364136223846793005 + 1442695040888963407) & M
+        k32[i] = (1000 * i + ((state >> 40) & 255)) & 0xFFFFFFFF
+        k64[i] = 5000000000 + 77 * i * i // 64 + ((state >> 20) & 4095)
+    return k32, k64
+
+
+def test_cpp_dropin_driver(tmp_path, orc, lc):
+    exe = tmp_path / "dropin"
+    lib_dir = os.path.dirname(lc.lib_path())
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "dropin_driver.cpp"), "-L", lib_dir, "-lleco_b200",
+                           f"-Wl,-rpath,{lib_dir}", "-o", str(exe)])
+    out = tmp_path / "blocks.bin"
+    r = subprocess.run([str(exe), str(out)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    k32, k64 = _keys()
+    data = out.read_bytes()
+    pos = 0
+    for codec, x, blocks in ((0, k32, 200), (0, k64, 49), (1, k64, 49), (2, k32, 200), (3, k64, 25)):
+        nb = struct.unpack_from("<I", data, pos)[0]
+        pos += 4
+        sizes = np.frombuffer(data, np.uint32, nb, pos)
+        pos += 4 * nb
+        bs = len(x) // blocks
+        for b in range(nb):
+            img = data[pos:pos + int(sizes[b])]
+            pos += int(sizes[b])
+            ref = orc.encode_block(codec, x[b * bs:(b + 1) * bs])
+            if codec == 2:
+                s, m = x.dtype.itemsize, len(x[b * bs:(b + 1) * bs])
+                off = np.array([0, len(img)], np.uint64)
+                img = mask_delta_last_fields(np.frombuffer(img, np.uint8), off, s, m, m).tobytes()
+                ref = mask_delta_last_fields(np.frombuffer(ref, np.uint8), np.array([0, len(ref)], np.uint64), s, m, m).tobytes()
+            assert img == ref, (codec, b)
