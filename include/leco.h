@@ -108,6 +108,23 @@ int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t
                 uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
                 void *d_workspace, uint64_t workspace_bytes, leco_stream_t stream);
 
+/* Same as leco_encode, for callers that cannot allocate device memory (no counterpart in the
+ * reference, whose encoder only writes host memory).  An engine whose buffer manager owns all
+ * device memory, or a latency-critical thread that must not call cudaMalloc/cudaFree (they can
+ * synchronize the whole device), can pass just the input and output buffers: the encoder's
+ * scratch lives in a fixed array inside the library (1 MiB per GPU that loads the library, held
+ * until the process exits).  Columns are limited to leco_encode_noalloc_max_blocks() blocks
+ * (32768); larger ones are rejected with LECO_ERR_ARG.  The first call on each device resolves
+ * the array's device address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Every call uses the same array and the scratch is re-zeroed by each call: calls whose
+ * work overlaps on the GPU (different streams, no ordering between them) race and must not be
+ * issued.  Allocates nothing. */
+int leco_encode_noalloc(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
+                        uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
+                        leco_stream_t stream);
+/* Largest column, in blocks, that leco_encode_noalloc accepts. */
+uint64_t leco_encode_noalloc_max_blocks(void);
+
 /* Decodes a whole column into d_out[n].  Replaces <Codec>::decodeArray8 per block
  * (piecewise_fix_integer_template.h:142-204, FOR_integer_template.h:83-112,
  * delta_integer_template.h:89-127, poly_fix_integer_template.h:93-158).  A block

@@ -60,6 +60,8 @@ SIGNATURES = [
     ("leco_encode_workspace_bytes", _U64, [_I, _I, _U64, _U32, _I]),
     ("leco_block_bytes", _U64, [_I, _I, _U32, _U32]),
     ("leco_encode", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P, _P, _U64, _P]),
+    ("leco_encode_noalloc", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P, _P]),
+    ("leco_encode_noalloc_max_blocks", _U64, []),
     ("leco_decode", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P]),
     ("leco_decode_range", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _U64, _P, _P]),
     ("leco_build_directory", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P]),

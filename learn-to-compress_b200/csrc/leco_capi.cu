@@ -19,6 +19,8 @@ static int fail(int code, const std::string &msg) {
   g_last_error = msg;
   return code;
 }
+int record_error(int code, const std::string &msg) { return fail(code, msg); }
+
 static int cuda_fail(cudaError_t e, const char *where) {
   return fail(LECO_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }

@@ -1,6 +1,7 @@
 // leco_internal.h -- declarations shared by the library's translation units.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "../../include/leco.h"
@@ -57,5 +58,8 @@ int launch_build_dir(int codec, int s, const uint8_t *payload, const uint64_t *o
 // by repeated multiplication (:80-99).  Host code, compiled with
 // -ffp-contract=off.
 void poly2_x_sums(uint32_t N, double X[5]);
+
+// Records `msg` as this thread's leco_last_error() message and returns `code`.
+int record_error(int code, const std::string &msg);
 
 }  // namespace leco
