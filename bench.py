@@ -33,7 +33,7 @@ METRIC = "LeCo-fix decode GB/s and batched random-access Mlookups/s, p50/p99, 1 
 N_DEFAULT = 200_000_000
 BS = 4096
 RA_BATCH = 1 << 24
-DECODE_KERNEL = "decode_kernel"
+DECODE_KERNEL = "decode_staged_kernel"
 
 
 def parse():
@@ -58,7 +58,7 @@ def peaks():
 
 def profile_traffic():
     """Per-launch DRAM bytes of the decode kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "decode_kernel_leco_u64_200M.txt")
+    p = os.path.join(ROOT, "profiles", "decode_staged_kernel_leco_u64_200M.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):

@@ -53,9 +53,16 @@ __device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ pay
 }
 
 template <int CODEC, int S>
-__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b) {
+__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b, uint64_t pol = 0) {
   const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
-  ulonglong2 q0 = __ldg(p), q1 = __ldg(p + 1);
+  ulonglong2 q0, q1;
+  if (pol) {
+    q0 = ldg_v2_hint(p, pol);
+    q1 = ldg_v2_hint(p + 1, pol);
+  } else {
+    q0 = __ldg(p);
+    q1 = __ldg(p + 1);
+  }
   BlockHdr h;
   h.body_bit = q0.x & ((1ull << 48) - 1);
   h.l = (uint32_t)(q0.x >> 56);
@@ -459,8 +466,90 @@ __global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_su
 }
 
 // ---- random access --------------------------------------------------------------
+// Value of one lookup from its block model and field (randomdecodeArray8 rules).
+template <int CODEC, int S>
+__device__ __forceinline__ uint64_t ra_value(const BlockHdr &h, uint32_t k, uint64_t f, uint32_t *error) {
+  constexpr uint32_t TB = 8u * S;
+  if (h.l == TB) return f;  // raw (…_integer_template.h:313-317)
+  if (h.l > TB) {           // sentinel / corrupt header: the reference's random access has no such case
+    atomicOr(error, kErrBadHeader);
+    return 0;
+  }
+  if (CODEC == kFor) return h.l ? h.base + f : h.base;
+  const double p = CODEC == kLinear ? pred_linear(h.a0, h.a1, k) : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
+  if (h.l) return apply_signed((uint64_t)f2i_x86(p), f, h.l);
+  return f2T_x86<S>(p);  // l == 0: (T)prediction directly (piecewise_fix_integer_template.h:334, poly :288)
+}
+
+// Batched random access: each thread keeps U lookups in flight (indices,
+// directory entries and payload words are each loaded for all U before any is
+// used), lookups i, i+G, i+2G, ... of one thread are strided by the grid so
+// index loads and output stores stay coalesced across a warp.
 template <typename T, int CODEC>
 __global__ void __launch_bounds__(256) gather_kernel(GatherLaunch a) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  constexpr int U = 4;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  T *out = reinterpret_cast<T *>(a.out);
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const bool small = a.n <= 0xffffffffull;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < a.m; i0 += G * U) {
+    uint64_t g[U], b[U];
+    uint32_t k[U];
+    bool live[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t i = i0 + (uint64_t)u * G;
+      live[u] = i < a.m;
+      g[u] = live[u] ? __ldg(a.idx + i) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (g[u] >= a.n) {
+        if (live[u]) {
+          out[i0 + (uint64_t)u * G] = 0;
+          atomicOr(a.error, kErrBadIndex);
+        }
+        live[u] = false;
+        g[u] = 0;
+      }
+      if (small) {
+        b[u] = (uint32_t)g[u] / a.bs;
+        k[u] = (uint32_t)g[u] - (uint32_t)b[u] * a.bs;
+      } else {
+        b[u] = g[u] / a.bs;
+        k[u] = (uint32_t)(g[u] - b[u] * a.bs);
+      }
+    }
+    BlockHdr h[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      h[u] = a.dir ? from_dir<CODEC, S>(a.dir, b[u]) : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b[u]));
+    uint64_t lo[U], hi[U];
+    uint32_t sh[U], l[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      l[u] = h[u].l > TB ? 0 : h[u].l;
+      const uint64_t bit = h[u].body_bit + (uint64_t)k[u] * l[u];
+      sh[u] = (uint32_t)(bit & 63);
+      // the second word only when the field crosses into it: a random lookup then
+      // touches one DRAM sector instead of two whenever the field sits in one word
+      lo[u] = l[u] ? __ldg(words + (bit >> 6)) : 0;
+      hi[u] = (l[u] && sh[u] + l[u] > 64) ? __ldg(words + (bit >> 6) + 1) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!live[u]) continue;
+      const uint64_t f = funnel64(lo[u], hi[u], sh[u]) & lowmask(l[u]);
+      out[i0 + (uint64_t)u * G] = (T)ra_value<CODEC, S>(h[u], k[u], f, a.error);
+    }
+  }
+}
+
+// Delta random access: prefix walk over fields 0..k-1 (bit_read.h:1292-1317).
+template <typename T>
+__global__ void __launch_bounds__(256) gather_delta_kernel(GatherLaunch a) {
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
@@ -472,33 +561,16 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherLaunch a) {
       atomicOr(a.error, kErrBadIndex);
       continue;
     }
-    uint64_t b;
-    uint32_t k;
-    if (a.n <= 0xffffffffull) {
-      b = (uint32_t)g / a.bs;
-      k = (uint32_t)g - (uint32_t)b * a.bs;
-    } else {
-      b = g / a.bs;
-      k = (uint32_t)(g - b * a.bs);
-    }
-    const BlockHdr h = a.dir ? from_dir<CODEC, S>(a.dir, b) : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+    const uint64_t b = g / a.bs;
+    const uint32_t k = (uint32_t)(g - b * a.bs);
+    const BlockHdr h = a.dir ? from_dir<kDelta, S>(a.dir, b) : parse_header<kDelta, S>(a.payload, __ldg(a.offsets + b));
     uint64_t v;
     if (h.l == TB) {
-      v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);  // raw (…_integer_template.h:313-317)
+      v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);
     } else if (h.l > TB) {
-      v = 0;  // sentinel / corrupt header: the reference's random access has no such case
+      v = 0;
       atomicOr(a.error, kErrBadHeader);
-    } else if (CODEC == kLinear) {
-      const double p = pred_linear(h.a0, h.a1, k);
-      if (h.l) v = apply_signed((uint64_t)f2i_x86(p), load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-      else v = f2T_x86<S>(p);  // (T)(theta0 + k*theta1) directly (:334)
-    } else if (CODEC == kPoly2) {
-      const double p = pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
-      if (h.l) v = apply_signed((uint64_t)f2i_x86(p), load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-      else v = f2T_x86<S>(p);  // poly_fix_integer_template.h:288
-    } else if (CODEC == kFor) {
-      v = h.l ? h.base + load_field(words, h.body_bit + (uint64_t)k * h.l, h.l) : h.base;
-    } else {  // Delta: prefix walk over fields 0..k-1 (bit_read.h:1292-1317)
+    } else {
       v = h.base;
       if (h.l)
         for (uint32_t j = 0; j < k; ++j) v += apply_signed(0, load_field(words, h.body_bit + (uint64_t)j * h.l, h.l), h.l);
@@ -597,8 +669,13 @@ static void run_gather(const GatherLaunch &L, cudaStream_t st) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const uint64_t need = (L.m + 255) / 256;
-  const unsigned grid = (unsigned)umin64(need, (uint64_t)sms * 16);
+  if (CODEC == kDelta) {
+    const unsigned grid = (unsigned)umin64((L.m + 255) / 256, (uint64_t)sms * 16);
+    gather_delta_kernel<T><<<grid, 256, 0, st>>>(L);
+    return;
+  }
+  const uint64_t need = (L.m + 4 * 256 - 1) / (4 * 256);  // 4 lookups in flight per thread
+  const unsigned grid = (unsigned)umin64(need, (uint64_t)sms * 8);
   gather_kernel<T, CODEC><<<grid, 256, 0, st>>>(L);
 }
 int launch_gather(int codec, int s, const GatherLaunch &L, cudaStream_t st) { LECO_DISPATCH(codec, s, run_gather, L, st); }

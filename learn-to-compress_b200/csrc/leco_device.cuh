@@ -190,6 +190,31 @@ __device__ __forceinline__ u128 block_reduce(u128 v, u128 *red) {
   return red[32];
 }
 
+// ---- L2 eviction-priority hints ---------------------------------------------
+// Random access streams gigabytes of random payload sectors through L2; these
+// keep the small, hot block directory resident (evict_last) and let the
+// streaming index/output traffic go first (evict_first).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ ulonglong2 ldg_v2_hint(const void *ptr, uint64_t pol) {
+  ulonglong2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint64_t ldg_u64_hint(const void *ptr, uint64_t pol) {
+  uint64_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(ptr), "l"(pol));
+  return v;
+}
+
 // ---- relaxed global word access for the look-back scan ----------------------
 __device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p) {
   uint64_t v;
