@@ -160,6 +160,45 @@ uint64_t leco_sum_workspace_bytes(uint64_t n, uint32_t block_size);
 int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
              uint32_t block_size, uint64_t *d_sum, void *d_partials, leco_stream_t stream);
 
+/* ---- batch engine: many columns, one persistent launch per pass --------
+ * No counterpart in the reference, whose drivers loop over the blocks of one
+ * column (experiments/leco_int_fix_template.cpp:111-127, :145-153). */
+
+typedef struct leco_column_desc {
+  int32_t codec;       /* LINEAR, FOR, DELTA or POLY2                          */
+  int32_t dtype;       /* LECO_U32 or LECO_U64                                 */
+  uint32_t block_size; /* values per block, 1..16384                           */
+  uint32_t reserved;
+  uint64_t n;          /* values in the column                                 */
+  const void *d_values;/* encode input (n values)                              */
+  void *d_out;         /* decode output (n values); may be NULL if never decoded */
+  uint8_t *d_payload;  /* block images (leco_max_payload_bytes capacity)       */
+  uint64_t payload_cap;
+  uint64_t *d_offsets; /* nblocks + 1                                          */
+  leco_dir_entry *d_dir; /* nblocks entries or NULL                            */
+} leco_column_desc;
+
+typedef struct leco_batch leco_batch; /* opaque */
+
+/* Builds a batch over ncols column descriptors (copied).  Allocates the device
+ * descriptor table and the batch workspace (the only allocations of the batch
+ * engine); sizes the persistent grids so every CTA is resident. */
+int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mode, leco_batch **out);
+int leco_batch_destroy(leco_batch *b);
+uint64_t leco_batch_total_blocks(const leco_batch *b);
+/* Encodes every block of every column with one persistent launch pulling
+ * (column, block) items from an atomic work queue (plus the sequential-fit pass
+ * for reference-fit columns that need it). */
+int leco_batch_encode(leco_batch *b, leco_stream_t stream);
+/* Decodes every column into its d_out with one persistent launch. */
+int leco_batch_decode(leco_batch *b, leco_stream_t stream);
+/* Captures the pass(es) (1 encode, 2 decode, 3 both) into a CUDA graph on the
+ * first call and replays the graph on every call. */
+int leco_batch_run_graph(leco_batch *b, int passes, leco_stream_t stream);
+/* The same work as one leco_encode / leco_decode call per column (baseline). */
+int leco_batch_encode_per_column(leco_batch *b, leco_stream_t stream);
+int leco_batch_decode_per_column(leco_batch *b, leco_stream_t stream);
+
 /* ---- host-buffer entry points (synchronous; allocate device memory) ----
  * These are the reference-facing calls: host in, host out, the same
  * arguments as the reference's per-column driver loops. */

@@ -75,6 +75,14 @@ SIGNATURES = [
     ("leco_block_decode", _I, [_I, _I, _P, _U64, _U32, _P]),
     ("leco_block_random", _I, [_I, _I, _P, _U64, _U32, _U32, _P]),
     ("leco_validate_host", _I, [_I, _I, _P, _U64, _P, _U64, _U32, _P]),
+    ("leco_batch_create", _I, [_P, _U32, _I, _P]),
+    ("leco_batch_destroy", _I, [_P]),
+    ("leco_batch_total_blocks", _U64, [_P]),
+    ("leco_batch_encode", _I, [_P, _P]),
+    ("leco_batch_decode", _I, [_P, _P]),
+    ("leco_batch_run_graph", _I, [_P, _I, _P]),
+    ("leco_batch_encode_per_column", _I, [_P, _P]),
+    ("leco_batch_decode_per_column", _I, [_P, _P]),
     ("leco_check", _I, [_P]),
     ("leco_last_error", ctypes.c_char_p, []),
     ("leco_version", ctypes.c_char_p, []),
@@ -355,3 +363,79 @@ def encode(values, codec: int = LINEAR, block_size: int = 4096, fit_mode: int = 
 
 def version() -> str:
     return lib().leco_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# Batch engine: many columns, one persistent launch per pass.
+# ---------------------------------------------------------------------------
+
+class ColumnDesc(ctypes.Structure):
+    """``leco_column_desc`` of include/leco.h."""
+    _fields_ = [("codec", ctypes.c_int32), ("dtype", ctypes.c_int32), ("block_size", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("n", ctypes.c_uint64), ("d_values", _P), ("d_out", _P),
+                ("d_payload", _P), ("payload_cap", ctypes.c_uint64), ("d_offsets", _P), ("d_dir", _P)]
+
+
+class Batch:
+    """Columns encoded/decoded together by the persistent batch kernels.
+
+    ``columns``: list of (values CUDA tensor, codec, block_size).  Payload,
+    offsets, directory and decode-output tensors are allocated here; the C
+    side keeps only raw pointers, so this object owns them.
+    """
+
+    def __init__(self, columns, fit_mode: int = FIT_REFERENCE, decode_out: bool = True):
+        torch = _torch()
+        L = lib()
+        self.fit_mode = fit_mode
+        self.values, self.cols = [], []
+        descs = (ColumnDesc * len(columns))()
+        for i, (v, codec, bs) in enumerate(columns):
+            s, n = v.element_size(), v.numel()
+            nb = L.leco_num_blocks(n, bs)
+            cap = L.leco_max_payload_bytes(codec, s, n, bs)
+            pay = torch.empty(cap, dtype=torch.uint8, device=v.device)
+            off = torch.empty(nb + 1, dtype=torch.int64, device=v.device)
+            d = torch.empty(nb * 32, dtype=torch.uint8, device=v.device)
+            out = torch.empty_like(v) if decode_out else None
+            col = Column(codec, s, n, bs, pay, off, d)
+            col.out = out
+            self.values.append(v)
+            self.cols.append(col)
+            descs[i] = ColumnDesc(codec, s, bs, 0, n, v.data_ptr(), out.data_ptr() if out is not None else None,
+                                  pay.data_ptr(), cap, off.data_ptr(), d.data_ptr())
+        self._descs = descs
+        h = _P()
+        _check(L.leco_batch_create(descs, len(columns), fit_mode, ctypes.byref(h)), "leco_batch_create")
+        self._h = h
+
+    @property
+    def total_blocks(self) -> int:
+        return lib().leco_batch_total_blocks(self._h)
+
+    def encode(self, stream=None):
+        _check(lib().leco_batch_encode(self._h, _stream_ptr(stream)), "leco_batch_encode")
+
+    def decode(self, stream=None):
+        _check(lib().leco_batch_decode(self._h, _stream_ptr(stream)), "leco_batch_decode")
+
+    def run_graph(self, passes: int = 3, stream=None):
+        """passes: 1 encode, 2 decode, 3 both -- captured once, replayed after."""
+        _check(lib().leco_batch_run_graph(self._h, passes, _stream_ptr(stream)), "leco_batch_run_graph")
+
+    def encode_per_column(self, stream=None):
+        _check(lib().leco_batch_encode_per_column(self._h, _stream_ptr(stream)), "leco_batch_encode_per_column")
+
+    def decode_per_column(self, stream=None):
+        _check(lib().leco_batch_decode_per_column(self._h, _stream_ptr(stream)), "leco_batch_decode_per_column")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().leco_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

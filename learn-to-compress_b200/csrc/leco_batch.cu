@@ -1,0 +1,365 @@
+// leco_batch.cu -- batch engine: thousands of columns of uneven length, mixed
+// uint32/uint64 and mixed LeCo/FOR/Delta/poly codecs, encoded and decoded by
+// one persistent launch per pass.
+//
+// Work queue: the batch's blocks are numbered column by column (block_prefix[c]
+// = number of blocks before column c).  Every CTA of a persistent grid takes the
+// next number from an atomic ticket, finds its column by binary search over
+// block_prefix and runs the per-block encoder or decoder for that column's codec
+// and value type.  Tickets are handed out in order and every CTA of the grid is
+// resident, so the encoder's per-column look-back (byte offsets) only ever waits
+// on blocks that are already being processed.
+//
+// The reference has no counterpart: its drivers loop over blocks of one column
+// (experiments/leco_int_fix_template.cpp:111-127, :145-153).  The per-column
+// path (leco_batch_*_per_column) is what a caller of leco_encode / leco_decode
+// does without the batch engine, kept as the baseline.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "leco_decode.cuh"
+#include "leco_encode.cuh"
+
+namespace leco {
+
+struct DevCol {
+  int32_t codec, dtype;
+  uint32_t bs, seq;
+  uint64_t n;
+  const void *values;
+  void *out;
+  uint8_t *payload;
+  uint64_t payload_cap;
+  uint64_t *offsets;
+  leco_dir_entry *dir;
+  double polyX[10];
+};
+
+__device__ __forceinline__ uint32_t find_column(const uint64_t *__restrict__ prefix, uint32_t ncols, uint64_t gb) {
+  uint32_t lo = 0, hi = ncols;  // largest c with prefix[c] <= gb
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(prefix + mid) <= gb) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+#define LECO_BATCH_DISPATCH(codec, dtype, FN, ...)                 \
+  do {                                                             \
+    if ((dtype) == 4) {                                            \
+      switch (codec) {                                             \
+        case kLinear: FN<uint32_t, kLinear>(__VA_ARGS__); break;   \
+        case kFor: FN<uint32_t, kFor>(__VA_ARGS__); break;         \
+        case kDelta: FN<uint32_t, kDelta>(__VA_ARGS__); break;     \
+        case kPoly2: FN<uint32_t, kPoly2>(__VA_ARGS__); break;     \
+      }                                                            \
+    } else {                                                       \
+      switch (codec) {                                             \
+        case kLinear: FN<uint64_t, kLinear>(__VA_ARGS__); break;   \
+        case kFor: FN<uint64_t, kFor>(__VA_ARGS__); break;         \
+        case kDelta: FN<uint64_t, kDelta>(__VA_ARGS__); break;     \
+        case kPoly2: FN<uint64_t, kPoly2>(__VA_ARGS__); break;     \
+      }                                                            \
+    }                                                              \
+  } while (0)
+
+struct BatchArgs {
+  const DevCol *cols;
+  const uint64_t *prefix;  // [ncols + 1]
+  uint32_t ncols;
+  uint64_t total;          // blocks in the batch
+  uint64_t *status;        // [total] look-back words (zeroed per encode pass)
+  unsigned long long *ticket;  // zeroed per pass
+  double *models;          // [total * 3] sequential-fit models
+  uint32_t *error;
+};
+
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b,
+                                                 uint8_t *smem) {
+  EncodeArgs a;
+  a.values = c.values;
+  a.n = c.n;
+  a.bs = c.bs;
+  const uint64_t p0 = __ldg(B.prefix + ci);
+  a.nb = __ldg(B.prefix + ci + 1) - p0;
+  a.payload = c.payload;
+  a.payload_cap = c.payload_cap;
+  a.offsets = c.offsets;
+  a.dir = c.dir;
+  a.seq_models = c.seq ? B.models + p0 * 3 : nullptr;
+  for (int i = 0; i < 10; ++i) a.polyX[i] = c.polyX[i];
+  a.status = B.status + p0;
+  a.ticket = nullptr;
+  a.error = B.error;
+  encode_block<T, CODEC>(a, b, smem);
+}
+
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_decode_one(const BatchArgs &B, const DevCol &c, uint64_t b) {
+  DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
+  decode_block<T, CODEC>(a, b);
+}
+
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_seq_one(const DevCol &c, uint64_t b, double *models) {
+  seq_fit_block<T, CODEC>(reinterpret_cast<const T *>(c.values), c.n, c.bs, b, c.polyX, models);
+}
+
+// Persistent encode: one ticket = one block of some column.
+__global__ void __launch_bounds__(256) batch_encode_kernel(BatchArgs B) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ unsigned long long item;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
+    __syncthreads();
+    const uint64_t gb = item;
+    __syncthreads();
+    if (gb >= B.total) break;
+    const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+    const DevCol &c = B.cols[ci];
+    const uint64_t b = gb - __ldg(B.prefix + ci);
+    LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_one, B, c, ci, b, smem);
+    __syncthreads();  // shared memory is reused by the next block
+  }
+}
+
+// Persistent decode: one ticket = one block of some column.
+__global__ void __launch_bounds__(256) batch_decode_kernel(BatchArgs B) {
+  __shared__ unsigned long long item;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
+    __syncthreads();
+    const uint64_t gb = item;
+    __syncthreads();
+    if (gb >= B.total) break;
+    const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+    const DevCol &c = B.cols[ci];
+    const uint64_t b = gb - __ldg(B.prefix + ci);
+    LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_one, B, c, b);
+  }
+}
+
+// Sequential reference fits for every block of the columns that need them.
+__global__ void __launch_bounds__(128) batch_seq_fit_kernel(BatchArgs B) {
+  const uint64_t gb = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gb >= B.total) return;
+  const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+  const DevCol &c = B.cols[ci];
+  if (!c.seq) return;
+  const uint64_t p0 = __ldg(B.prefix + ci);
+  LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_seq_one, c, gb - p0, B.models + p0 * 3);
+}
+
+}  // namespace leco
+
+using namespace leco;
+
+struct leco_batch {
+  std::vector<leco_column_desc> cols;
+  std::vector<uint64_t> prefix;
+  int fit_mode = LECO_FIT_REFERENCE;
+  bool any_seq = false;
+  int device = 0;
+  DevCol *d_cols = nullptr;
+  uint64_t *d_prefix = nullptr;
+  uint8_t *d_ws = nullptr;  // status [total] | ticket | models [total*3]
+  uint64_t ws_bytes = 0, status_bytes = 0, models_off = 0;
+  uint32_t enc_smem = 0;
+  int enc_grid = 0, dec_grid = 0;
+  uint32_t *err = nullptr;               // library error word on this device
+  cudaStream_t capture_stream = nullptr;  // graphs are captured here (the caller's stream may be the legacy default stream)
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int berr(int code, const std::string &m) { return leco::record_error(code, m); }
+
+bool needs_seq(int codec, int dtype, uint32_t bs, int fit_mode) {
+  if (fit_mode != LECO_FIT_REFERENCE) return false;
+  if (codec == kLinear) return !(dtype == LECO_U32 && bs <= 2048);
+  return codec == kPoly2;
+}
+
+BatchArgs args_of(const leco_batch *b, uint32_t *err) {
+  BatchArgs B;
+  B.cols = b->d_cols;
+  B.prefix = b->d_prefix;
+  B.ncols = (uint32_t)b->cols.size();
+  B.total = b->prefix.back();
+  B.status = reinterpret_cast<uint64_t *>(b->d_ws);
+  B.ticket = reinterpret_cast<unsigned long long *>(b->d_ws + b->status_bytes);
+  B.models = reinterpret_cast<double *>(b->d_ws + b->models_off);
+  B.error = err;
+  return B;
+}
+
+}  // namespace
+
+extern "C" {
+
+int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mode, leco_batch **out) {
+  if (!h_cols || !ncols || !out) return berr(LECO_ERR_ARG, "leco_batch_create: null pointer or empty batch");
+  if (fit_mode != LECO_FIT_REFERENCE && fit_mode != LECO_FIT_EXACT) return berr(LECO_ERR_ARG, "leco_batch_create: bad fit_mode");
+  auto *b = new leco_batch();
+  b->cols.assign(h_cols, h_cols + ncols);
+  b->fit_mode = fit_mode;
+  cudaGetDevice(&b->device);
+  b->prefix.resize(ncols + 1);
+  std::vector<DevCol> dc(ncols);
+  uint64_t total = 0;
+  uint32_t max_smem = 0;
+  for (uint32_t i = 0; i < ncols; ++i) {
+    const leco_column_desc &c = h_cols[i];
+    if (c.codec < kLinear || c.codec > kPoly2 || (c.dtype != 4 && c.dtype != 8) || !c.block_size ||
+        c.block_size > LECO_MAX_BLOCK || !c.n || !c.d_payload || !c.d_offsets) {
+      delete b;
+      return berr(LECO_ERR_ARG, "leco_batch_create: bad descriptor for column " + std::to_string(i));
+    }
+    b->prefix[i] = total;
+    total += leco_num_blocks(c.n, c.block_size);
+    DevCol &d = dc[i];
+    d.codec = c.codec;
+    d.dtype = c.dtype;
+    d.bs = c.block_size;
+    d.seq = needs_seq(c.codec, c.dtype, c.block_size, fit_mode);
+    b->any_seq |= d.seq != 0;
+    d.n = c.n;
+    d.values = c.d_values;
+    d.out = c.d_out;
+    d.payload = c.d_payload;
+    d.payload_cap = c.payload_cap;
+    d.offsets = c.d_offsets;
+    d.dir = c.d_dir;
+    for (int k = 0; k < 10; ++k) d.polyX[k] = 0;
+    if (c.codec == kPoly2) {
+      const uint64_t nb = leco_num_blocks(c.n, c.block_size);
+      poly2_x_sums((uint32_t)std::min<uint64_t>(c.n, c.block_size), d.polyX);
+      poly2_x_sums((uint32_t)(c.n - (nb - 1) * c.block_size), d.polyX + 5);
+    }
+    max_smem = std::max(max_smem, enc_smem_bytes(c.block_size, (uint32_t)c.dtype));
+  }
+  b->prefix[ncols] = total;
+  if (total > 0xffffffffull) {
+    delete b;
+    return berr(LECO_ERR_ARG, "leco_batch_create: more than 2^32 blocks");
+  }
+  b->status_bytes = (total * 8 + 255) / 256 * 256;
+  b->models_off = b->status_bytes + 256;
+  b->ws_bytes = b->models_off + (b->any_seq ? (total * 24 + 255) / 256 * 256 : 0);
+  b->enc_smem = max_smem;
+  cudaError_t e = cudaMalloc(&b->d_cols, ncols * sizeof(DevCol));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, (ncols + 1) * sizeof(uint64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_ws, b->ws_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_cols, dc.data(), ncols * sizeof(DevCol), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, b->prefix.data(), (ncols + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && leco::device_error_word(&b->err)) e = cudaErrorUnknown;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && max_smem > 48 * 1024)
+    e = cudaFuncSetAttribute(batch_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+  int sms = 148, per_enc = 1, per_dec = 1;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_enc, batch_encode_kernel, 256, max_smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_dec, batch_decode_kernel, 256, 0);
+  if (e != cudaSuccess || per_enc < 1 || per_dec < 1) {
+    leco_batch_destroy(b);
+    return berr(e != cudaSuccess ? LECO_ERR_CUDA : LECO_ERR_ARG,
+                std::string("leco_batch_create: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "no resident CTA fits"));
+  }
+  // every CTA of the persistent grid must be resident (the look-back waits on them)
+  b->enc_grid = (int)std::min<uint64_t>(total, (uint64_t)sms * per_enc);
+  b->dec_grid = (int)std::min<uint64_t>(total, (uint64_t)sms * per_dec);
+  *out = b;
+  return LECO_OK;
+}
+
+int leco_batch_destroy(leco_batch *b) {
+  if (!b) return LECO_OK;
+  for (auto &g : b->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+  if (b->d_cols) cudaFree(b->d_cols);
+  if (b->d_prefix) cudaFree(b->d_prefix);
+  if (b->d_ws) cudaFree(b->d_ws);
+  delete b;
+  return LECO_OK;
+}
+
+uint64_t leco_batch_total_blocks(const leco_batch *b) { return b ? b->prefix.back() : 0; }
+
+int leco_batch_encode(leco_batch *b, leco_stream_t stream) {
+  if (!b) return berr(LECO_ERR_ARG, "leco_batch_encode: null batch");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const BatchArgs B = args_of(b, b->err);
+  cudaError_t e = cudaMemsetAsync(b->d_ws, 0, b->status_bytes + 256, st);  // look-back words + ticket
+  if (e == cudaSuccess && b->any_seq)
+    batch_seq_fit_kernel<<<(unsigned)((B.total + 127) / 128), 128, 0, st>>>(B);
+  if (e == cudaSuccess) batch_encode_kernel<<<b->enc_grid, 256, b->enc_smem, st>>>(B);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : berr(LECO_ERR_CUDA, std::string("leco_batch_encode: ") + cudaGetErrorString(e));
+}
+
+int leco_batch_decode(leco_batch *b, leco_stream_t stream) {
+  if (!b) return berr(LECO_ERR_ARG, "leco_batch_decode: null batch");
+  for (const auto &c : b->cols)
+    if (!c.d_out) return berr(LECO_ERR_ARG, "leco_batch_decode: a column has no output buffer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const BatchArgs B = args_of(b, b->err);
+  cudaError_t e = cudaMemsetAsync(b->d_ws + b->status_bytes, 0, 256, st);  // ticket
+  if (e == cudaSuccess) batch_decode_kernel<<<b->dec_grid, 256, 0, st>>>(B);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : berr(LECO_ERR_CUDA, std::string("leco_batch_decode: ") + cudaGetErrorString(e));
+}
+
+int leco_batch_run_graph(leco_batch *b, int passes, leco_stream_t stream) {
+  if (!b || passes < 1 || passes > 3) return berr(LECO_ERR_ARG, "leco_batch_run_graph: passes must be 1 (encode), 2 (decode) or 3");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (!b->graph[passes]) {
+    cudaGraph_t g = nullptr;
+    cudaStream_t cs = b->capture_stream;
+    leco_stream_t lcs = reinterpret_cast<leco_stream_t>(cs);
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return berr(LECO_ERR_CUDA, std::string("leco_batch_run_graph: ") + cudaGetErrorString(e));
+    int rc = LECO_OK;
+    if (passes & 1) rc = leco_batch_encode(b, lcs);
+    if (!rc && (passes & 2)) rc = leco_batch_decode(b, lcs);
+    e = cudaStreamEndCapture(cs, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[passes], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) return berr(LECO_ERR_CUDA, std::string("leco_batch_run_graph: ") + cudaGetErrorString(e));
+  }
+  cudaError_t e = cudaGraphLaunch(b->graph[passes], st);
+  return e == cudaSuccess ? LECO_OK : berr(LECO_ERR_CUDA, std::string("leco_batch_run_graph: ") + cudaGetErrorString(e));
+}
+
+// Baseline: one leco_encode call per column (the batch's workspace is reused;
+// each call resets it).
+int leco_batch_encode_per_column(leco_batch *b, leco_stream_t stream) {
+  if (!b) return berr(LECO_ERR_ARG, "null batch");
+  for (const auto &c : b->cols) {
+    int rc = leco_encode(c.codec, c.dtype, c.d_values, c.n, c.block_size, b->fit_mode, c.d_payload, c.payload_cap,
+                         c.d_offsets, c.d_dir, b->d_ws, b->ws_bytes, stream);
+    if (rc) return rc;
+  }
+  return LECO_OK;
+}
+
+int leco_batch_decode_per_column(leco_batch *b, leco_stream_t stream) {
+  if (!b) return berr(LECO_ERR_ARG, "null batch");
+  for (const auto &c : b->cols) {
+    int rc = leco_decode(c.codec, c.dtype, c.d_payload, c.d_offsets, c.n, c.block_size, c.d_out, stream);
+    if (rc) return rc;
+  }
+  return LECO_OK;
+}
+
+}  // extern "C"

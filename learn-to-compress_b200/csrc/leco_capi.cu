@@ -44,6 +44,8 @@ static int error_ptr(uint32_t **p) {
   return LECO_OK;
 }
 
+int device_error_word(uint32_t **p) { return error_ptr(p); }
+
 static bool codec_ok(int codec) { return codec >= kLinear && codec <= kPoly2; }
 static bool dtype_ok(int dtype) { return dtype == LECO_U32 || dtype == LECO_U64; }
 

@@ -13,274 +13,11 @@
 // A block is raw iff l == 8*sizeof(T) everywhere (the reference's random-access
 // rule).  The reference's bulk decoders also call l == 8*sizeof(T)-1 raw, which
 // mis-decodes such packed blocks; this decoder reads them correctly.
-#include "leco_device.cuh"
-#include "leco_internal.h"
+#include "leco_decode.cuh"
 
 #include <cstdlib>
 
 namespace leco {
-
-// Block model parsed from a header (or a directory entry).
-struct BlockHdr {
-  uint64_t body_bit;  // absolute bit address of field 0 (raw: of value 0)
-  uint32_t l;         // field width; 8*S = raw; 126/127 = 2/1-value sentinels
-  double a0, a1, a2;  // model
-  uint64_t base;      // FOR minimum / Delta first value
-};
-
-template <int CODEC, int S>
-__device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ payload, uint64_t off) {
-  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
-  BlockHdr h;
-  uint64_t w0 = load_u64_at(words, off);
-  h.l = (uint32_t)(w0 & 0xff);
-  h.a0 = h.a1 = h.a2 = 0;
-  h.base = 0;
-  if (h.l == 8u * S || h.l == 126 || h.l == 127) {
-    h.body_bit = (off + 1) * 8;
-    return h;
-  }
-  if (CODEC == kLinear || CODEC == kPoly2) {
-    h.a0 = __longlong_as_double((long long)load_u64_at(words, off + 1));
-    h.a1 = __longlong_as_double((long long)load_u64_at(words, off + 9));
-    if (CODEC == kPoly2) h.a2 = __longlong_as_double((long long)load_u64_at(words, off + 17));
-  } else {
-    uint64_t v = load_u64_at(words, off + 1);
-    h.base = S == 8 ? v : (v & 0xffffffffull);
-  }
-  h.body_bit = (off + Hdr<CODEC, S>::bytes) * 8;
-  return h;
-}
-
-template <int CODEC, int S>
-__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b, uint64_t pol = 0) {
-  const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
-  ulonglong2 q0, q1;
-  if (pol) {
-    q0 = ldg_v2_hint(p, pol);
-    q1 = ldg_v2_hint(p + 1, pol);
-  } else {
-    q0 = __ldg(p);
-    q1 = __ldg(p + 1);
-  }
-  BlockHdr h;
-  h.body_bit = q0.x & ((1ull << 48) - 1);
-  h.l = (uint32_t)(q0.x >> 56);
-  h.a0 = __longlong_as_double((long long)q0.y);
-  h.a1 = __longlong_as_double((long long)q1.x);
-  h.a2 = __longlong_as_double((long long)q1.y);
-  h.base = S == 8 ? q0.y : (q0.y & 0xffffffffull);
-  return h;
-}
-
-// Value k of a non-raw, non-Delta block given its field f (bulk decode rules).
-template <int CODEC, int S>
-__device__ __forceinline__ uint64_t value_from_field(const BlockHdr &h, uint32_t k, uint64_t f) {
-  if (CODEC == kFor) return h.base + f;
-  int64_t pred;
-  if (CODEC == kLinear) pred = f2i_x86(pred_linear(h.a0, h.a1, k));
-  else pred = f2i_x86(pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k)));
-  return h.l ? apply_signed((uint64_t)pred, f, h.l) : (uint64_t)pred;
-}
-
-// Delta running sum split over the CTA: each thread owns a contiguous chunk
-// [k0, k1) of values; a block-wide exclusive scan of the chunks' delta sums
-// gives each thread the value at k0.  Must be called by all threads.
-struct DeltaChunk {
-  uint32_t k0, k1;
-  uint64_t run;  // decoded value k0 (mod 2^64)
-};
-__device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len) {
-  __shared__ uint64_t wsum[32];
-  const uint32_t nt = blockDim.x, tid = threadIdx.x;
-  const uint32_t chunk = (len + nt - 1) / nt;
-  DeltaChunk c;
-  c.k0 = min(len, tid * chunk);
-  c.k1 = min(len, c.k0 + chunk);
-  uint64_t local = 0;  // fields k0 .. k1-1 feed values k0+1 .. k1; field len-1 is not a delta
-  if (h.l)
-    for (uint32_t k = c.k0; k < c.k1 && k + 1 < len; ++k)
-      local += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-  const int lane = tid & 31, warp = tid >> 5;
-  uint64_t incl = local;
-  for (int d = 1; d < 32; d <<= 1) {
-    uint64_t y = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl += y;
-  }
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = (nt + 31) >> 5;
-    uint64_t x = lane < nw ? wsum[lane] : 0, xi = x;
-    for (int d = 1; d < 32; d <<= 1) {
-      uint64_t y = __shfl_up_sync(0xffffffffu, xi, d);
-      if (lane >= d) xi += y;
-    }
-    if (lane < nw) wsum[lane] = xi - x;
-  }
-  __syncthreads();
-  c.run = h.base + wsum[warp] + (incl - local);
-  return c;
-}
-
-template <typename T>
-__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v, int cnt, bool full);
-template <>
-__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
-}
-template <>
-__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
-}
-
-
-// True when every prediction of the block is a finite double inside
-// (-2^63, 2^63), so the x86 out-of-range rule of f2i_x86 can never apply:
-// |a0| + |a1|*(len-1) + |a2|*(len-1)^2 < 2^62 bounds them (rounding moves a
-// prediction by a few ulps only).  NaN/inf models fail the comparison.
-template <int CODEC>
-__device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
-  const double L = __uint2double_rn(len ? len - 1 : 0);
-  double b = fabs(h.a0) + fabs(h.a1) * L;
-  if (CODEC == kPoly2) b += fabs(h.a2) * L * L;
-  return b < 4611686018427387904.0;
-}
-
-// Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
-// (raw u32 blocks included).  Each thread produces VEC consecutive values per
-// step and writes them with one 16-byte store.
-template <typename T, int CODEC, bool FAST, bool SMEM = false>
-__device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32, T *out,
-                                              uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
-  constexpr int S = sizeof(T);
-  constexpr int VEC = 16 / S;
-  const uint32_t l = raw ? 32u : h.l;
-  // words32 + body_bit/32: the body's first word (global payload or a staged copy in shared memory)
-  const uint32_t *bp = words32 + (h.body_bit >> 5);
-  const uint32_t bsh = (uint32_t)(h.body_bit & 31);
-  const uint32_t mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
-  const uint32_t sb = l ? l - 1 : 0, m1 = mask >> 1;
-  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
-    uint64_t v[VEC];
-#pragma unroll
-    for (int j = 0; j < VEC; ++j) {
-      const int32_t k = kv + j;
-      const uint32_t kk = k < (int32_t)lo ? lo : (uint32_t)k;  // values before lo are not stored
-      const uint32_t r = bsh + kk * l;
-      const uint32_t *p = bp + (r >> 5);
-      const uint32_t w0 = SMEM ? p[0] : __ldg(p), w1 = SMEM ? p[1] : __ldg(p + 1);
-      const uint32_t f = l ? (__funnelshift_r(w0, w1, r) & mask) : 0u;
-      if (raw) {
-        v[j] = f;
-      } else if (CODEC == kFor) {
-        v[j] = h.base + f;
-      } else {
-        const double pd = CODEC == kLinear ? pred_linear(h.a0, h.a1, kk)
-                                           : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
-        const int64_t pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
-        const uint32_t mag = f & m1;
-        const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
-        v[j] = (uint64_t)(pred + d);
-      }
-    }
-    const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
-    store_vals<T>(out, obase + kv, v, VEC, full);
-    if (!full) {
-#pragma unroll
-      for (int j = 0; j < VEC; ++j)
-        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
-    }
-  }
-}
-
-// ---- bulk / range decode ----------------------------------------------------
-// One CTA per block.  Each thread decodes VEC = 16/sizeof(T) consecutive values
-// per step from a three-word window of the packed body and writes them with one
-// 16-byte store.
-template <typename T, int CODEC>
-__device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) {
-  constexpr int S = sizeof(T);
-  constexpr uint32_t TB = 8u * S;
-  constexpr int VEC = 16 / S;
-  const uint64_t base = b * a.bs;
-  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
-  // values of this block inside [first, first+count)
-  const uint64_t r0 = a.first > base ? a.first : base, r1 = umin64(a.first + a.count, base + len);
-  if (r0 >= r1) return;
-  const uint32_t lo = (uint32_t)(r0 - base), hi = (uint32_t)(r1 - base);
-  T *out = reinterpret_cast<T *>(a.out);
-  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
-  const BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
-  const uint64_t obase = base - a.first;  // out index of block value 0
-
-  if (h.l == 126 || h.l == 127) {  // sentinel blocks (…_integer_template.h:152-170)
-    if (CODEC == kFor) { if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader); return; }
-    if (threadIdx.x == 0) {
-      const uint32_t cnt = h.l == 127 ? 1 : 2;
-      for (uint32_t k = lo; k < cnt && k < hi; ++k)
-        out[obase + k] = (T)load_field(words, h.body_bit + (uint64_t)k * TB, TB);
-    }
-    return;
-  }
-  if (h.l > TB) {
-    if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader);
-    return;
-  }
-  const bool raw = h.l == TB;
-
-  if (CODEC == kDelta && !raw) {
-    // Running sum: value k = x0 + sum_{i<k} signed(field_i) (mod 2^(8S)).
-    const DeltaChunk c = delta_chunk_start(words, h, len);
-    uint64_t run = c.run;
-    for (uint32_t k = c.k0; k < c.k1; ++k) {
-      if (k >= lo && k < hi) out[obase + k] = (T)run;
-      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-    }
-    return;
-  }
-
-  // First vector start so that out[obase + kv] is 16-byte aligned (out must be
-  // sizeof(T)-aligned); kv may start up to VEC-1 values before lo.
-  const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + obase + lo);
-  const int32_t kstart = (int32_t)lo - (int32_t)((oaddr & 15) / S);
-  const uint32_t l = raw ? TB : h.l;
-  if (l <= 32) {
-    // Narrow fields (every u32 block, u64 blocks with l <= 32): 32-bit field
-    // extraction; predictions converted without range checks when the block's
-    // model keeps every prediction inside int64 (decided once per block).
-    const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
-    const uint32_t *w32 = reinterpret_cast<const uint32_t *>(a.payload);
-    if (fast) decode_narrow<T, CODEC, true>(h, raw, w32, out, obase, lo, hi, kstart);
-    else decode_narrow<T, CODEC, false>(h, raw, w32, out, obase, lo, hi, kstart);
-    return;
-  }
-  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
-    uint64_t v[VEC];
-    const uint32_t kw = kv < (int32_t)lo ? lo : (uint32_t)kv;  // first value actually needed
-    const uint64_t bit0 = h.body_bit + (uint64_t)kw * l;
-    const uint64_t w = bit0 >> 6;
-    const uint64_t W0 = __ldg(words + w), W1 = __ldg(words + w + 1), W2 = __ldg(words + w + 2);
-    const uint32_t sh0 = (uint32_t)(bit0 & 63);
-#pragma unroll
-    for (int j = 0; j < VEC; ++j) {
-      const int32_t k = kv + j;
-      const uint32_t rel = sh0 + (uint32_t)(k - (int32_t)kw) * l;  // unused when k < kw
-      const uint32_t sh = rel & 63;
-      const uint64_t lo64 = rel < 64 ? W0 : (rel < 128 ? W1 : W2);
-      const uint64_t hi64 = rel < 64 ? W1 : W2;
-      const uint64_t f = funnel64(lo64, hi64, sh) & lowmask(l);
-      v[j] = raw ? f : value_from_field<CODEC, S>(h, (uint32_t)k, f);
-    }
-    const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
-    store_vals<T>(out, obase + kv, v, VEC, full);
-    if (!full) {
-#pragma unroll
-      for (int j = 0; j < VEC; ++j)
-        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
-    }
-  }
-}
 
 // Direct decode: one CTA per block of the range, everything read from global memory.
 template <typename T, int CODEC>
@@ -466,21 +203,6 @@ __global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_su
 }
 
 // ---- random access --------------------------------------------------------------
-// Value of one lookup from its block model and field (randomdecodeArray8 rules).
-template <int CODEC, int S>
-__device__ __forceinline__ uint64_t ra_value(const BlockHdr &h, uint32_t k, uint64_t f, uint32_t *error) {
-  constexpr uint32_t TB = 8u * S;
-  if (h.l == TB) return f;  // raw (…_integer_template.h:313-317)
-  if (h.l > TB) {           // sentinel / corrupt header: the reference's random access has no such case
-    atomicOr(error, kErrBadHeader);
-    return 0;
-  }
-  if (CODEC == kFor) return h.l ? h.base + f : h.base;
-  const double p = CODEC == kLinear ? pred_linear(h.a0, h.a1, k) : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
-  if (h.l) return apply_signed((uint64_t)f2i_x86(p), f, h.l);
-  return f2T_x86<S>(p);  // l == 0: (T)prediction directly (piecewise_fix_integer_template.h:334, poly :288)
-}
-
 // Batched random access: each thread keeps U lookups in flight (indices,
 // directory entries and payload words are each loaded for all U before any is
 // used), lookups i, i+G, i+2G, ... of one thread are strided by the grid so

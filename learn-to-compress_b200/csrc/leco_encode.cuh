@@ -1,0 +1,422 @@
+// leco_encode.cuh -- per-block encoder shared by the single-column kernels
+// (leco_encode.cu) and the persistent multi-column batch kernels (leco_batch.cu).
+//
+// Reference: Leco_int<T>::encodeArray8_int (piecewise_fix_integer_template.h:27-140),
+// FOR_int<T>::encodeArray8_int (FOR_integer_template.h:26-81),
+// Delta_int<T>::encodeArray8_int (delta_integer_template.h:26-87),
+// Leco_int_poly<T,2>::encodeArray8_int (poly_fix_integer_template.h:28-91),
+// packers write_delta_int_T / write_FOR_int_T (bit_write.h:257-390).
+#pragma once
+#include "leco_device.cuh"
+#include "leco_internal.h"
+
+namespace leco {
+
+constexpr uint64_t kFlagAgg = 1ull << 62, kFlagIncl = 2ull << 62, kValMask = (1ull << 62) - 1;
+constexpr uint32_t kSpinLimit = 1u << 22;  // x ~64-512 ns backoff: far above any real wait
+
+// Per-block model scratch: the sequential reference fit writes 3 doubles per block.
+struct EncodeArgs {
+  const void *values;
+  uint64_t n;
+  uint32_t bs;
+  uint64_t nb;
+  uint8_t *payload;
+  uint64_t payload_cap;
+  uint64_t *offsets;
+  leco_dir_entry *dir;
+  const double *seq_models;  // [nb*3] or null (exact fit in-kernel)
+  double polyX[10];          // X sums for full blocks [0..4] and for the tail block [5..9]
+  uint64_t *status;          // [nb] look-back words, zeroed
+  uint32_t *ticket;          // zeroed
+  uint32_t *error;           // error word
+};
+
+// Shared-memory layout helper.
+template <typename T>
+struct EncSmem {
+  T *vals;          // [bs] values, later residual magnitudes (linear / poly2)
+  uint32_t *signs;  // [bs/32 + 9] sign bits (one word per 32 values, rounded up to 256)
+  u128 *red;        // [33]
+  uint8_t *hdr;     // [32] header bytes
+  uint64_t *bcast;  // [8]
+};
+
+template <typename T>
+__device__ __forceinline__ EncSmem<T> enc_smem(uint8_t *base, uint32_t bs) {
+  EncSmem<T> s;
+  s.red = reinterpret_cast<u128 *>(base);                      // 33 * 16 = 528
+  s.bcast = reinterpret_cast<uint64_t *>(base + 528);          // 8 * 8 = 64
+  s.hdr = base + 592;                                          // 32
+  s.signs = reinterpret_cast<uint32_t *>(base + 624);          // (bs/32+9)*4
+  uint32_t soff = 624 + ((bs / 32 + 9) * 4 + 15) / 16 * 16;
+  s.vals = reinterpret_cast<T *>(base + soff);
+  return s;
+}
+__host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
+  return 624 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + bs * s;
+}
+
+// Decoupled look-back (single-pass prefix sum over block image sizes).  Run by
+// warp 0.  Returns the exclusive prefix; on a wait that exceeds the spin limit
+// sets kErrTimeout and returns ~0.
+__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error) {
+  const int lane = threadIdx.x & 31;
+  if (b == 0) {
+    if (lane == 0) st_relaxed(&status[0], kFlagIncl | my);
+    return 0;
+  }
+  if (lane == 0) st_relaxed(&status[b], kFlagAgg | my);
+  uint64_t excl = 0;
+  int64_t j = (int64_t)b - 1;
+  for (;;) {
+    int64_t idx = j - lane;
+    uint64_t v = kFlagIncl;  // lanes before block 0 read as "inclusive 0"
+    uint32_t spins = 0, ns = 64;
+    for (;;) {
+      if (idx >= 0) v = ld_relaxed(&status[idx]);
+      if (__all_sync(0xffffffffu, (v >> 62) != 0)) break;
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicOr(error, kErrTimeout);
+        return ~0ull;
+      }
+      __nanosleep(ns);
+      if (ns < 512) ns <<= 1;
+    }
+    uint32_t incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+    if (incl) {
+      int first = __ffs(incl) - 1;  // nearest predecessor with an inclusive prefix
+      uint64_t x = lane <= first ? (v & kValMask) : 0;
+      excl += warp_sum_u64(x);
+      break;
+    }
+    excl += warp_sum_u64(v & kValMask);
+    j -= 32;
+  }
+  if (lane == 0) st_relaxed(&status[b], kFlagIncl | (excl + my));
+  return excl;
+}
+
+// Image writer: writes image bytes [0, size) of a block to payload[goff...].
+// Image byte i < H is hdr[i]; byte i >= H is byte (i-H) of the LSB-first
+// concatenation of fields 0..n-1 (l bits each), zero past the last field.
+template <typename FieldFn>
+__device__ __forceinline__ uint64_t gather_bits(uint32_t p, uint32_t nbits, uint32_t l, uint32_t n, FieldFn field) {
+  uint32_t k = p / l, o = p - k * l;
+  u128 acc = k < n ? (u128)(field(k) >> o) : (u128)0;
+  uint32_t have = l - o;
+  ++k;
+  while (have < nbits) {
+    if (k < n) acc |= (u128)field(k) << have;
+    have += l;
+    ++k;
+  }
+  return (uint64_t)acc & lowmask(nbits);
+}
+
+template <typename FieldFn>
+__device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
+                                            const uint8_t *hdr, uint32_t l, uint32_t nfields, FieldFn field) {
+  const uint64_t gend = goff + size;
+  const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
+  const uint64_t body0 = goff + H;  // first body byte (global)
+  for (uint64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const uint64_t cb = c << 4;
+    if (cb >= body0 && cb + 16 <= gend && l) {
+      uint32_t p = (uint32_t)((cb - body0) * 8);
+      uint64_t lo = gather_bits(p, 64, l, nfields, field);
+      uint64_t hi = gather_bits(p + 64, 64, l, nfields, field);
+      *reinterpret_cast<ulonglong2 *>(payload + cb) = make_ulonglong2(lo, hi);
+    } else {
+      for (int j = 0; j < 16; ++j) {
+        uint64_t g = cb + j;
+        if (g < goff || g >= gend) continue;
+        uint64_t i = g - goff;
+        uint8_t byte;
+        if (i < H) byte = hdr[i];
+        else if (!l) byte = 0;
+        else byte = (uint8_t)gather_bits((uint32_t)((i - H) * 8), 8, l, nfields, field);
+        payload[g] = byte;
+      }
+    }
+  }
+}
+
+// Encodes block b of the column described by `a` with the whole CTA.  The
+// caller guarantees that every block of the column with a smaller index was
+// handed to a CTA that has already started (ticket order), which makes the
+// look-back wait finite.  smem_raw: enc_smem_bytes(a.bs, sizeof(T)) bytes.
+template <typename T, int CODEC>
+__device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  EncSmem<T> sm = enc_smem<T>(smem_raw, a.bs);
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  const T *src = reinterpret_cast<const T *>(a.values) + base;
+
+  // ---- stage the block ------------------------------------------------------
+  constexpr uint32_t V = 16 / S;
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    const uint32_t nvec = len / V;
+    for (uint32_t i = tid; i < nvec; i += nt)
+      reinterpret_cast<uint4 *>(sm.vals)[i] = __ldg(reinterpret_cast<const uint4 *>(src) + i);
+    for (uint32_t i = nvec * V + tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
+  } else {
+    for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
+  }
+  __syncthreads();
+
+  uint32_t l = 0;
+  double m0 = 0, m1 = 0, m2 = 0;  // model (theta0/theta1 or poly a0..a2)
+  uint64_t fbase = 0;             // FOR min / Delta first value
+  uint32_t H = Hdr<CODEC, S>::bytes;
+
+  if (CODEC == kLinear || CODEC == kPoly2) {
+    // ---- fit -----------------------------------------------------------------
+    if (a.seq_models) {
+      m0 = a.seq_models[b * 3 + 0];
+      m1 = a.seq_models[b * 3 + 1];
+      m2 = a.seq_models[b * 3 + 2];
+    } else {
+      u128 sy = 0, siy = 0, sqy = 0;
+      for (uint32_t i = tid; i < len; i += nt) {
+        uint64_t y = (uint64_t)sm.vals[i];
+        sy += y;
+        siy += (u128)y * i;
+        if (CODEC == kPoly2) sqy += (u128)y * ((uint64_t)i * i);
+      }
+      sy = block_reduce<0>(sy, sm.red);
+      siy = block_reduce<0>(siy, sm.red);
+      if (CODEC == kPoly2) sqy = block_reduce<0>(sqy, sm.red);
+      const double md = __uint2double_rn(len);
+      if (CODEC == kLinear) {
+        // lr_int_T::caltheta (lr.h:79-83) on exact moments
+        const uint64_t m = len;
+        const double sumx = __ull2double_rn(m * (m - 1) / 2);
+        const double sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
+        const double sumy = u128_to_double(sy), sumxy = u128_to_double(siy);
+        const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+        const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+        m1 = __ddiv_rn(ccc, xxx);
+        m0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(m1, sumx)), md);
+      } else {
+        const double *X = a.polyX + (len == a.bs ? 0 : 5);
+        double Y[3] = {u128_to_double(sy), u128_to_double(siy), u128_to_double(sqy)};
+        double c[3];
+        poly2_solve(X, Y, c);
+        m0 = c[0];
+        m1 = c[1];
+        m2 = c[2];
+      }
+    }
+    if (CODEC == kLinear) {
+      // ---- midpoint shift (piecewise_fix_integer_template.h:36-46) -----------
+      int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
+      for (uint32_t i = tid; i < len; i += nt) {
+        int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)f2i_x86(pred_linear(m0, m1, i)));
+        dmax = d > dmax ? d : dmax;
+        dmin = d < dmin ? d : dmin;
+      }
+      dmax = (int64_t)(uint64_t)block_reduce<3>((u128)(uint64_t)dmax, sm.red);
+      dmin = (int64_t)(uint64_t)block_reduce<4>((u128)(uint64_t)dmin, sm.red);
+      const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
+      m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
+    }
+    // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
+    uint64_t rmax = 0;
+    for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+      const uint32_t i = i0 + tid;
+      bool pos = false;
+      if (i < len) {
+        const uint64_t y = (uint64_t)sm.vals[i];
+        uint64_t r;
+        if (CODEC == kLinear) {
+          const int64_t pred = f2i_x86(pred_linear(m0, m1, i));
+          pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
+          r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+        } else {
+          const int64_t pred = f2i_x86(pred_poly2(m0, m1, m2, __uint2double_rn(i)));
+          pos = (int64_t)y > pred;
+          r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+        }
+        r &= (S == 8 ? ~0ull : 0xffffffffull);
+        sm.vals[i] = (T)r;
+        rmax = r > rmax ? r : rmax;
+      }
+      const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+      if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+    }
+    rmax = (uint64_t)block_reduce<1>((u128)rmax, sm.red);
+    l = rmax ? bits_of(rmax) + 1 : 0;
+    if (l > TB) l = TB;
+  } else if (CODEC == kFor) {
+    // ---- frame of reference (FOR_integer_template.h:26-52) --------------------
+    uint64_t mn = ~0ull, mx = 0;
+    for (uint32_t i = tid; i < len; i += nt) {
+      uint64_t y = (uint64_t)sm.vals[i];
+      mn = y < mn ? y : mn;
+      mx = y > mx ? y : mx;
+    }
+    mn = (uint64_t)block_reduce<2>((u128)mn, sm.red);
+    mx = (uint64_t)block_reduce<1>((u128)mx, sm.red);
+    fbase = mn;
+    m1 = __longlong_as_double((long long)mx);
+    l = bits_of(mx - mn);
+  } else {  // kDelta (delta_integer_template.h:34-66)
+    uint64_t rmax = 0;
+    for (uint32_t i = tid; i + 1 < len; i += nt) {
+      uint64_t x0 = (uint64_t)sm.vals[i], x1 = (uint64_t)sm.vals[i + 1];
+      uint64_t r = x1 > x0 ? x1 - x0 : x0 - x1;
+      rmax = r > rmax ? r : rmax;
+    }
+    rmax = (uint64_t)block_reduce<1>((u128)rmax, sm.red);
+    l = rmax ? bits_of(rmax) + 1 : 0;
+    if (l > TB) l = TB;
+    fbase = (uint64_t)sm.vals[0];
+  }
+  // A width of 8*sizeof(T)-1 is written raw: the reference's bulk decoders
+  // treat l >= 8*sizeof(T)-1 as raw (piecewise_fix_integer_template.h:171,
+  // FOR_integer_template.h:89, poly_fix_integer_template.h:121), so a packed
+  // block of that width would not decode there.  Delta has no such rule.
+  if (CODEC != kDelta && l == TB - 1) l = TB;
+  const bool raw = (l == TB);
+  if (raw) {  // residuals overwrote the values: restage them
+    __syncthreads();
+    for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
+  }
+  const uint64_t size = block_bytes<CODEC, S>(l, len);
+
+  // ---- offset by look-back ----------------------------------------------------
+  if (tid < 32) {
+    uint64_t excl = lookback_prefix(a.status, b, size, a.error);
+    if (tid == 0) sm.bcast[1] = excl;
+  }
+  // ---- header bytes ------------------------------------------------------------
+  if (tid == 0) {
+    sm.hdr[0] = (uint8_t)l;
+    if (raw) {
+      H = 1;
+    } else if (CODEC == kLinear || CODEC == kPoly2) {
+      uint64_t w0 = (uint64_t)__double_as_longlong(m0), w1 = (uint64_t)__double_as_longlong(m1),
+               w2 = (uint64_t)__double_as_longlong(m2);
+      for (int j = 0; j < 8; ++j) {
+        sm.hdr[1 + j] = (uint8_t)(w0 >> (8 * j));
+        sm.hdr[9 + j] = (uint8_t)(w1 >> (8 * j));
+        if (CODEC == kPoly2) sm.hdr[17 + j] = (uint8_t)(w2 >> (8 * j));
+      }
+    } else if (CODEC == kFor) {
+      uint64_t mx = (uint64_t)__double_as_longlong(m1);
+      for (int j = 0; j < S; ++j) {
+        sm.hdr[1 + j] = (uint8_t)(fbase >> (8 * j));
+        sm.hdr[1 + S + j] = (uint8_t)(mx >> (8 * j));
+      }
+    } else {
+      for (int j = 0; j < S; ++j) sm.hdr[1 + j] = (uint8_t)(fbase >> (8 * j));
+    }
+  }
+  __syncthreads();
+  const uint64_t goff = sm.bcast[1];
+  if (raw) H = 1;
+  if (goff == ~0ull) return;                       // look-back gave up (error word set)
+  if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {  // never write past the buffer
+    if (tid == 0) atomicOr(a.error, kErrCapacity);
+    return;
+  }
+
+  // ---- body ----------------------------------------------------------------------
+  const T *vals = sm.vals;
+  const uint32_t *signs = sm.signs;
+  if (raw) {
+    write_image(a.payload, goff, size, 1, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; });
+  } else if (CODEC == kLinear || CODEC == kPoly2) {
+    const uint32_t sb = l ? l - 1 : 0;
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
+      return (uint64_t)vals[k] | ((uint64_t)((signs[k >> 5] >> (k & 31)) & 1u) << sb);
+    });
+  } else if (CODEC == kFor) {
+    const uint64_t mnv = fbase;
+    const uint64_t tm = S == 8 ? ~0ull : 0xffffffffull;
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t { return ((uint64_t)vals[k] - mnv) & tm; });
+  } else {
+    const uint32_t sb = l ? l - 1 : 0;
+    const uint32_t last = len - 1;
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
+      if (k >= last) return 0;  // the reference writes an out-of-bounds field here (delta_integer_template.h:83)
+      uint64_t x0 = (uint64_t)vals[k], x1 = (uint64_t)vals[k + 1];
+      bool pos = x1 > x0;
+      return (pos ? x1 - x0 : x0 - x1) | ((uint64_t)pos << sb);
+    });
+  }
+
+  // ---- offsets and directory -------------------------------------------------------
+  if (tid == 0) {
+    a.offsets[b] = goff;
+    if (b == a.nb - 1) a.offsets[a.nb] = goff + size;
+    if (a.dir) {
+      leco_dir_entry e;
+      uint64_t body_bit = (goff + H) * 8;
+      e.word0 = body_bit | ((uint64_t)l << 56) | ((uint64_t)CODEC << 48);
+      if (CODEC == kLinear || CODEC == kPoly2) {
+        e.a0 = m0; e.a1 = m1; e.a2 = m2;
+      } else {
+        e.a0 = __longlong_as_double((long long)fbase);
+        e.a1 = 0; e.a2 = 0;
+      }
+      a.dir[b] = e;
+    }
+  }
+}
+
+// ---- sequential reference fits (LECO_FIT_REFERENCE) ---------------------------
+// One thread per block runs the reference's own FP64 loop, so the model is
+// bit-identical to lr_int_T::caltheta (lr.h:66-85) or to the Y sums of
+// polynomial_regression_iter (polynomial_regression_internals.hpp:129-137).
+struct PolyX {
+  double x[10];
+};
+
+template <typename T, int CODEC>
+__device__ __forceinline__ void seq_fit_block(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t b,
+                                              const double *polyX, double *__restrict__ models) {
+  const uint64_t base = b * bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)bs, n - base);
+  const T *y = values + base;
+  if (CODEC == kLinear) {
+    double sumx = 0, sumy = 0, sumxx = 0, sumxy = 0;
+#pragma unroll 4
+    for (uint32_t i = 0; i < len; ++i) {
+      const double di = __uint2double_rn(i), yi = to_double<T>(__ldg(y + i));
+      sumx = __dadd_rn(sumx, di);
+      sumy = __dadd_rn(sumy, yi);
+      sumxx = __dadd_rn(sumxx, __dmul_rn(di, di));
+      sumxy = __dadd_rn(sumxy, __dmul_rn(di, yi));
+    }
+    const double md = __uint2double_rn(len);
+    const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+    const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+    const double t1 = __ddiv_rn(ccc, xxx);
+    const double t0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(t1, sumx)), md);
+    models[b * 3 + 0] = t0;
+    models[b * 3 + 1] = t1;
+    models[b * 3 + 2] = 0.0;
+  } else {
+    double Y0 = 0, Y1 = 0, Y2 = 0;
+#pragma unroll 4
+    for (uint32_t i = 0; i < len; ++i) {
+      const double di = __uint2double_rn(i), yi = to_double<T>(__ldg(y + i));
+      Y0 = __dadd_rn(Y0, __dmul_rn(1.0, yi));
+      Y1 = __dadd_rn(Y1, __dmul_rn(di, yi));
+      Y2 = __dadd_rn(Y2, __dmul_rn(__dmul_rn(di, di), yi));
+    }
+    const double *X = polyX + (len == bs ? 0 : 5);
+    double Y[3] = {Y0, Y1, Y2}, c[3];
+    poly2_solve(X, Y, c);
+    models[b * 3 + 0] = c[0];
+    models[b * 3 + 1] = c[1];
+    models[b * 3 + 2] = c[2];
+  }
+}
+
+}  // namespace leco

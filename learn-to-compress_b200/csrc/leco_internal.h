@@ -59,6 +59,9 @@ int launch_build_dir(int codec, int s, const uint8_t *payload, const uint64_t *o
 // -ffp-contract=off.
 void poly2_x_sums(uint32_t N, double X[5]);
 
+// Device address of the library's error word on the current device.
+int device_error_word(uint32_t **p);
+
 // Records `msg` as this thread's leco_last_error() message and returns `code`.
 int record_error(int code, const std::string &msg);
 
