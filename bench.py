@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch"],
+                    help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
+                         "the persistent batch engine vs per-column launches")
+    ap.add_argument("--ncols", type=int, default=4096)
+    ap.add_argument("--fit", default="reference", choices=["reference", "exact"])
     return ap.parse_args()
 
 
@@ -210,11 +215,99 @@ def run_reference(args, world, rank):
     print(json.dumps(out), flush=True)
 
 
+def run_batch(args, world, rank, local):
+    """4096 columns, lengths log-uniform in [1K, 4M], 50 % u32 / 50 % u64, four
+    data families, codec LeCo-fix / Delta-fix / FOR per column, block size from
+    the committed autotune table.  Times one encode+decode pass three ways on
+    the same columns: one leco_encode + leco_decode call per column, the
+    persistent batch kernels, and the batch pass replayed as a CUDA graph."""
+    import math
+
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import autotune, workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(3 + rank)
+    fams = autotune.FAMILIES
+    cols, raw, shapes = [], 0, {}
+    for i in range(args.ncols):
+        n = int(math.exp(rng.uniform(math.log(1000), math.log(4_000_000))))
+        s = 4 if rng.random() < 0.5 else 8
+        fam = fams[int(rng.integers(4))]
+        codec = (lc.LINEAR, lc.DELTA, lc.FOR)[int(rng.integers(3))]
+        x = workloads.families(n, fam, s, rng)
+        bs = autotune.pick_block_size(codec, s, n, autotune.classify(x))
+        shapes[bs] = shapes.get(bs, 0) + 1
+        cols.append((torch.from_numpy(x.view(np.int64 if s == 8 else np.int32)).to(dev), codec, bs))
+        raw += n * s
+    fit = lc.FIT_EXACT if args.fit == "exact" else lc.FIT_REFERENCE
+    b = lc.Batch(cols, fit_mode=fit)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def verify():
+        lc.check()
+        for (x, _, _), c in zip(cols, b.cols):
+            assert torch.equal(c.out, x), "batch decode mismatch"
+
+    per_col = lambda: (b.encode_per_column(), b.decode_per_column())
+    batch = lambda: (b.encode(), b.decode())
+    graph = lambda: b.run_graph(3)
+    for fn in (per_col, batch, graph):
+        for _ in range(max(1, args.warmup)):
+            fn()
+    torch.cuda.synchronize()
+    verify()
+    k = max(3, args.steps // 5)
+    t_col = timed(per_col, k)
+    verify()
+    t_batch = timed(batch, k)
+    verify()
+    with ClockSampler(local) as clk:
+        t_graph = timed(graph, k)
+    verify()
+    t_dec_col = timed(b.decode_per_column, k)
+    t_dec_batch = timed(b.decode, k)
+    comp = sum(c.nbytes for c in b.cols)
+    if rank == 0:
+        line = {"metric": "batched persistent encode+decode pass vs per-column launches (speed-up)",
+                "value": round(t_col / t_graph, 3), "unit": "x", "n_gpus": world, "steps": k, "warmup": args.warmup,
+                "ms_per_step": round(t_graph, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u32+u64", "data": "synthetic",
+                "config": {"workload": f"{args.ncols} columns, lengths log-uniform 1K-4M, 50% u32/50% u64, "
+                                       "families linear/step/walk/uniform, codecs LeCo/Delta/FOR, autotuned block size",
+                           "raw_bytes": raw, "blocks": b.total_blocks, "fit": args.fit,
+                           "block_sizes": {str(k_): v for k_, v in sorted(shapes.items())}},
+                "ms_per_pass": {"per_column_launches": round(t_col, 3), "persistent": round(t_batch, 3),
+                                "persistent_graph": round(t_graph, 3)},
+                "decode_ms": {"per_column_launches": round(t_dec_col, 3), "persistent": round(t_dec_batch, 3)},
+                "pass_gbs_graph": round(2 * raw / (t_graph / 1e3) / 1e9, 1),
+                "compressed_ratio": round(comp / raw, 5), "gpu_launches_per_pass": 3 + (1 if b.fit_mode == 0 else 0),
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "batch":
+        run_batch(args, world, rank, local)
         return
 
     import torch

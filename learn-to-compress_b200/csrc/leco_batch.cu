@@ -2,13 +2,14 @@
 // uint32/uint64 and mixed LeCo/FOR/Delta/poly codecs, encoded and decoded by
 // one persistent launch per pass.
 //
-// Work queue: the batch's blocks are numbered column by column (block_prefix[c]
-// = number of blocks before column c).  Every CTA of a persistent grid takes the
-// next number from an atomic ticket, finds its column by binary search over
-// block_prefix and runs the per-block encoder or decoder for that column's codec
-// and value type.  Tickets are handed out in order and every CTA of the grid is
-// resident, so the encoder's per-column look-back (byte offsets) only ever waits
-// on blocks that are already being processed.
+// Work queue: the batch's blocks are listed column by column as work items --
+// one block of a column with large blocks, or up to eight consecutive blocks of
+// a column with small blocks (<= 512 values; one warp each).  Every CTA of a
+// persistent grid takes the next item from an atomic ticket and runs the
+// per-block encoder or decoder for that column's codec and value type.  Items
+// are handed out in order and every CTA of the grid is resident, so the
+// encoder's per-column look-back (byte offsets) only ever waits on blocks that
+// are already being processed.
 //
 // The reference has no counterpart: its drivers loop over blocks of one column
 // (experiments/leco_int_fix_template.cpp:111-127, :145-153).  The per-column
@@ -69,8 +70,11 @@ __device__ __forceinline__ uint32_t find_column(const uint64_t *__restrict__ pre
 
 struct BatchArgs {
   const DevCol *cols;
-  const uint64_t *prefix;  // [ncols + 1]
+  const uint64_t *prefix;  // [ncols + 1] blocks before each column
+  const uint64_t *items;   // [nitems] (column << 32) | first block
   uint32_t ncols;
+  uint64_t nitems;
+  uint32_t warp_slice;     // shared-memory bytes per warp for small-block columns
   uint64_t total;          // blocks in the batch
   uint64_t *status;        // [total] look-back words (zeroed per encode pass)
   unsigned long long *ticket;  // zeroed per pass
@@ -78,7 +82,7 @@ struct BatchArgs {
   uint32_t *error;
 };
 
-template <typename T, int CODEC>
+template <typename T, int CODEC, int G>
 __device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b,
                                                  uint8_t *smem) {
   EncodeArgs a;
@@ -96,13 +100,26 @@ __device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCo
   a.status = B.status + p0;
   a.ticket = nullptr;
   a.error = B.error;
-  encode_block<T, CODEC>(a, b, smem);
+  encode_block<T, CODEC, G>(a, b, smem);
+}
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_encode_cta(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
+  batch_encode_one<T, CODEC, 256>(B, c, ci, b, smem);
+}
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_encode_warp(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
+  batch_encode_one<T, CODEC, 32>(B, c, ci, b, smem);
 }
 
 template <typename T, int CODEC>
-__device__ __forceinline__ void batch_decode_one(const BatchArgs &B, const DevCol &c, uint64_t b) {
+__device__ __forceinline__ void batch_decode_cta(const BatchArgs &B, const DevCol &c, uint64_t b) {
   DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
-  decode_block<T, CODEC>(a, b);
+  decode_block<T, CODEC, 256>(a, b);
+}
+template <typename T, int CODEC>
+__device__ __forceinline__ void batch_decode_warp(const BatchArgs &B, const DevCol &c, uint64_t b) {
+  DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
+  decode_block<T, CODEC, 32>(a, b);
 }
 
 template <typename T, int CODEC>
@@ -110,37 +127,51 @@ __device__ __forceinline__ void batch_seq_one(const DevCol &c, uint64_t b, doubl
   seq_fit_block<T, CODEC>(reinterpret_cast<const T *>(c.values), c.n, c.bs, b, c.polyX, models);
 }
 
-// Persistent encode: one ticket = one block of some column.
+// Persistent encode: one ticket = one work item.
 __global__ void __launch_bounds__(256) batch_encode_kernel(BatchArgs B) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ unsigned long long item;
   for (;;) {
     if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
     __syncthreads();
-    const uint64_t gb = item;
+    const uint64_t it = item;
     __syncthreads();
-    if (gb >= B.total) break;
-    const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+    if (it >= B.nitems) break;
+    const uint64_t e = __ldg(B.items + it);
+    const uint32_t ci = (uint32_t)(e >> 32);
+    const uint64_t b0 = e & 0xffffffffull;
     const DevCol &c = B.cols[ci];
-    const uint64_t b = gb - __ldg(B.prefix + ci);
-    LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_one, B, c, ci, b, smem);
-    __syncthreads();  // shared memory is reused by the next block
+    if (c.bs <= kWarpBlock) {
+      const uint32_t w = threadIdx.x >> 5;
+      const uint64_t b = b0 + w;
+      if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci))
+        LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_warp, B, c, ci, b, smem + (size_t)w * B.warp_slice);
+    } else {
+      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_cta, B, c, ci, b0, smem);
+    }
+    __syncthreads();  // shared memory is reused by the next item
   }
 }
 
-// Persistent decode: one ticket = one block of some column.
+// Persistent decode: one ticket = one work item.
 __global__ void __launch_bounds__(256) batch_decode_kernel(BatchArgs B) {
   __shared__ unsigned long long item;
   for (;;) {
     if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
     __syncthreads();
-    const uint64_t gb = item;
+    const uint64_t it = item;
     __syncthreads();
-    if (gb >= B.total) break;
-    const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+    if (it >= B.nitems) break;
+    const uint64_t e = __ldg(B.items + it);
+    const uint32_t ci = (uint32_t)(e >> 32);
+    const uint64_t b0 = e & 0xffffffffull;
     const DevCol &c = B.cols[ci];
-    const uint64_t b = gb - __ldg(B.prefix + ci);
-    LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_one, B, c, b);
+    if (c.bs <= kWarpBlock) {
+      const uint64_t b = b0 + (threadIdx.x >> 5);
+      if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci)) LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_warp, B, c, b);
+    } else {
+      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_cta, B, c, b0);
+    }
   }
 }
 
@@ -167,6 +198,9 @@ struct leco_batch {
   int device = 0;
   DevCol *d_cols = nullptr;
   uint64_t *d_prefix = nullptr;
+  uint64_t *d_items = nullptr;
+  uint64_t nitems = 0;
+  uint32_t warp_slice = 0;
   uint8_t *d_ws = nullptr;  // status [total] | ticket | models [total*3]
   uint64_t ws_bytes = 0, status_bytes = 0, models_off = 0;
   uint32_t enc_smem = 0;
@@ -190,6 +224,9 @@ BatchArgs args_of(const leco_batch *b, uint32_t *err) {
   BatchArgs B;
   B.cols = b->d_cols;
   B.prefix = b->d_prefix;
+  B.items = b->d_items;
+  B.nitems = b->nitems;
+  B.warp_slice = b->warp_slice;
   B.ncols = (uint32_t)b->cols.size();
   B.total = b->prefix.back();
   B.status = reinterpret_cast<uint64_t *>(b->d_ws);
@@ -242,8 +279,19 @@ int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mo
       poly2_x_sums((uint32_t)std::min<uint64_t>(c.n, c.block_size), d.polyX);
       poly2_x_sums((uint32_t)(c.n - (nb - 1) * c.block_size), d.polyX + 5);
     }
-    max_smem = std::max(max_smem, enc_smem_bytes(c.block_size, (uint32_t)c.dtype));
+    const uint32_t sm = enc_smem_bytes(c.block_size, (uint32_t)c.dtype);
+    if (c.block_size <= kWarpBlock) b->warp_slice = std::max(b->warp_slice, (sm + 15) / 16 * 16);
+    else max_smem = std::max(max_smem, sm);
   }
+  max_smem = std::max(max_smem, 8 * b->warp_slice);
+  // work items: (column << 32) | first block; eight blocks per item for small-block columns
+  std::vector<uint64_t> items;
+  for (uint32_t i = 0; i < ncols; ++i) {
+    const uint64_t nb = leco_num_blocks(h_cols[i].n, h_cols[i].block_size);
+    const uint64_t step = h_cols[i].block_size <= kWarpBlock ? 8 : 1;
+    for (uint64_t blk = 0; blk < nb; blk += step) items.push_back(((uint64_t)i << 32) | blk);
+  }
+  b->nitems = items.size();
   b->prefix[ncols] = total;
   if (total > 0xffffffffull) {
     delete b;
@@ -258,6 +306,8 @@ int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mo
   if (e == cudaSuccess) e = cudaMalloc(&b->d_ws, b->ws_bytes);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_cols, dc.data(), ncols * sizeof(DevCol), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, b->prefix.data(), (ncols + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(uint64_t));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(uint64_t), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && leco::device_error_word(&b->err)) e = cudaErrorUnknown;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess && max_smem > 48 * 1024)
@@ -272,8 +322,8 @@ int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mo
                 std::string("leco_batch_create: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "no resident CTA fits"));
   }
   // every CTA of the persistent grid must be resident (the look-back waits on them)
-  b->enc_grid = (int)std::min<uint64_t>(total, (uint64_t)sms * per_enc);
-  b->dec_grid = (int)std::min<uint64_t>(total, (uint64_t)sms * per_dec);
+  b->enc_grid = (int)std::min<uint64_t>(b->nitems, (uint64_t)sms * per_enc);
+  b->dec_grid = (int)std::min<uint64_t>(b->nitems, (uint64_t)sms * per_dec);
   *out = b;
   return LECO_OK;
 }
@@ -285,6 +335,7 @@ int leco_batch_destroy(leco_batch *b) {
   if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
   if (b->d_cols) cudaFree(b->d_cols);
   if (b->d_prefix) cudaFree(b->d_prefix);
+  if (b->d_items) cudaFree(b->d_items);
   if (b->d_ws) cudaFree(b->d_ws);
   delete b;
   return LECO_OK;

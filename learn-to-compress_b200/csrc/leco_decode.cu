@@ -25,6 +25,13 @@ __global__ void __launch_bounds__(256) decode_kernel(DecodeLaunch a) {
   decode_block<T, CODEC>(a, a.first / a.bs + blockIdx.x);
 }
 
+// Small blocks: one warp per block, eight blocks per CTA.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) decode_kernel_warp(DecodeLaunch a, uint64_t nblk) {
+  const uint64_t i = (uint64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (i < nblk) decode_block<T, CODEC, 32>(a, a.first / a.bs + i);
+}
+
 // ---- TMA-staged persistent decode --------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
@@ -185,7 +192,7 @@ __global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_su
   }
   const bool raw = h.l == TB;
   if (CODEC == kDelta && !raw) {
-    const DeltaChunk c = delta_chunk_start(words, h, len);
+    const DeltaChunk c = delta_chunk_start<256>(words, h, len);
     uint64_t run = c.run;
     for (uint32_t k = c.k0; k < c.k1; ++k) {
       acc += run & tmask;
@@ -360,9 +367,10 @@ static void run_decode(const DecodeLaunch &L, cudaStream_t st) {
   const uint64_t b0 = L.first / L.bs, b1 = (L.first + L.count - 1) / L.bs;
   const uint64_t nblk = b1 - b0 + 1;
   const bool staged = L.first == 0 && L.count == L.n && (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 &&
-                      CODEC != kDelta && nblk >= 1024 && staged_decode_enabled();
+                      CODEC != kDelta && nblk >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
   if (!staged) {
-    decode_kernel<T, CODEC><<<(unsigned)nblk, 256, 0, st>>>(L);
+    if (L.bs <= kWarpBlock) decode_kernel_warp<T, CODEC><<<(unsigned)((nblk + 7) / 8), 256, 0, st>>>(L, nblk);
+    else decode_kernel<T, CODEC><<<(unsigned)nblk, 256, 0, st>>>(L);
     return;
   }
   int dev = 0, sms = 148, per_sm = 1;

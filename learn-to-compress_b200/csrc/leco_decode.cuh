@@ -39,16 +39,9 @@ __device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ pay
 }
 
 template <int CODEC, int S>
-__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b, uint64_t pol = 0) {
+__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b) {
   const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
-  ulonglong2 q0, q1;
-  if (pol) {
-    q0 = ldg_v2_hint(p, pol);
-    q1 = ldg_v2_hint(p + 1, pol);
-  } else {
-    q0 = __ldg(p);
-    q1 = __ldg(p + 1);
-  }
+  const ulonglong2 q0 = __ldg(p), q1 = __ldg(p + 1);
   BlockHdr h;
   h.body_bit = q0.x & ((1ull << 48) - 1);
   h.l = (uint32_t)(q0.x >> 56);
@@ -76,9 +69,10 @@ struct DeltaChunk {
   uint32_t k0, k1;
   uint64_t run;  // decoded value k0 (mod 2^64)
 };
+template <int G>
 __device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len) {
   __shared__ uint64_t wsum[32];
-  const uint32_t nt = blockDim.x, tid = threadIdx.x;
+  const uint32_t nt = group_size<G>(), tid = group_rank<G>();
   const uint32_t chunk = (len + nt - 1) / nt;
   DeltaChunk c;
   c.k0 = min(len, tid * chunk);
@@ -92,6 +86,10 @@ __device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restri
   for (int d = 1; d < 32; d <<= 1) {
     uint64_t y = __shfl_up_sync(0xffffffffu, incl, d);
     if (lane >= d) incl += y;
+  }
+  if (G == 32) {  // one warp owns the block: the warp scan is the whole scan
+    c.run = h.base + (incl - local);
+    return c;
   }
   if (lane == 31) wsum[warp] = incl;
   __syncthreads();
@@ -136,7 +134,7 @@ __device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
 // Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
 // (raw u32 blocks included).  Each thread produces VEC consecutive values per
 // step and writes them with one 16-byte store.
-template <typename T, int CODEC, bool FAST, bool SMEM = false>
+template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256>
 __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32, T *out,
                                               uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
   constexpr int S = sizeof(T);
@@ -147,7 +145,7 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
   const uint32_t bsh = (uint32_t)(h.body_bit & 31);
   const uint32_t mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
   const uint32_t sb = l ? l - 1 : 0, m1 = mask >> 1;
-  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
+  for (int32_t kv = kstart + (int32_t)group_rank<G>() * VEC; kv < (int32_t)hi; kv += (int32_t)group_size<G>() * VEC) {
     uint64_t v[VEC];
 #pragma unroll
     for (int j = 0; j < VEC; ++j) {
@@ -184,8 +182,11 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
 // One CTA per block.  Each thread decodes VEC = 16/sizeof(T) consecutive values
 // per step from a three-word window of the packed body and writes them with one
 // 16-byte store.
-template <typename T, int CODEC>
+// Decodes the values of block b inside [a.first, a.first + a.count) with one
+// thread group: the whole CTA (G = 256) or one warp (G = 32, small blocks).
+template <typename T, int CODEC, int G = 256>
 __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) {
+  const uint32_t rank = group_rank<G>();
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   constexpr int VEC = 16 / S;
@@ -201,8 +202,8 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   const uint64_t obase = base - a.first;  // out index of block value 0
 
   if (h.l == 126 || h.l == 127) {  // sentinel blocks (…_integer_template.h:152-170)
-    if (CODEC == kFor) { if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader); return; }
-    if (threadIdx.x == 0) {
+    if (CODEC == kFor) { if (rank == 0) atomicOr(a.error, kErrBadHeader); return; }
+    if (rank == 0) {
       const uint32_t cnt = h.l == 127 ? 1 : 2;
       for (uint32_t k = lo; k < cnt && k < hi; ++k)
         out[obase + k] = (T)load_field(words, h.body_bit + (uint64_t)k * TB, TB);
@@ -210,14 +211,14 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
     return;
   }
   if (h.l > TB) {
-    if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader);
+    if (rank == 0) atomicOr(a.error, kErrBadHeader);
     return;
   }
   const bool raw = h.l == TB;
 
   if (CODEC == kDelta && !raw) {
     // Running sum: value k = x0 + sum_{i<k} signed(field_i) (mod 2^(8S)).
-    const DeltaChunk c = delta_chunk_start(words, h, len);
+    const DeltaChunk c = delta_chunk_start<G>(words, h, len);
     uint64_t run = c.run;
     for (uint32_t k = c.k0; k < c.k1; ++k) {
       if (k >= lo && k < hi) out[obase + k] = (T)run;
@@ -237,11 +238,11 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
     // model keeps every prediction inside int64 (decided once per block).
     const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
     const uint32_t *w32 = reinterpret_cast<const uint32_t *>(a.payload);
-    if (fast) decode_narrow<T, CODEC, true>(h, raw, w32, out, obase, lo, hi, kstart);
-    else decode_narrow<T, CODEC, false>(h, raw, w32, out, obase, lo, hi, kstart);
+    if (fast) decode_narrow<T, CODEC, true, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
+    else decode_narrow<T, CODEC, false, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
     return;
   }
-  for (int32_t kv = kstart + (int32_t)threadIdx.x * VEC; kv < (int32_t)hi; kv += (int32_t)blockDim.x * VEC) {
+  for (int32_t kv = kstart + (int32_t)rank * VEC; kv < (int32_t)hi; kv += (int32_t)group_size<G>() * VEC) {
     uint64_t v[VEC];
     const uint32_t kw = kv < (int32_t)lo ? lo : (uint32_t)kv;  // first value actually needed
     const uint64_t bit0 = h.body_bit + (uint64_t)kw * l;

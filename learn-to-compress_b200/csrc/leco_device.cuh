@@ -18,6 +18,10 @@ typedef __int128 i128;
 
 constexpr int kLinear = 0, kFor = 1, kDelta = 2, kPoly2 = 3, kVarlen = 4;
 
+// Blocks of at most this many values are encoded/decoded by one warp (eight
+// per CTA) instead of a whole CTA.
+constexpr uint32_t kWarpBlock = 512;
+
 // Error word bits (device error word, read by leco_check).
 constexpr uint32_t kErrBadIndex = 1u, kErrBadHeader = 2u, kErrTimeout = 4u, kErrCapacity = 8u;
 
@@ -190,29 +194,30 @@ __device__ __forceinline__ u128 block_reduce(u128 v, u128 *red) {
   return red[32];
 }
 
-// ---- L2 eviction-priority hints ---------------------------------------------
-// Random access streams gigabytes of random payload sectors through L2; these
-// keep the small, hot block directory resident (evict_last) and let the
-// streaming index/output traffic go first (evict_first).
-__device__ __forceinline__ uint64_t l2_policy_evict_last() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
+// ---- thread groups ----------------------------------------------------------
+// A block of values is processed either by a whole CTA (G = CTA size) or by one
+// warp (G = 32, several small blocks per CTA).  These helpers give the rank in
+// the group, synchronise it and reduce over it.
+template <int G>
+__device__ __forceinline__ uint32_t group_rank() { return G == 32 ? (threadIdx.x & 31) : threadIdx.x; }
+template <int G>
+__device__ __forceinline__ uint32_t group_size() { return G == 32 ? 32u : blockDim.x; }
+template <int G>
+__device__ __forceinline__ void group_sync() {
+  if (G == 32) __syncwarp();
+  else __syncthreads();
 }
-__device__ __forceinline__ uint64_t l2_policy_evict_first() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ ulonglong2 ldg_v2_hint(const void *ptr, uint64_t pol) {
-  ulonglong2 v;
-  asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(ptr), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ uint64_t ldg_u64_hint(const void *ptr, uint64_t pol) {
-  uint64_t v;
-  asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(ptr), "l"(pol));
-  return v;
+template <int OP, int G>
+__device__ __forceinline__ u128 group_reduce(u128 v, u128 *red) {
+  if (G != 32) return block_reduce<OP>(v, red);
+  switch (OP) {
+    case 0: return warp_sum_u128(v);
+    case 1: return warp_max_u64((uint64_t)v);
+    case 2: return warp_min_u64((uint64_t)v);
+    case 3: return (u128)(uint64_t)warp_max_i64((int64_t)(uint64_t)v);
+    case 4: return (u128)(uint64_t)warp_min_i64((int64_t)(uint64_t)v);
+    default: return warp_sum_u64((uint64_t)v);
+  }
 }
 
 // ---- relaxed global word access for the look-back scan ----------------------

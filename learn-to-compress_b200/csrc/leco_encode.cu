@@ -31,6 +31,19 @@ __global__ void __launch_bounds__(256) encode_kernel(EncodeArgs a) {
   encode_block<T, CODEC>(a, b, smem_raw);
 }
 
+// Small blocks: one warp per block, eight blocks per CTA, each warp with its
+// own slice of shared memory and its own ticket.
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) encode_kernel_warp(EncodeArgs a, uint32_t slice) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t t = 0;
+  if (lane == 0) t = atomicAdd(a.ticket, 1u);
+  const uint64_t b = __shfl_sync(0xffffffffu, t, 0);
+  if (b >= a.nb) return;
+  encode_block<T, CODEC, 32>(a, b, smem_raw + (size_t)w * slice);
+}
+
 template <typename T, int CODEC>
 __global__ void __launch_bounds__(128) seq_fit_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t nb,
                                                        PolyX px, double *__restrict__ models) {
@@ -55,10 +68,14 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
     a.seq_models = L.seq_models;
   }
   const uint32_t smem = enc_smem_bytes(L.bs, sizeof(T));
+  if (L.bs <= kWarpBlock) {
+    const uint32_t slice = (smem + 15) / 16 * 16;
+    encode_kernel_warp<T, CODEC><<<(unsigned)((L.nb + 7) / 8), 256, 8 * slice, st>>>(a, slice);
+    return 0;
+  }
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(encode_kernel<T, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const uint32_t threads = L.bs >= 256 ? 256 : ((L.bs + 31) / 32) * 32;
-  encode_kernel<T, CODEC><<<(unsigned)L.nb, threads, smem, st>>>(a);
+  encode_kernel<T, CODEC><<<(unsigned)L.nb, 256, smem, st>>>(a);
   return 0;
 }
 

@@ -116,11 +116,12 @@ __device__ __forceinline__ uint64_t gather_bits(uint32_t p, uint32_t nbits, uint
 
 template <typename FieldFn>
 __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
-                                            const uint8_t *hdr, uint32_t l, uint32_t nfields, FieldFn field) {
+                                            const uint8_t *hdr, uint32_t l, uint32_t nfields, FieldFn field,
+                                            uint32_t rank, uint32_t nthreads) {
   const uint64_t gend = goff + size;
   const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
   const uint64_t body0 = goff + H;  // first body byte (global)
-  for (uint64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+  for (uint64_t c = c0 + rank; c < c1; c += nthreads) {
     const uint64_t cb = c << 4;
     if (cb >= body0 && cb + 16 <= gend && l) {
       uint32_t p = (uint32_t)((cb - body0) * 8);
@@ -142,16 +143,18 @@ __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uin
   }
 }
 
-// Encodes block b of the column described by `a` with the whole CTA.  The
-// caller guarantees that every block of the column with a smaller index was
-// handed to a CTA that has already started (ticket order), which makes the
-// look-back wait finite.  smem_raw: enc_smem_bytes(a.bs, sizeof(T)) bytes.
-template <typename T, int CODEC>
+// Encodes block b of the column described by `a` with one thread group: the
+// whole CTA (G = 256) or one warp (G = 32, for small blocks).  The caller
+// guarantees that every block of the column with a smaller index was handed
+// to a group that has already started (ticket order), which makes the
+// look-back wait finite.  smem_raw: enc_smem_bytes(a.bs, sizeof(T)) bytes
+// owned by this group.
+template <typename T, int CODEC, int G = 256>
 __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   EncSmem<T> sm = enc_smem<T>(smem_raw, a.bs);
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t tid = group_rank<G>(), nt = group_size<G>();
   const uint64_t base = b * a.bs;
   const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
   const T *src = reinterpret_cast<const T *>(a.values) + base;
@@ -166,7 +169,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   } else {
     for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
   }
-  __syncthreads();
+  group_sync<G>();
 
   uint32_t l = 0;
   double m0 = 0, m1 = 0, m2 = 0;  // model (theta0/theta1 or poly a0..a2)
@@ -187,9 +190,9 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         siy += (u128)y * i;
         if (CODEC == kPoly2) sqy += (u128)y * ((uint64_t)i * i);
       }
-      sy = block_reduce<0>(sy, sm.red);
-      siy = block_reduce<0>(siy, sm.red);
-      if (CODEC == kPoly2) sqy = block_reduce<0>(sqy, sm.red);
+      sy = group_reduce<0, G>(sy, sm.red);
+      siy = group_reduce<0, G>(siy, sm.red);
+      if (CODEC == kPoly2) sqy = group_reduce<0, G>(sqy, sm.red);
       const double md = __uint2double_rn(len);
       if (CODEC == kLinear) {
         // lr_int_T::caltheta (lr.h:79-83) on exact moments
@@ -219,8 +222,8 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         dmax = d > dmax ? d : dmax;
         dmin = d < dmin ? d : dmin;
       }
-      dmax = (int64_t)(uint64_t)block_reduce<3>((u128)(uint64_t)dmax, sm.red);
-      dmin = (int64_t)(uint64_t)block_reduce<4>((u128)(uint64_t)dmin, sm.red);
+      dmax = (int64_t)(uint64_t)group_reduce<3, G>((u128)(uint64_t)dmax, sm.red);
+      dmin = (int64_t)(uint64_t)group_reduce<4, G>((u128)(uint64_t)dmin, sm.red);
       const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
       m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
     }
@@ -248,7 +251,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
       if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
     }
-    rmax = (uint64_t)block_reduce<1>((u128)rmax, sm.red);
+    rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
     l = rmax ? bits_of(rmax) + 1 : 0;
     if (l > TB) l = TB;
   } else if (CODEC == kFor) {
@@ -259,8 +262,8 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       mn = y < mn ? y : mn;
       mx = y > mx ? y : mx;
     }
-    mn = (uint64_t)block_reduce<2>((u128)mn, sm.red);
-    mx = (uint64_t)block_reduce<1>((u128)mx, sm.red);
+    mn = (uint64_t)group_reduce<2, G>((u128)mn, sm.red);
+    mx = (uint64_t)group_reduce<1, G>((u128)mx, sm.red);
     fbase = mn;
     m1 = __longlong_as_double((long long)mx);
     l = bits_of(mx - mn);
@@ -271,7 +274,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       uint64_t r = x1 > x0 ? x1 - x0 : x0 - x1;
       rmax = r > rmax ? r : rmax;
     }
-    rmax = (uint64_t)block_reduce<1>((u128)rmax, sm.red);
+    rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
     l = rmax ? bits_of(rmax) + 1 : 0;
     if (l > TB) l = TB;
     fbase = (uint64_t)sm.vals[0];
@@ -283,7 +286,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   if (CODEC != kDelta && l == TB - 1) l = TB;
   const bool raw = (l == TB);
   if (raw) {  // residuals overwrote the values: restage them
-    __syncthreads();
+    group_sync<G>();
     for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
   }
   const uint64_t size = block_bytes<CODEC, S>(l, len);
@@ -316,7 +319,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       for (int j = 0; j < S; ++j) sm.hdr[1 + j] = (uint8_t)(fbase >> (8 * j));
     }
   }
-  __syncthreads();
+  group_sync<G>();
   const uint64_t goff = sm.bcast[1];
   if (raw) H = 1;
   if (goff == ~0ull) return;                       // look-back gave up (error word set)
@@ -329,16 +332,16 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   const T *vals = sm.vals;
   const uint32_t *signs = sm.signs;
   if (raw) {
-    write_image(a.payload, goff, size, 1, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; });
+    write_image(a.payload, goff, size, 1, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; }, tid, nt);
   } else if (CODEC == kLinear || CODEC == kPoly2) {
     const uint32_t sb = l ? l - 1 : 0;
     write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
       return (uint64_t)vals[k] | ((uint64_t)((signs[k >> 5] >> (k & 31)) & 1u) << sb);
-    });
+    }, tid, nt);
   } else if (CODEC == kFor) {
     const uint64_t mnv = fbase;
     const uint64_t tm = S == 8 ? ~0ull : 0xffffffffull;
-    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t { return ((uint64_t)vals[k] - mnv) & tm; });
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t { return ((uint64_t)vals[k] - mnv) & tm; }, tid, nt);
   } else {
     const uint32_t sb = l ? l - 1 : 0;
     const uint32_t last = len - 1;
@@ -347,7 +350,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       uint64_t x0 = (uint64_t)vals[k], x1 = (uint64_t)vals[k + 1];
       bool pos = x1 > x0;
       return (pos ? x1 - x0 : x0 - x1) | ((uint64_t)pos << sb);
-    });
+    }, tid, nt);
   }
 
   // ---- offsets and directory -------------------------------------------------------
