@@ -45,11 +45,15 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch"],
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
     ap.add_argument("--fit", default="reference", choices=["reference", "exact"])
+    ap.add_argument("--serve-cols", type=int, default=64)
+    ap.add_argument("--serve-n", type=int, default=100_000_000)
+    ap.add_argument("--requests", type=int, default=4000)
+    ap.add_argument("--rate", type=float, default=50_000.0, help="offered requests per second (Poisson)")
     return ap.parse_args()
 
 
@@ -300,6 +304,92 @@ def run_batch(args, world, rank, local):
     b.close()
 
 
+def run_serve(args, world, rank, local):
+    """64 resident LeCo-fix columns of 100M u64 keys (the 200M-key generator,
+    one seed per column), a Poisson request stream: 80 % point lookups of
+    log-uniform 1..65536 random indices, 20 % range scans of log-uniform
+    16..1M values.  The same trace is served twice: by the continuous-batching
+    server and by plain per-request launches (one request per launch, one at
+    a time).  Latency = submit -> results in the client's pinned buffer."""
+    import math
+    import threading
+
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    raws, cols = [], []
+    for c in range(args.serve_cols):
+        x = workloads.piecewise_linear_u64(args.serve_n, seed=100 + c + 1000 * rank, device=dev)
+        cols.append(lc.encode(x, lc.LINEAR, BS, lc.FIT_EXACT).compact())
+        raws.append(x)
+    torch.cuda.synchronize()
+    comp = sum(c.nbytes for c in cols)
+    rng = np.random.default_rng(17 + rank)
+    reqs, n_look, n_scan = [], 0, 0
+    for i in range(args.requests):
+        ci = int(rng.integers(args.serve_cols))
+        if rng.random() < 0.8:
+            m = int(math.exp(rng.uniform(0, math.log(65536))))
+            idx = torch.from_numpy(rng.integers(0, args.serve_n, m).astype(np.int64)).pin_memory()
+            reqs.append((ci, idx, 0, m))
+            n_look += m
+        else:
+            m = int(math.exp(rng.uniform(math.log(16), math.log(1_000_000))))
+            reqs.append((ci, None, int(rng.integers(0, args.serve_n - m)), m))
+            n_scan += m
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    outs = [torch.empty(r[3], dtype=torch.int64).pin_memory() for r in reqs]
+
+    def serve(**opt):
+        srv = lc.Server(cols, **opt)
+        # warm-up: a few requests through the same server
+        for r, o in list(zip(reqs, outs))[:16]:
+            srv.wait(srv.submit(r[0], o, idx=r[1], first=r[2], count=r[3]))
+        srv.reset_stats()
+        ids = []
+        t0 = time.perf_counter()
+        for (ci, idx, first, m), o, ta in zip(reqs, outs, arrivals):
+            while time.perf_counter() - t0 < ta:
+                pass
+            ids.append(srv.submit(ci, o, idx=idx, first=first, count=m))
+        srv.drain()
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        for i in ids:
+            srv.wait(i)
+        srv.close()
+        lc.check()
+        # verify a sample of the results against the stored keys
+        for j in range(0, len(reqs), max(1, len(reqs) // 64)):
+            ci, idx, first, m = reqs[j]
+            exp = raws[ci][idx.to(dev)] if idx is not None else raws[ci][first:first + m]
+            assert torch.equal(outs[j].to(dev), exp), "served result mismatch"
+        return st, span
+
+    with ClockSampler(local) as clk:
+        st_b, span_b = serve(slots=4, max_requests_per_batch=1024)
+    st_p, span_p = serve(slots=1, max_requests_per_batch=1)
+    if rank == 0:
+        arm = lambda st, span: {"lookups_per_s": round(st["lookups"] / span, 1), "scanned_values_per_s": round(st["scanned_values"] / span, 1),
+                                "p50_us": round(st["p50_us"], 1), "p99_us": round(st["p99_us"], 1), "mean_us": round(st["mean_us"], 1),
+                                "makespan_s": round(span, 4), "batches": st["batches"], "max_requests_in_batch": st["max_requests_in_batch"]}
+        line = {"metric": "served random access: lookups/s and p50/p99 latency (continuous batching)",
+                "value": round(st_b["lookups"] / span_b / 1e6, 3), "unit": "Mlookups/s", "n_gpus": world,
+                "steps": args.requests, "warmup": 16, "ms_per_step": round(1e3 * span_b / args.requests, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"{args.serve_cols} resident LeCo-fix columns x {args.serve_n} u64, Poisson "
+                                       f"{args.rate:.0f} req/s, 80% lookups logU[1,65536], 20% scans logU[16,1M]",
+                           "requests": args.requests, "lookups": n_look, "scanned_values": n_scan,
+                           "compressed_bytes_resident": comp},
+                "continuous_batching": arm(st_b, span_b), "per_request_launches": arm(st_p, span_p),
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -308,6 +398,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, world, rank, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, world, rank, local)
         return
 
     import torch

@@ -199,6 +199,53 @@ int leco_batch_run_graph(leco_batch *b, int passes, leco_stream_t stream);
 int leco_batch_encode_per_column(leco_batch *b, leco_stream_t stream);
 int leco_batch_decode_per_column(leco_batch *b, leco_stream_t stream);
 
+/* ---- serving: continuous batching of lookups and range scans -----------
+ * No counterpart in the reference (its random access is a per-index CPU loop,
+ * experiments/leco_int_fix_template.cpp:189-207).  Columns stay resident in HBM
+ * (encoded with leco_encode / leco_batch_*); requests from any thread are
+ * admitted by free device memory for their index and output buffers, coalesced
+ * into one kernel launch per batch, and several batches overlap on the GPU. */
+
+enum leco_request_kind { LECO_REQ_LOOKUP = 0, LECO_REQ_RANGE = 1 };
+
+typedef struct leco_request {
+  uint32_t column;       /* index into the server's columns                          */
+  uint32_t kind;         /* LECO_REQ_LOOKUP or LECO_REQ_RANGE                         */
+  uint64_t count;        /* lookups, or values in the range                           */
+  const uint64_t *h_idx; /* LOOKUP: count indices (pinned host memory for async copy) */
+  uint64_t first;        /* RANGE: first value                                        */
+  void *h_out;           /* count results (pinned host memory for async copy)         */
+} leco_request;
+
+typedef struct leco_server_options {
+  uint32_t slots;                  /* batches in flight (streams); 0 -> 4                  */
+  uint32_t max_requests_per_batch; /* 0 -> 1024; 1 with slots = 1 = per-request launches   */
+  uint32_t max_items_per_batch;    /* CTAs per batch launch; 0 -> 65536                    */
+  uint32_t reserved;
+  uint64_t hbm_budget_bytes;       /* device arena for indices + results; 0 -> 1/4 of free */
+} leco_server_options;
+
+typedef struct leco_server_stats {
+  uint64_t completed, lookups, scanned_values, batches, max_requests_in_batch, arena_bytes;
+  double p50_us, p99_us, mean_us, max_us; /* submit -> results in the client's buffer */
+} leco_server_stats;
+
+typedef struct leco_server leco_server; /* opaque */
+
+/* Starts a server (one host thread) over encoded resident columns; allocates
+ * its device arena and per-slot item tables. */
+int leco_server_create(const leco_column_desc *h_cols, uint32_t ncols, const leco_server_options *opt, leco_server **out);
+/* Queues a request (thread-safe, returns at once).  LECO_ERR_NOMEM if the request
+ * could never fit the server's device budget. */
+int leco_server_submit(leco_server *sv, const leco_request *req, uint64_t *req_id);
+/* Blocks until the request's results are in its h_out; *latency_us = submit -> done. */
+int leco_server_wait(leco_server *sv, uint64_t req_id, double *latency_us);
+/* Blocks until every submitted request has completed. */
+int leco_server_drain(leco_server *sv);
+int leco_server_get_stats(leco_server *sv, leco_server_stats *out);
+int leco_server_reset_stats(leco_server *sv);
+int leco_server_destroy(leco_server *sv);
+
 /* ---- host-buffer entry points (synchronous; allocate device memory) ----
  * These are the reference-facing calls: host in, host out, the same
  * arguments as the reference's per-column driver loops. */

@@ -83,6 +83,13 @@ SIGNATURES = [
     ("leco_batch_run_graph", _I, [_P, _I, _P]),
     ("leco_batch_encode_per_column", _I, [_P, _P]),
     ("leco_batch_decode_per_column", _I, [_P, _P]),
+    ("leco_server_create", _I, [_P, _U32, _P, _P]),
+    ("leco_server_submit", _I, [_P, _P, _P]),
+    ("leco_server_wait", _I, [_P, _U64, _P]),
+    ("leco_server_drain", _I, [_P]),
+    ("leco_server_get_stats", _I, [_P, _P]),
+    ("leco_server_reset_stats", _I, [_P]),
+    ("leco_server_destroy", _I, [_P]),
     ("leco_check", _I, [_P]),
     ("leco_last_error", ctypes.c_char_p, []),
     ("leco_version", ctypes.c_char_p, []),
@@ -307,6 +314,18 @@ class Column:
                                           self.block_size, _tptr(self.dir), _stream_ptr(stream)), "leco_build_directory")
         return self.dir
 
+    def compact(self):
+        """Moves the payload into an exactly sized buffer (encode allocates the
+        worst case); returns self."""
+        torch = _torch()
+        n = self.nbytes
+        buf = torch.zeros(n + PAYLOAD_SLACK, dtype=torch.uint8, device=self.payload.device)
+        buf[:n].copy_(self.payload[:n])
+        self.payload = buf
+        if self.dir is not None:  # the directory holds bit addresses, not pointers: still valid
+            pass
+        return self
+
     def to_host(self):
         """(payload bytes as uint8 numpy, offsets as uint64 numpy)."""
         off = self.offsets.cpu().numpy().view(np.uint64)
@@ -432,6 +451,92 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             lib().leco_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Serving loop: continuous batching of lookups and range scans.
+# ---------------------------------------------------------------------------
+
+REQ_LOOKUP, REQ_RANGE = 0, 1
+
+
+class Request(ctypes.Structure):
+    """``leco_request`` of include/leco.h."""
+    _fields_ = [("column", ctypes.c_uint32), ("kind", ctypes.c_uint32), ("count", ctypes.c_uint64),
+                ("h_idx", _P), ("first", ctypes.c_uint64), ("h_out", _P)]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("max_requests_per_batch", ctypes.c_uint32),
+                ("max_items_per_batch", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("hbm_budget_bytes", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("lookups", ctypes.c_uint64), ("scanned_values", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64), ("max_requests_in_batch", ctypes.c_uint64), ("arena_bytes", ctypes.c_uint64),
+                ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double),
+                ("max_us", ctypes.c_double)]
+
+
+class Server:
+    """A request loop over resident encoded ``Column`` objects.
+
+    ``submit`` takes pinned host buffers (torch ``pin_memory=True`` tensors):
+    ``idx`` (int64 indices) for a lookup or ``first`` for a range scan, and
+    ``out`` for the results.  The buffers must stay alive until ``wait``
+    returns for that request."""
+
+    def __init__(self, columns, slots: int = 4, max_requests_per_batch: int = 1024, hbm_budget_bytes: int = 0,
+                 max_items_per_batch: int = 0):
+        L = lib()
+        self.columns = list(columns)
+        descs = (ColumnDesc * len(self.columns))()
+        for i, c in enumerate(self.columns):
+            if c.dir is None:
+                c.build_directory()
+            descs[i] = ColumnDesc(c.codec, c.dtype, c.block_size, 0, c.n, None, None, c.payload.data_ptr(),
+                                  c.payload.numel(), c.offsets.data_ptr(), c.dir.data_ptr())
+        opt = ServerOptions(slots, max_requests_per_batch, max_items_per_batch, 0, hbm_budget_bytes)
+        h = _P()
+        _check(L.leco_server_create(descs, len(self.columns), ctypes.byref(opt), ctypes.byref(h)), "leco_server_create")
+        self._h = h
+
+    def submit(self, column: int, out, idx=None, first: int = 0, count: int | None = None) -> int:
+        if idx is not None:
+            r = Request(column, REQ_LOOKUP, idx.numel(), idx.data_ptr(), 0, out.data_ptr())
+        else:
+            r = Request(column, REQ_RANGE, count if count is not None else out.numel(), None, first, out.data_ptr())
+        rid = ctypes.c_uint64()
+        _check(lib().leco_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "leco_server_submit")
+        return rid.value
+
+    def wait(self, rid: int) -> float:
+        lat = ctypes.c_double()
+        _check(lib().leco_server_wait(self._h, rid, ctypes.byref(lat)), "leco_server_wait")
+        return lat.value
+
+    def drain(self):
+        _check(lib().leco_server_drain(self._h), "leco_server_drain")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().leco_server_get_stats(self._h, ctypes.byref(st)), "leco_server_get_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(lib().leco_server_reset_stats(self._h), "leco_server_reset_stats")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().leco_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -210,70 +210,10 @@ __global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_su
 }
 
 // ---- random access --------------------------------------------------------------
-// Batched random access: each thread keeps U lookups in flight (indices,
-// directory entries and payload words are each loaded for all U before any is
-// used), lookups i, i+G, i+2G, ... of one thread are strided by the grid so
-// index loads and output stores stay coalesced across a warp.
+// Batched random access over the whole index array (see gather_lookups).
 template <typename T, int CODEC>
 __global__ void __launch_bounds__(256) gather_kernel(GatherLaunch a) {
-  constexpr int S = sizeof(T);
-  constexpr uint32_t TB = 8u * S;
-  constexpr int U = 4;
-  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
-  T *out = reinterpret_cast<T *>(a.out);
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
-  const bool small = a.n <= 0xffffffffull;
-  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < a.m; i0 += G * U) {
-    uint64_t g[U], b[U];
-    uint32_t k[U];
-    bool live[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const uint64_t i = i0 + (uint64_t)u * G;
-      live[u] = i < a.m;
-      g[u] = live[u] ? __ldg(a.idx + i) : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (g[u] >= a.n) {
-        if (live[u]) {
-          out[i0 + (uint64_t)u * G] = 0;
-          atomicOr(a.error, kErrBadIndex);
-        }
-        live[u] = false;
-        g[u] = 0;
-      }
-      if (small) {
-        b[u] = (uint32_t)g[u] / a.bs;
-        k[u] = (uint32_t)g[u] - (uint32_t)b[u] * a.bs;
-      } else {
-        b[u] = g[u] / a.bs;
-        k[u] = (uint32_t)(g[u] - b[u] * a.bs);
-      }
-    }
-    BlockHdr h[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      h[u] = a.dir ? from_dir<CODEC, S>(a.dir, b[u]) : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b[u]));
-    uint64_t lo[U], hi[U];
-    uint32_t sh[U], l[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      l[u] = h[u].l > TB ? 0 : h[u].l;
-      const uint64_t bit = h[u].body_bit + (uint64_t)k[u] * l[u];
-      sh[u] = (uint32_t)(bit & 63);
-      // the second word only when the field crosses into it: a random lookup then
-      // touches one DRAM sector instead of two whenever the field sits in one word
-      lo[u] = l[u] ? __ldg(words + (bit >> 6)) : 0;
-      hi[u] = (l[u] && sh[u] + l[u] > 64) ? __ldg(words + (bit >> 6) + 1) : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!live[u]) continue;
-      const uint64_t f = funnel64(lo[u], hi[u], sh[u]) & lowmask(l[u]);
-      out[i0 + (uint64_t)u * G] = (T)ra_value<CODEC, S>(h[u], k[u], f, a.error);
-    }
-  }
+  gather_lookups<T, CODEC>(a, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
 }
 
 // Delta random access: prefix walk over fields 0..k-1 (bit_read.h:1292-1317).
