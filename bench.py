@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve"],
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
@@ -390,6 +390,82 @@ def run_serve(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_varlen(args, world, rank, local):
+    """500M u64 keys from the regime-switching generator (linear, quadratic and
+    flat regimes of geometric length, noise 2^8): variable-length segments from
+    the host partitioner (coarse blocks of 2000 values, merge penalty 12 bits,
+    as the reference's benchmark script runs its u64 variable-length codec) and
+    the degree-2 polynomial codec with 8192-value blocks.  Times GPU encode,
+    bulk decode, 2^24 random lookups and the compressed-domain sum."""
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n if args.n != N_DEFAULT else 500_000_000
+    x = workloads.regime_switching_u64(n, seed=5 + rank, device=dev)
+    xh = x.cpu().numpy().view(np.uint64)
+    stream = torch.cuda.current_stream()
+
+    def ev_time(fn, reps=max(3, args.steps // 4)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t0 = time.perf_counter()
+    starts = lc.varlen_partition(xh, n // 2000, 12)
+    t_part = time.perf_counter() - t0
+    vc = lc.varlen_encode(x, starts, lc.FIT_REFERENCE)
+    out = torch.empty_like(x)
+    idx = torch.randint(0, n, (RA_BATCH,), device=dev)
+    ra = torch.empty(RA_BATCH, dtype=torch.int64, device=dev)
+    res = {}
+    res["varlen"] = {
+        "segments": int(len(starts)), "partition_host_s": round(t_part, 3), "host_threads": os.cpu_count(),
+        "encode_ms": round(ev_time(lambda: lc.varlen_encode(x, vc.starts, lc.FIT_REFERENCE)), 3),
+        "decode_ms": round(ev_time(lambda: vc.decode(out=out)), 3),
+        "gather_ms_2^24": round(ev_time(lambda: vc.gather(idx, out=ra)), 3),
+        "sum_ms": round(ev_time(lambda: vc.sum()), 3), "compressed_ratio": round(vc.nbytes / (8 * n), 5)}
+    assert torch.equal(vc.decode(out=out), x) and torch.equal(vc.gather(idx, out=ra), x[idx])
+    assert vc.sum() == int(x.sum().item()) & 0xFFFFFFFFFFFFFFFF
+    del vc
+    pc = lc.encode(x, lc.POLY2, 8192, lc.FIT_REFERENCE)
+    res["poly2_8192"] = {
+        "encode_ms_reference_fit": round(ev_time(lambda: lc.encode(x, lc.POLY2, 8192, lc.FIT_REFERENCE, payload=pc.payload)), 3),
+        "encode_ms_exact_fit": round(ev_time(lambda: lc.encode(x, lc.POLY2, 8192, lc.FIT_EXACT, payload=pc.payload)), 3),
+        "decode_ms": 0.0, "gather_ms_2^24": 0.0, "sum_ms": 0.0}
+    pc = lc.encode(x, lc.POLY2, 8192, lc.FIT_REFERENCE)
+    res["poly2_8192"]["decode_ms"] = round(ev_time(lambda: pc.decode(out=out)), 3)
+    res["poly2_8192"]["gather_ms_2^24"] = round(ev_time(lambda: pc.gather(idx, out=ra)), 3)
+    res["poly2_8192"]["sum_ms"] = round(ev_time(lambda: pc.sum()), 3)
+    res["poly2_8192"]["compressed_ratio"] = round(pc.nbytes / (8 * n), 5)
+    assert torch.equal(pc.decode(out=out), x) and torch.equal(pc.gather(idx, out=ra), x[idx])
+    assert pc.sum() == int(x.sum().item()) & 0xFFFFFFFFFFFFFFFF
+    lc.check()
+    for k in res:
+        r = res[k]
+        r["decode_gbs"] = round(8 * n / (r["decode_ms"] / 1e3) / 1e9, 1)
+        r["mlookups_s"] = round(RA_BATCH / (r["gather_ms_2^24"] / 1e3) / 1e6, 1)
+        r["sum_gbs"] = round(8 * n / (r["sum_ms"] / 1e3) / 1e9, 1)
+    if rank == 0:
+        line = {"metric": "variable-length and degree-2 LeCo on 500M u64: decode GB/s, random access, sum",
+                "value": res["varlen"]["decode_gbs"], "unit": "GB/s", "n_gpus": world, "steps": max(3, args.steps // 4),
+                "warmup": 1, "ms_per_step": res["varlen"]["decode_ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"{n} u64 regime-switching (linear/quadratic/flat, sigma 2^8); varlen: coarse "
+                                       "blocks of 2000, delta 12; poly2: 8192-value blocks", "keys": n},
+                **res}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -401,6 +477,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, world, rank, local)
+        return
+    if args.workload == "varlen":
+        run_varlen(args, world, rank, local)
         return
 
     import torch

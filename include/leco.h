@@ -160,6 +160,37 @@ uint64_t leco_sum_workspace_bytes(uint64_t n, uint32_t block_size);
 int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
              uint32_t block_size, uint64_t *d_sum, void *d_partials, leco_stream_t stream);
 
+/* ---- variable-length segments (Leco_cost_merge_double_wo_round<uint64_t>) ----
+ * headers/piecewise_cost_merge_integer_template_double_wo_round.h:18-700.  A column is
+ * payload (segment images back to back), offsets[nseg + 1] and starts[nseg] (value
+ * index of each segment's first value, starts[0] = 0; segment s covers
+ * [starts[s], starts[s+1]) and the last one ends at n). */
+
+/* Host partitioner (encodeArray8_int's split + merge passes, :283-570): coarse blocks
+ * as the reference driver cuts them (n / coarse_blocks values each), `delta` = the
+ * reference's merge penalty in bits.  Writes the segment starts (<= starts_cap) and
+ * *nseg.  threads <= 0: all host cores. */
+int leco_varlen_partition(const uint64_t *h_values, uint64_t n, uint32_t coarse_blocks, int64_t delta,
+                          uint64_t *h_starts, uint64_t starts_cap, uint64_t *nseg, int threads);
+uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg);
+uint64_t leco_varlen_workspace_bytes(uint64_t nseg);
+/* Longest segment leco_varlen_encode accepts (values). */
+uint64_t leco_varlen_max_segment(void);
+/* Writes every segment image (newsegment / newsegment_1 / newsegment_2, :134-272) for the
+ * given starts; LECO_FIT_REFERENCE gives the reference's bytes. */
+int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, int fit_mode,
+                       uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
+                       uint64_t workspace_bytes, leco_stream_t stream);
+/* decodeArray8 over all segments (:573-626); a raw segment yields its own values. */
+int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                       uint64_t n, uint64_t *d_out, leco_stream_t stream);
+/* randomdecodeArray8 for each index (:636-698): binary search of the device start array. */
+int leco_varlen_gather(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                       uint64_t n, const uint64_t *d_idx, uint64_t m, uint64_t *d_out, leco_stream_t stream);
+/* Sum of all values mod 2^64 without materialising them. */
+int leco_varlen_sum(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                    uint64_t n, uint64_t *d_sum, leco_stream_t stream);
+
 /* ---- batch engine: many columns, one persistent launch per pass --------
  * No counterpart in the reference, whose drivers loop over the blocks of one
  * column (experiments/leco_int_fix_template.cpp:111-127, :145-153). */

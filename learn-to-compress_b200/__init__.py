@@ -90,6 +90,14 @@ SIGNATURES = [
     ("leco_server_get_stats", _I, [_P, _P]),
     ("leco_server_reset_stats", _I, [_P]),
     ("leco_server_destroy", _I, [_P]),
+    ("leco_varlen_partition", _I, [_P, _U64, _U32, ctypes.c_int64, _P, _U64, _P, _I]),
+    ("leco_varlen_max_payload_bytes", _U64, [_U64, _U64]),
+    ("leco_varlen_workspace_bytes", _U64, [_U64]),
+    ("leco_varlen_max_segment", _U64, []),
+    ("leco_varlen_encode", _I, [_P, _U64, _P, _U64, _I, _P, _U64, _P, _P, _U64, _P]),
+    ("leco_varlen_decode", _I, [_P, _P, _P, _U64, _U64, _P, _P]),
+    ("leco_varlen_gather", _I, [_P, _P, _P, _U64, _U64, _P, _U64, _P, _P]),
+    ("leco_varlen_sum", _I, [_P, _P, _P, _U64, _U64, _P, _P]),
     ("leco_check", _I, [_P]),
     ("leco_last_error", ctypes.c_char_p, []),
     ("leco_version", ctypes.c_char_p, []),
@@ -544,3 +552,78 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Variable-length segments.
+# ---------------------------------------------------------------------------
+
+def varlen_partition(values: np.ndarray, coarse_blocks: int, delta: int, threads: int = 0) -> np.ndarray:
+    """Segment starts (uint64) of a uint64 column, computed on the host cores."""
+    values = np.ascontiguousarray(values, np.uint64)
+    out = np.zeros(len(values), np.uint64)
+    ns = ctypes.c_uint64()
+    _check(lib().leco_varlen_partition(_np_ptr(values), len(values), coarse_blocks, delta, _np_ptr(out), len(out),
+                                       ctypes.byref(ns), threads), "leco_varlen_partition")
+    return out[: ns.value].copy()
+
+
+@dataclass
+class VarlenColumn:
+    n: int
+    starts: object   # int64 CUDA tensor [nseg]
+    payload: object  # uint8 CUDA tensor
+    offsets: object  # int64 CUDA tensor [nseg + 1]
+
+    @property
+    def nseg(self) -> int:
+        return self.starts.numel()
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.offsets[-1].item())
+
+    def decode(self, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.n, dtype=torch.int64, device=self.payload.device)
+        _check(lib().leco_varlen_decode(_tptr(self.payload), _tptr(self.offsets), _tptr(self.starts), self.nseg, self.n,
+                                        _tptr(out), _stream_ptr(stream)), "leco_varlen_decode")
+        return out
+
+    def gather(self, idx, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(idx.numel(), dtype=torch.int64, device=self.payload.device)
+        _check(lib().leco_varlen_gather(_tptr(self.payload), _tptr(self.offsets), _tptr(self.starts), self.nseg, self.n,
+                                        _tptr(idx), idx.numel(), _tptr(out), _stream_ptr(stream)), "leco_varlen_gather")
+        return out
+
+    def sum(self, stream=None) -> int:
+        torch = _torch()
+        out = torch.empty(1, dtype=torch.int64, device=self.payload.device)
+        _check(lib().leco_varlen_sum(_tptr(self.payload), _tptr(self.offsets), _tptr(self.starts), self.nseg, self.n,
+                                     _tptr(out), _stream_ptr(stream)), "leco_varlen_sum")
+        return int(out.item()) & 0xFFFFFFFFFFFFFFFF
+
+    def to_host(self):
+        off = self.offsets.cpu().numpy().view(np.uint64)
+        return self.payload[: int(off[-1])].cpu().numpy(), off, self.starts.cpu().numpy().view(np.uint64)
+
+
+def varlen_encode(values, starts, fit_mode: int = FIT_REFERENCE, stream=None) -> VarlenColumn:
+    """Encodes a uint64 CUDA tensor (int64 view) with the given segment starts."""
+    torch = _torch()
+    L = lib()
+    n = values.numel()
+    st = starts if hasattr(starts, "is_cuda") else torch.from_numpy(np.ascontiguousarray(starts, np.uint64).view(np.int64))
+    st = st.to(values.device)
+    ns = st.numel()
+    cap = L.leco_varlen_max_payload_bytes(n, ns)
+    pay = torch.empty(cap, dtype=torch.uint8, device=values.device)
+    off = torch.empty(ns + 1, dtype=torch.int64, device=values.device)
+    wsb = L.leco_varlen_workspace_bytes(ns)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=values.device)
+    _check(L.leco_varlen_encode(_tptr(values), n, _tptr(st), ns, fit_mode, _tptr(pay), cap, _tptr(off), _tptr(ws), wsb,
+                                _stream_ptr(stream)), "leco_varlen_encode")
+    return VarlenColumn(n, st, pay, off)

@@ -1,0 +1,351 @@
+// leco_varlen.cu -- variable-length LeCo segments on the GPU: segment encode
+// (given the partition), bulk decode, random access and compressed-domain sum.
+//
+// Segment image (Leco_cost_merge_double_wo_round<uint64_t>,
+// headers/piecewise_cost_merge_integer_template_double_wo_round.h:134-272):
+//   [u32 start][u8 l][f64 theta0][f32 slope][packed l-bit fields]   (l < 64)
+//   [u32 start][u8 64][u64 x n]                                      (raw)
+//   [u32 start][u8 127][u64]   one value,  [u32 start][u8 126][u64][u64]  two values
+// Prediction theta0 + (double)slope * k.  The encoder converts it to a 128-bit
+// integer (:158); bulk decode converts it to uint64_t (bit_read.h:530).
+// A column: payload (segment images back to back), offsets[nseg+1], and the
+// value index where each segment starts, starts[nseg] (starts[0] = 0).
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "leco_encode.cuh"
+
+namespace leco {
+
+constexpr uint32_t kVarlenMaxSeg = 16384;  // values per segment the encoder stages in shared memory
+
+__device__ __forceinline__ i128 f2i128(double x) {
+  // truncation toward zero (__fixdfti) for |x| < 2^127
+  if (fabs(x) < 9223372036854775808.0) return (i128)__double2ll_rz(x);
+  const uint64_t bits = (uint64_t)__double_as_longlong(x);
+  const int e = (int)((bits >> 52) & 0x7ff) - 1075;
+  const uint64_t m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+  const i128 v = e >= 0 ? ((i128)m << e) : (i128)(m >> (-e));
+  return x < 0 ? -v : v;
+}
+
+struct VarArgs {
+  const uint64_t *values;
+  uint64_t n;
+  const uint64_t *starts;
+  uint64_t nseg;
+  uint8_t *payload;
+  uint64_t payload_cap;
+  uint64_t *offsets;
+  uint64_t *status;
+  uint32_t *ticket;
+  uint32_t *error;
+  int exact_fit;
+};
+
+__device__ __forceinline__ uint64_t seg_bytes(uint32_t l, uint32_t len) {
+  if (len == 1) return 13;
+  if (len == 2) return 21;
+  if (l >= 64) return 5 + 8ull * len;
+  if (!l) return 17;
+  const uint64_t end = ((uint64_t)l * len + 7) / 8;
+  return 17 + end + 1 + (8 - end % 8);
+}
+
+// One CTA encodes one segment (newsegment / newsegment_1 / newsegment_2).
+__global__ void __launch_bounds__(256) varlen_encode_kernel(VarArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  __shared__ uint64_t s_ticket, s_off;
+  __shared__ u128 red[40];
+  __shared__ uint8_t hdr[32];
+  __shared__ double s_model[2];
+  uint64_t *vals = reinterpret_cast<uint64_t *>(smem_raw);
+  uint32_t *signs = reinterpret_cast<uint32_t *>(smem_raw + 8 * kVarlenMaxSeg);
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) s_ticket = atomicAdd(a.ticket, 1u);
+  __syncthreads();
+  const uint64_t sgi = s_ticket;
+  if (sgi >= a.nseg) return;
+  const uint64_t st = a.starts[sgi], en = sgi + 1 < a.nseg ? a.starts[sgi + 1] : a.n;
+  if (en <= st || en - st > kVarlenMaxSeg || en > a.n) {  // bad partition: report, keep successors moving
+    if (tid < 32) lookback_prefix(a.status, sgi, 0, a.error);
+    if (tid == 0) atomicOr(a.error, kErrBadHeader);
+    return;
+  }
+  const uint32_t len = (uint32_t)(en - st);
+  for (uint32_t i = tid; i < len; i += nt) vals[i] = __ldg(a.values + st + i);
+  __syncthreads();
+  uint32_t l = 0;
+  double t0 = 0, t1d = 0;
+  float slope = 0.f;
+  if (len >= 3) {
+    if (a.exact_fit) {
+      u128 sy = 0, siy = 0;
+      for (uint32_t i = tid; i < len; i += nt) {
+        sy += vals[i];
+        siy += (u128)vals[i] * i;
+      }
+      sy = block_reduce<0>(sy, red);
+      siy = block_reduce<0>(siy, red);
+      if (tid == 0) {
+        const uint64_t m = len;
+        const double md = __uint2double_rn(len);
+        const double sumx = __ull2double_rn(m * (m - 1) / 2), sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
+        const double sumy = u128_to_double(sy), sumxy = u128_to_double(siy);
+        const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+        const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+        const double th1 = __ddiv_rn(ccc, xxx);
+        s_model[1] = th1;
+        s_model[0] = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(th1, sumx)), md);
+      }
+    } else if (tid == 0) {  // lr_int_T::caltheta, the reference's sequential FP64 loop (lr.h:66-85)
+      double sumx = 0, sumy = 0, sumxx = 0, sumxy = 0;
+      for (uint32_t i = 0; i < len; ++i) {
+        const double di = __uint2double_rn(i), yi = __ull2double_rn(vals[i]);
+        sumx = __dadd_rn(sumx, di);
+        sumy = __dadd_rn(sumy, yi);
+        sumxx = __dadd_rn(sumxx, __dmul_rn(di, di));
+        sumxy = __dadd_rn(sumxy, __dmul_rn(di, yi));
+      }
+      const double md = __uint2double_rn(len);
+      const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+      const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+      const double th1 = __ddiv_rn(ccc, xxx);
+      s_model[1] = th1;
+      s_model[0] = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(th1, sumx)), md);
+    }
+    __syncthreads();
+    t0 = s_model[0];
+    slope = __double2float_rn(s_model[1]);  // float final_slope = mylr.theta1 (:148)
+    t1d = (double)slope;
+    uint64_t rmax = 0;
+    for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+      const uint32_t i = i0 + tid;
+      bool pos = false;
+      if (i < len) {
+        const i128 pred = f2i128(__dadd_rn(t0, __dmul_rn(t1d, __uint2double_rn(i))));
+        const i128 y = (i128)vals[i];
+        pos = y > pred;
+        const uint64_t r = (uint64_t)(pos ? y - pred : pred - y);
+        vals[i] = r;
+        rmax = r > rmax ? r : rmax;
+      }
+      const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+      if ((tid & 31) == 0) signs[i0 / 32 + tid / 32] = ballot;
+    }
+    rmax = (uint64_t)block_reduce<1>((u128)rmax, red);
+    l = rmax ? bits_of(rmax) + 1 : 0;
+    if (l >= 64) {
+      l = 64;
+      __syncthreads();
+      for (uint32_t i = tid; i < len; i += nt) vals[i] = __ldg(a.values + st + i);
+    }
+  }
+  const uint64_t size = seg_bytes(l, len);
+  if (tid < 32) {
+    const uint64_t excl = lookback_prefix(a.status, sgi, size, a.error);
+    if (tid == 0) s_off = excl;
+  }
+  uint32_t H;
+  if (tid == 0) {
+    const uint32_t s32 = (uint32_t)st;
+    for (int j = 0; j < 4; ++j) hdr[j] = (uint8_t)(s32 >> (8 * j));
+    hdr[4] = (uint8_t)(len == 1 ? 127 : len == 2 ? 126 : l);
+    if (len >= 3 && l < 64) {
+      const uint64_t w0 = (uint64_t)__double_as_longlong(t0);
+      const uint32_t w1 = (uint32_t)__float_as_uint(slope);
+      for (int j = 0; j < 8; ++j) hdr[5 + j] = (uint8_t)(w0 >> (8 * j));
+      for (int j = 0; j < 4; ++j) hdr[13 + j] = (uint8_t)(w1 >> (8 * j));
+    }
+  }
+  __syncthreads();
+  const uint64_t goff = s_off;
+  if (goff == ~0ull) return;
+  if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {
+    if (tid == 0) atomicOr(a.error, kErrCapacity);
+    return;
+  }
+  if (len <= 2 || l == 64) {  // values stored as they are
+    H = 5;
+    write_image(a.payload, goff, size, H, hdr, 64, len, [&](uint32_t k) -> uint64_t { return vals[k]; }, tid, nt);
+  } else {
+    H = 17;
+    const uint32_t sb = l ? l - 1 : 0;
+    write_image(a.payload, goff, size, H, hdr, l, len, [&](uint32_t k) -> uint64_t {
+      return vals[k] | ((uint64_t)((signs[k >> 5] >> (k & 31)) & 1u) << sb);
+    }, tid, nt);
+  }
+  if (tid == 0) {
+    a.offsets[sgi] = goff;
+    if (sgi == a.nseg - 1) a.offsets[a.nseg] = goff + size;
+  }
+}
+
+struct SegHdr {
+  uint64_t start;
+  uint32_t l;
+  double t0, slope;
+  uint64_t body_bit;
+};
+
+__device__ __forceinline__ SegHdr parse_seg(const uint8_t *payload, uint64_t off) {
+  const uint64_t *w = reinterpret_cast<const uint64_t *>(payload);
+  const uint64_t h0 = load_u64_at(w, off);
+  SegHdr s;
+  s.start = h0 & 0xffffffffull;
+  s.l = (uint32_t)((h0 >> 32) & 0xff);
+  s.t0 = s.slope = 0;
+  s.body_bit = (off + 5) * 8;
+  if (s.l < 64) {
+    s.t0 = __longlong_as_double((long long)load_u64_at(w, off + 5));
+    s.slope = (double)__uint_as_float((uint32_t)load_u64_at(w, off + 13));
+    s.body_bit = (off + 17) * 8;
+  }
+  return s;
+}
+
+// Value k of a segment of length len (bulk-decode rules; also used for random access).
+__device__ __forceinline__ uint64_t seg_value(const uint64_t *words, const SegHdr &h, uint32_t k) {
+  if (h.l == 127 || h.l == 126 || h.l == 64) return load_field(words, h.body_bit + (uint64_t)k * 64, 64);
+  if (h.l > 64) return 0;
+  if (!h.l) return f2u_x86(__dadd_rn(h.t0, __dmul_rn(h.slope, __uint2double_rn(k))));
+  const uint64_t pred = f2u_x86(__dadd_rn(h.t0, __dmul_rn(__uint2double_rn(k), h.slope)));
+  return apply_signed(pred, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+}
+
+// One CTA per segment (Leco_cost_merge_double_wo_round::decodeArray8, :573-626).
+__global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *payload, const uint64_t *offsets,
+                                                            const uint64_t *starts, uint64_t nseg, uint64_t n,
+                                                            uint64_t *out, uint32_t *error) {
+  const uint64_t sgi = blockIdx.x;
+  const uint64_t st = starts[sgi], en = sgi + 1 < nseg ? starts[sgi + 1] : n;
+  const uint32_t len = (uint32_t)(en - st);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
+  const SegHdr h = parse_seg(payload, offsets[sgi]);
+  if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
+    if (threadIdx.x == 0) atomicOr(error, kErrBadHeader);
+    return;
+  }
+  const uint32_t cnt = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
+  for (uint32_t k = threadIdx.x; k < cnt && k < len; k += blockDim.x) __stcs(out + st + k, seg_value(words, h, k));
+}
+
+// Random access: binary search over the segment starts, then one value
+// (randomdecodeArray8, :636-698; the raw case indexes inside the segment).
+__global__ void __launch_bounds__(256) varlen_gather_kernel(const uint8_t *payload, const uint64_t *offsets,
+                                                            const uint64_t *starts, uint64_t nseg, uint64_t n,
+                                                            const uint64_t *idx, uint64_t m, uint64_t *out,
+                                                            uint32_t *error) {
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = __ldg(idx + i);
+    if (g >= n) {
+      out[i] = 0;
+      atomicOr(error, kErrBadIndex);
+      continue;
+    }
+    uint64_t lo = 0, hi = nseg;  // largest s with starts[s] <= g
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (__ldg(starts + mid) <= g) lo = mid;
+      else hi = mid;
+    }
+    const SegHdr h = parse_seg(payload, __ldg(offsets + lo));
+    out[i] = seg_value(words, h, (uint32_t)(g - h.start));
+  }
+}
+
+__global__ void __launch_bounds__(256) varlen_sum_kernel(const uint8_t *payload, const uint64_t *offsets,
+                                                         const uint64_t *starts, uint64_t nseg, uint64_t n,
+                                                         uint64_t *d_sum) {
+  __shared__ u128 red[33];
+  const uint64_t sgi = blockIdx.x;
+  const uint64_t st = starts[sgi], en = sgi + 1 < nseg ? starts[sgi + 1] : n;
+  const uint32_t len = (uint32_t)(en - st);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
+  const SegHdr h = parse_seg(payload, offsets[sgi]);
+  uint64_t acc = 0;
+  for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) acc += seg_value(words, h, k);
+  acc = (uint64_t)block_reduce<5>((u128)acc, red);
+  if (threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long *>(d_sum), (unsigned long long)acc);
+}
+
+}  // namespace leco
+
+using namespace leco;
+
+namespace {
+int verr(int code, const std::string &m) { return leco::record_error(code, m); }
+}  // namespace
+
+extern "C" {
+
+uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg) { return 8 * n + 32 * nseg + LECO_PAYLOAD_SLACK; }
+uint64_t leco_varlen_workspace_bytes(uint64_t nseg) { return (nseg * 8 + 255) / 256 * 256 + 256; }
+uint64_t leco_varlen_max_segment(void) { return kVarlenMaxSeg; }
+
+int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, int fit_mode,
+                       uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
+                       uint64_t workspace_bytes, leco_stream_t stream) {
+  if (!d_values || !d_starts || !nseg || !n || !d_payload || !d_offsets || !d_workspace)
+    return verr(LECO_ERR_ARG, "leco_varlen_encode: null pointer or empty column");
+  if (workspace_bytes < leco_varlen_workspace_bytes(nseg)) return verr(LECO_ERR_ARG, "leco_varlen_encode: workspace too small");
+  if (nseg > 0xffffffffull || n > 0xffffffffull) return verr(LECO_ERR_ARG, "leco_varlen_encode: segments start at 32-bit indices");
+  uint32_t *err = nullptr;
+  int rc = leco::device_error_word(&err);
+  if (rc) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  uint8_t *ws = static_cast<uint8_t *>(d_workspace);
+  const uint64_t status_bytes = (nseg * 8 + 255) / 256 * 256;
+  VarArgs a{d_values, n, d_starts, nseg, d_payload, payload_cap, d_offsets, reinterpret_cast<uint64_t *>(ws),
+            reinterpret_cast<uint32_t *>(ws + status_bytes), err, fit_mode == LECO_FIT_EXACT};
+  cudaError_t e = cudaMemsetAsync(ws, 0, status_bytes + 256, st);
+  const int smem = 8 * kVarlenMaxSeg + (kVarlenMaxSeg / 32 + 9) * 4;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(varlen_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) varlen_encode_kernel<<<(unsigned)nseg, 256, smem, st>>>(a);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_encode: ") + cudaGetErrorString(e));
+}
+
+int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                       uint64_t n, uint64_t *d_out, leco_stream_t stream) {
+  if (!d_payload || !d_offsets || !d_starts || !d_out || !nseg) return verr(LECO_ERR_ARG, "leco_varlen_decode: null pointer");
+  uint32_t *err = nullptr;
+  int rc = leco::device_error_word(&err);
+  if (rc) return rc;
+  varlen_decode_kernel<<<(unsigned)nseg, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts,
+                                                                                          nseg, n, d_out, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_decode: ") + cudaGetErrorString(e));
+}
+
+int leco_varlen_gather(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                       uint64_t n, const uint64_t *d_idx, uint64_t m, uint64_t *d_out, leco_stream_t stream) {
+  if (!d_payload || !d_offsets || !d_starts || !nseg || (m && (!d_idx || !d_out)))
+    return verr(LECO_ERR_ARG, "leco_varlen_gather: null pointer");
+  if (!m) return LECO_OK;
+  uint32_t *err = nullptr;
+  int rc = leco::device_error_word(&err);
+  if (rc) return rc;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)umin64((m + 255) / 256, (uint64_t)sms * 16);
+  varlen_gather_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts, nseg, n,
+                                                                                d_idx, m, d_out, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_gather: ") + cudaGetErrorString(e));
+}
+
+int leco_varlen_sum(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
+                    uint64_t n, uint64_t *d_sum, leco_stream_t stream) {
+  if (!d_payload || !d_offsets || !d_starts || !nseg || !d_sum) return verr(LECO_ERR_ARG, "leco_varlen_sum: null pointer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(d_sum, 0, 8, st);
+  if (e == cudaSuccess) varlen_sum_kernel<<<(unsigned)nseg, 256, 0, st>>>(d_payload, d_offsets, d_starts, nseg, n, d_sum);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_sum: ") + cudaGetErrorString(e));
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+"""GPU tier: variable-length segments -- segment images byte-identical to the
+reference's, bulk decode, random access and compressed-domain sum bit-exact."""
+import numpy as np
+import pytest
+
+from test_varlen_partition import _gen
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(x, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x).view(np.int64)).to(dev)
+
+
+def test_golden_segments_bytes(lc, golden, dev):
+    x = golden["varlen__values"]
+    col = lc.varlen_encode(_dev(x, dev), golden["varlen__starts"].astype(np.uint64), lc.FIT_REFERENCE)
+    pay, off, st = col.to_host()
+    assert np.array_equal(off, golden["varlen__offsets"])
+    assert np.array_equal(pay, golden["varlen__payload"])
+    assert np.array_equal(col.decode().cpu().numpy().view(np.uint64), x)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_varlen_against_reference(lc, ref, orc, dev, kind):
+    import torch
+
+    rng = np.random.default_rng(40 + kind)
+    n = 200_000
+    x = _gen(rng, n, kind)
+    st_ref, off_ref, pay_ref, _ = ref.varlen_encode(x, 100, 12)
+    starts = lc.varlen_partition(x, 100, 12)
+    assert np.array_equal(starts, st_ref.astype(np.uint64))
+    xd = _dev(x, dev)
+    col = lc.varlen_encode(xd, starts, lc.FIT_REFERENCE)
+    pay, off, _ = col.to_host()
+    assert np.array_equal(off, off_ref) and np.array_equal(pay, pay_ref), kind
+    assert torch.equal(col.decode(), xd)
+    idx = torch.randint(0, n, (100_000,), device=dev)
+    assert torch.equal(col.gather(idx), xd[idx])
+    edge = torch.tensor([0, n - 1] + [int(s) for s in starts[:50]], device=dev, dtype=torch.int64)
+    assert torch.equal(col.gather(edge), xd[edge])
+    assert col.sum() == int(x.sum(dtype=np.uint64))
+    # the exact-fit stream decodes in the oracle's restatement of the reference decoder
+    ce = lc.varlen_encode(xd, starts, lc.FIT_EXACT)
+    pe, oe, se = ce.to_host()
+    ends = list(se[1:]) + [n]
+    for s in range(0, len(se), 7):
+        seg = pe[oe[s]:oe[s + 1]].tobytes()
+        assert np.array_equal(orc.varseg_decode(seg, int(ends[s] - se[s])), x[se[s]:ends[s]])
+    assert torch.equal(ce.decode(), xd)
+    lc.check()
+
+
+def test_varlen_short_and_raw_segments(lc, orc, dev):
+    """One- and two-value segments (sentinels 127/126) and raw segments."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    n = 5000
+    x = np.cumsum(rng.integers(0, 100, n)).astype(np.uint64)
+    x[3000:3100] = rng.integers(0, 2 ** 64 - 1, 100, dtype=np.uint64)  # forces a raw segment
+    starts = np.array([0, 1, 3, 100, 101, 3000, 3100, 4998], np.uint64)
+    xd = _dev(x, dev)
+    col = lc.varlen_encode(xd, starts)
+    pay, off, _ = col.to_host()
+    ends = list(starts[1:]) + [n]
+    for s in range(len(starts)):
+        assert pay[off[s]:off[s + 1]].tobytes() == orc.varseg_encode(x, int(starts[s]), int(ends[s]) - 1), s
+    assert torch.equal(col.decode(), xd)
+    idx = torch.arange(n, device=dev)
+    assert torch.equal(col.gather(idx), xd)
+    lc.check()
