@@ -177,8 +177,10 @@ uint64_t leco_varlen_workspace_bytes(uint64_t nseg);
 /* Longest segment leco_varlen_encode accepts (values). */
 uint64_t leco_varlen_max_segment(void);
 /* Writes every segment image (newsegment / newsegment_1 / newsegment_2, :134-272) for the
- * given starts; LECO_FIT_REFERENCE gives the reference's bytes. */
-int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, int fit_mode,
+ * given starts; LECO_FIT_REFERENCE gives the reference's bytes.  max_segment_len bounds the
+ * longest segment (0 = leco_varlen_max_segment()); it sizes the per-segment staging. */
+int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg,
+                       uint32_t max_segment_len, int fit_mode,
                        uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
                        uint64_t workspace_bytes, leco_stream_t stream);
 /* decodeArray8 over all segments (:573-626); a raw segment yields its own values. */
@@ -316,6 +318,11 @@ int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t 
 /* Reads and clears the device error word (bad index, bad header, bounded-wait
  * timeout). Synchronous. Returns LECO_OK, LECO_ERR_CORRUPT or LECO_ERR_TIMEOUT. */
 int leco_check(leco_stream_t stream);
+/* Runs the encoder's look-back wait on a predecessor that never publishes, with
+ * at most spin_limit polls (the encoder itself uses about 4 million, ~1-2 s), and
+ * returns what leco_check reports afterwards: LECO_ERR_TIMEOUT when the bounded
+ * wait gave up as designed (*h_result = ~0).  Synchronous; the context stays usable. */
+int leco_test_bounded_wait(uint32_t spin_limit, uint64_t *h_result);
 /* Message of the last error on this thread ("" if none). */
 const char *leco_last_error(void);
 /* Library version string. */

@@ -94,10 +94,11 @@ SIGNATURES = [
     ("leco_varlen_max_payload_bytes", _U64, [_U64, _U64]),
     ("leco_varlen_workspace_bytes", _U64, [_U64]),
     ("leco_varlen_max_segment", _U64, []),
-    ("leco_varlen_encode", _I, [_P, _U64, _P, _U64, _I, _P, _U64, _P, _P, _U64, _P]),
+    ("leco_varlen_encode", _I, [_P, _U64, _P, _U64, _U32, _I, _P, _U64, _P, _P, _U64, _P]),
     ("leco_varlen_decode", _I, [_P, _P, _P, _U64, _U64, _P, _P]),
     ("leco_varlen_gather", _I, [_P, _P, _P, _U64, _U64, _P, _U64, _P, _P]),
     ("leco_varlen_sum", _I, [_P, _P, _P, _U64, _U64, _P, _P]),
+    ("leco_test_bounded_wait", _I, [_U32, _P]),
     ("leco_check", _I, [_P]),
     ("leco_last_error", ctypes.c_char_p, []),
     ("leco_version", ctypes.c_char_p, []),
@@ -611,12 +612,18 @@ class VarlenColumn:
         return self.payload[: int(off[-1])].cpu().numpy(), off, self.starts.cpu().numpy().view(np.uint64)
 
 
-def varlen_encode(values, starts, fit_mode: int = FIT_REFERENCE, stream=None) -> VarlenColumn:
-    """Encodes a uint64 CUDA tensor (int64 view) with the given segment starts."""
+def varlen_encode(values, starts, fit_mode: int = FIT_REFERENCE, stream=None, max_segment_len: int = 0) -> VarlenColumn:
+    """Encodes a uint64 CUDA tensor (int64 view) with the given segment starts
+    (host numpy array, or a CUDA tensor together with max_segment_len)."""
     torch = _torch()
     L = lib()
     n = values.numel()
-    st = starts if hasattr(starts, "is_cuda") else torch.from_numpy(np.ascontiguousarray(starts, np.uint64).view(np.int64))
+    if not hasattr(starts, "is_cuda"):
+        sh = np.ascontiguousarray(starts, np.uint64)
+        max_segment_len = int(np.max(np.diff(np.append(sh, np.uint64(n))))) if len(sh) else 0
+        st = torch.from_numpy(sh.view(np.int64))
+    else:
+        st = starts
     st = st.to(values.device)
     ns = st.numel()
     cap = L.leco_varlen_max_payload_bytes(n, ns)
@@ -624,6 +631,8 @@ def varlen_encode(values, starts, fit_mode: int = FIT_REFERENCE, stream=None) ->
     off = torch.empty(ns + 1, dtype=torch.int64, device=values.device)
     wsb = L.leco_varlen_workspace_bytes(ns)
     ws = torch.empty(wsb, dtype=torch.uint8, device=values.device)
-    _check(L.leco_varlen_encode(_tptr(values), n, _tptr(st), ns, fit_mode, _tptr(pay), cap, _tptr(off), _tptr(ws), wsb,
-                                _stream_ptr(stream)), "leco_varlen_encode")
-    return VarlenColumn(n, st, pay, off)
+    _check(L.leco_varlen_encode(_tptr(values), n, _tptr(st), ns, max_segment_len, fit_mode, _tptr(pay), cap, _tptr(off),
+                                _tptr(ws), wsb, _stream_ptr(stream)), "leco_varlen_encode")
+    col = VarlenColumn(n, st, pay, off)
+    col.max_segment_len = max_segment_len
+    return col

@@ -18,6 +18,8 @@
 // packers write_delta_int_T / write_FOR_int_T (bit_write.h:257-390).
 #include "leco_encode.cuh"
 
+#include <string>
+
 namespace leco {
 
 template <typename T, int CODEC>
@@ -98,4 +100,32 @@ int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st) {
   return -1;
 }
 
+// Bounded-wait check: block 1 of a two-block look-back whose block 0 never
+// publishes its size (a status word nothing sets).  The wait must give up after
+// `spin_limit` polls, set the error word and return.
+__global__ void lookback_timeout_probe_kernel(uint64_t *status, uint32_t *error, uint32_t spin_limit, uint64_t *result) {
+  if (threadIdx.x < 32) {
+    const uint64_t excl = lookback_prefix(status, 1, 16, error, spin_limit);
+    if (threadIdx.x == 0) *result = excl;
+  }
+}
+
 }  // namespace leco
+
+extern "C" int leco_test_bounded_wait(uint32_t spin_limit, uint64_t *h_result) {
+  using namespace leco;
+  uint32_t *err = nullptr;
+  int rc = device_error_word(&err);
+  if (rc) return rc;
+  uint64_t *buf = nullptr;  // [2] status words + [1] result
+  cudaError_t e = cudaMalloc(&buf, 3 * sizeof(uint64_t));
+  if (e == cudaSuccess) e = cudaMemset(buf, 0, 3 * sizeof(uint64_t));
+  if (e == cudaSuccess) {
+    lookback_timeout_probe_kernel<<<1, 32>>>(buf, err, spin_limit, buf + 2);
+    e = cudaDeviceSynchronize();
+  }
+  if (e == cudaSuccess && h_result) e = cudaMemcpy(h_result, buf + 2, sizeof(uint64_t), cudaMemcpyDeviceToHost);
+  if (buf) cudaFree(buf);
+  if (e != cudaSuccess) return record_error(LECO_ERR_CUDA, std::string("leco_test_bounded_wait: ") + cudaGetErrorString(e));
+  return leco_check(nullptr);
+}

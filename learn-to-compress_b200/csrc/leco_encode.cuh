@@ -60,7 +60,8 @@ __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
 // Decoupled look-back (single-pass prefix sum over block image sizes).  Run by
 // warp 0.  Returns the exclusive prefix; on a wait that exceeds the spin limit
 // sets kErrTimeout and returns ~0.
-__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error) {
+__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error,
+                                                    uint32_t spin_limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
   if (b == 0) {
     if (lane == 0) st_relaxed(&status[0], kFlagIncl | my);
@@ -76,7 +77,7 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
     for (;;) {
       if (idx >= 0) v = ld_relaxed(&status[idx]);
       if (__all_sync(0xffffffffu, (v >> 62) != 0)) break;
-      if (++spins > kSpinLimit) {
+      if (++spins > spin_limit) {
         if (lane == 0) atomicOr(error, kErrTimeout);
         return ~0ull;
       }

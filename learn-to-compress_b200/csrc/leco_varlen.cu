@@ -42,6 +42,7 @@ struct VarArgs {
   uint32_t *ticket;
   uint32_t *error;
   int exact_fit;
+  uint32_t max_seg;  // longest segment of this partition (sizes the shared-memory stage)
 };
 
 __device__ __forceinline__ uint64_t seg_bytes(uint32_t l, uint32_t len) {
@@ -61,14 +62,14 @@ __global__ void __launch_bounds__(256) varlen_encode_kernel(VarArgs a) {
   __shared__ uint8_t hdr[32];
   __shared__ double s_model[2];
   uint64_t *vals = reinterpret_cast<uint64_t *>(smem_raw);
-  uint32_t *signs = reinterpret_cast<uint32_t *>(smem_raw + 8 * kVarlenMaxSeg);
+  uint32_t *signs = reinterpret_cast<uint32_t *>(smem_raw + 8 * (size_t)a.max_seg);
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
   if (tid == 0) s_ticket = atomicAdd(a.ticket, 1u);
   __syncthreads();
   const uint64_t sgi = s_ticket;
   if (sgi >= a.nseg) return;
   const uint64_t st = a.starts[sgi], en = sgi + 1 < a.nseg ? a.starts[sgi + 1] : a.n;
-  if (en <= st || en - st > kVarlenMaxSeg || en > a.n) {  // bad partition: report, keep successors moving
+  if (en <= st || en - st > a.max_seg || en > a.n) {  // bad partition: report, keep successors moving
     if (tid < 32) lookback_prefix(a.status, sgi, 0, a.error);
     if (tid == 0) atomicOr(a.error, kErrBadHeader);
     return;
@@ -215,6 +216,9 @@ __device__ __forceinline__ uint64_t seg_value(const uint64_t *words, const SegHd
 }
 
 // One CTA per segment (Leco_cost_merge_double_wo_round::decodeArray8, :573-626).
+// Fields of at most 32 bits are extracted with one 32-bit funnel shift; when
+// every prediction of the segment lies inside (-2^62, 2^62) the uint64_t
+// conversion needs no out-of-range handling.
 __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *payload, const uint64_t *offsets,
                                                             const uint64_t *starts, uint64_t nseg, uint64_t n,
                                                             uint64_t *out, uint32_t *error) {
@@ -225,6 +229,22 @@ __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *paylo
   const SegHdr h = parse_seg(payload, offsets[sgi]);
   if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
     if (threadIdx.x == 0) atomicOr(error, kErrBadHeader);
+    return;
+  }
+  const bool fast = fabs(h.t0) + fabs(h.slope) * __uint2double_rn(len) < 4611686018427387904.0;
+  if (h.l >= 1 && h.l <= 32 && fast) {
+    const uint32_t *w32 = reinterpret_cast<const uint32_t *>(payload) + (h.body_bit >> 5);
+    const uint32_t bsh = (uint32_t)(h.body_bit & 31), l = h.l, mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
+    const uint32_t sb = l - 1, m1 = mask >> 1;
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+      const uint32_t r = bsh + k * l;
+      const uint32_t *p = w32 + (r >> 5);
+      const uint32_t f = __funnelshift_r(__ldg(p), __ldg(p + 1), r) & mask;
+      const int64_t pred = __double2ll_rz(__dadd_rn(h.t0, __dmul_rn(__uint2double_rn(k), h.slope)));
+      const uint32_t mag = f & m1;
+      const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
+      __stcs(out + st + k, (uint64_t)(pred + d));
+    }
     return;
   }
   const uint32_t cnt = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
@@ -285,11 +305,14 @@ uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg) { return 8 * n
 uint64_t leco_varlen_workspace_bytes(uint64_t nseg) { return (nseg * 8 + 255) / 256 * 256 + 256; }
 uint64_t leco_varlen_max_segment(void) { return kVarlenMaxSeg; }
 
-int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, int fit_mode,
-                       uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
+int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, uint32_t max_segment_len,
+                       int fit_mode, uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
                        uint64_t workspace_bytes, leco_stream_t stream) {
   if (!d_values || !d_starts || !nseg || !n || !d_payload || !d_offsets || !d_workspace)
     return verr(LECO_ERR_ARG, "leco_varlen_encode: null pointer or empty column");
+  if (!max_segment_len) max_segment_len = kVarlenMaxSeg;
+  if (max_segment_len > kVarlenMaxSeg)
+    return verr(LECO_ERR_UNSUPPORTED, "leco_varlen_encode: segments longer than 16384 values are not supported");
   if (workspace_bytes < leco_varlen_workspace_bytes(nseg)) return verr(LECO_ERR_ARG, "leco_varlen_encode: workspace too small");
   if (nseg > 0xffffffffull || n > 0xffffffffull) return verr(LECO_ERR_ARG, "leco_varlen_encode: segments start at 32-bit indices");
   uint32_t *err = nullptr;
@@ -299,10 +322,11 @@ int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_s
   uint8_t *ws = static_cast<uint8_t *>(d_workspace);
   const uint64_t status_bytes = (nseg * 8 + 255) / 256 * 256;
   VarArgs a{d_values, n, d_starts, nseg, d_payload, payload_cap, d_offsets, reinterpret_cast<uint64_t *>(ws),
-            reinterpret_cast<uint32_t *>(ws + status_bytes), err, fit_mode == LECO_FIT_EXACT};
+            reinterpret_cast<uint32_t *>(ws + status_bytes), err, fit_mode == LECO_FIT_EXACT, max_segment_len};
   cudaError_t e = cudaMemsetAsync(ws, 0, status_bytes + 256, st);
-  const int smem = 8 * kVarlenMaxSeg + (kVarlenMaxSeg / 32 + 9) * 4;
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(varlen_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int smem = 8 * max_segment_len + (max_segment_len / 32 + 9) * 4;
+  if (e == cudaSuccess && smem > 48 * 1024)
+    e = cudaFuncSetAttribute(varlen_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess) varlen_encode_kernel<<<(unsigned)nseg, 256, smem, st>>>(a);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_encode: ") + cudaGetErrorString(e));

@@ -218,3 +218,19 @@ def test_staged_decode_large_mixed(lc, orc, dev, s):
         c2 = lc.Column.from_host(codec, s, 1_100_000, 1000, pay, off)
         assert np.array_equal(to_np(c2.decode(), s), x[:1_100_000]), codec
     lc.check()
+
+
+def test_bounded_wait_times_out_without_faulting(lc):
+    """Failure detection on the GPU: a look-back wait on a flag nothing sets gives
+    up after its poll limit, the kernel reports LECO_ERR_TIMEOUT through the error
+    word and the context keeps working."""
+    import ctypes
+
+    import torch
+
+    res = ctypes.c_uint64()
+    rc = lc.lib().leco_test_bounded_wait(2000, ctypes.byref(res))
+    assert rc == -5 and res.value == 0xFFFFFFFFFFFFFFFF
+    lc.check()  # the error word was read and cleared
+    x = torch.arange(10000, dtype=torch.int64, device="cuda:0") * 3
+    assert torch.equal(lc.encode(x, lc.LINEAR, 1000).decode(), x)
