@@ -194,6 +194,45 @@ __device__ __forceinline__ u128 block_reduce(u128 v, u128 *red) {
   return red[32];
 }
 
+// Two block-wide reductions in one shared-memory round: `red` needs 66 entries.
+template <int OPA, int OPB>
+__device__ __forceinline__ void block_reduce2(u128 &a, u128 &b, u128 *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  auto wred = [](u128 x, int op) -> u128 {
+    switch (op) {
+      case 0: return warp_sum_u128(x);
+      case 1: return warp_max_u64((uint64_t)x);
+      case 2: return warp_min_u64((uint64_t)x);
+      case 3: return (u128)(uint64_t)warp_max_i64((int64_t)(uint64_t)x);
+      case 4: return (u128)(uint64_t)warp_min_i64((int64_t)(uint64_t)x);
+      default: return warp_sum_u64((uint64_t)x);
+    }
+  };
+  auto ident = [](int op) -> u128 {
+    return op == 2 ? (u128)~0ull : op == 3 ? (u128)0x8000000000000000ull : op == 4 ? (u128)0x7fffffffffffffffull : (u128)0;
+  };
+  a = wred(a, OPA);
+  b = wred(b, OPB);
+  __syncthreads();
+  if (lane == 0) {
+    red[warp] = a;
+    red[33 + warp] = b;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    u128 x = lane < nw ? red[lane] : ident(OPA), y = lane < nw ? red[33 + lane] : ident(OPB);
+    x = wred(x, OPA);
+    y = wred(y, OPB);
+    if (lane == 0) {
+      red[32] = x;
+      red[65] = y;
+    }
+  }
+  __syncthreads();
+  a = red[32];
+  b = red[65];
+}
+
 // ---- thread groups ----------------------------------------------------------
 // A block of values is processed either by a whole CTA (G = CTA size) or by one
 // warp (G = 32, several small blocks per CTA).  These helpers give the rank in
@@ -218,6 +257,16 @@ __device__ __forceinline__ u128 group_reduce(u128 v, u128 *red) {
     case 4: return (u128)(uint64_t)warp_min_i64((int64_t)(uint64_t)v);
     default: return warp_sum_u64((uint64_t)v);
   }
+}
+
+template <int OPA, int OPB, int G>
+__device__ __forceinline__ void group_reduce2(u128 &a, u128 &b, u128 *red) {
+  if (G != 32) {
+    block_reduce2<OPA, OPB>(a, b, red);
+    return;
+  }
+  a = group_reduce<OPA, 32>(a, red);
+  b = group_reduce<OPB, 32>(b, red);
 }
 
 // ---- relaxed global word access for the look-back scan ----------------------

@@ -37,7 +37,7 @@ template <typename T>
 struct EncSmem {
   T *vals;          // [bs] values, later residual magnitudes (linear / poly2)
   uint32_t *signs;  // [bs/32 + 9] sign bits (one word per 32 values, rounded up to 256)
-  u128 *red;        // [33]
+  u128 *red;        // [66]
   uint8_t *hdr;     // [32] header bytes
   uint64_t *bcast;  // [8]
 };
@@ -45,16 +45,16 @@ struct EncSmem {
 template <typename T>
 __device__ __forceinline__ EncSmem<T> enc_smem(uint8_t *base, uint32_t bs) {
   EncSmem<T> s;
-  s.red = reinterpret_cast<u128 *>(base);                      // 33 * 16 = 528
-  s.bcast = reinterpret_cast<uint64_t *>(base + 528);          // 8 * 8 = 64
-  s.hdr = base + 592;                                          // 32
-  s.signs = reinterpret_cast<uint32_t *>(base + 624);          // (bs/32+9)*4
-  uint32_t soff = 624 + ((bs / 32 + 9) * 4 + 15) / 16 * 16;
+  s.red = reinterpret_cast<u128 *>(base);                      // 66 * 16 = 1056
+  s.bcast = reinterpret_cast<uint64_t *>(base + 1056);         // 8 * 8 = 64
+  s.hdr = base + 1120;                                         // 32
+  s.signs = reinterpret_cast<uint32_t *>(base + 1152);         // (bs/32+9)*4
+  uint32_t soff = 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16;
   s.vals = reinterpret_cast<T *>(base + soff);
   return s;
 }
 __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
-  return 624 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + bs * s;
+  return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + bs * s;
 }
 
 // Decoupled look-back (single-pass prefix sum over block image sizes).  Run by
@@ -98,6 +98,13 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
   return excl;
 }
 
+// True when every prediction of a len-value block with model (a0, a1, a2) is a
+// finite double inside (-2^62, 2^62): the x86 out-of-range rule cannot apply.
+__device__ __forceinline__ bool model_in_range(double a0, double a1, double a2, uint32_t len) {
+  const double L = __uint2double_rn(len ? len - 1 : 0);
+  return fabs(a0) + fabs(a1) * L + fabs(a2) * L * L < 4611686018427387904.0;
+}
+
 // Image writer: writes image bytes [0, size) of a block to payload[goff...].
 // Image byte i < H is hdr[i]; byte i >= H is byte (i-H) of the LSB-first
 // concatenation of fields 0..n-1 (l bits each), zero past the last field.
@@ -115,6 +122,31 @@ __device__ __forceinline__ uint64_t gather_bits(uint32_t p, uint32_t nbits, uint
   return (uint64_t)acc & lowmask(nbits);
 }
 
+// 128 bits of the body starting at body bit p, for fields of at most 32 bits:
+// 32-bit output words assembled in a 64-bit accumulator; k0 = p / l through a
+// reciprocal (exact for p < 2^21 and l <= 64).
+template <typename FieldFn>
+__device__ __forceinline__ uint4 gather128_narrow(uint32_t p, uint32_t l, uint32_t rcp, uint32_t n, FieldFn field) {
+  uint32_t k = l == 1 ? p : __umulhi(p, rcp);
+  const uint32_t o = p - k * l;
+  uint64_t acc = k < n ? ((uint64_t)field(k) >> o) : 0;
+  uint32_t have = l - o;
+  ++k;
+  uint32_t w[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    while (have < 32) {
+      if (k < n) acc |= (uint64_t)field(k) << have;
+      have += l;
+      ++k;
+    }
+    w[q] = (uint32_t)acc;
+    acc >>= 32;
+    have -= 32;
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 template <typename FieldFn>
 __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
                                             const uint8_t *hdr, uint32_t l, uint32_t nfields, FieldFn field,
@@ -122,13 +154,18 @@ __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uin
   const uint64_t gend = goff + size;
   const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
   const uint64_t body0 = goff + H;  // first body byte (global)
+  const uint32_t rcp = l > 1 ? (uint32_t)((0x100000000ull + l - 1) / l) : 0;  // ceil(2^32 / l); l == 1 divides trivially
   for (uint64_t c = c0 + rank; c < c1; c += nthreads) {
     const uint64_t cb = c << 4;
     if (cb >= body0 && cb + 16 <= gend && l) {
       uint32_t p = (uint32_t)((cb - body0) * 8);
-      uint64_t lo = gather_bits(p, 64, l, nfields, field);
-      uint64_t hi = gather_bits(p + 64, 64, l, nfields, field);
-      *reinterpret_cast<ulonglong2 *>(payload + cb) = make_ulonglong2(lo, hi);
+      if (l <= 32) {
+        *reinterpret_cast<uint4 *>(payload + cb) = gather128_narrow(p, l, rcp, nfields, field);
+      } else {
+        uint64_t lo = gather_bits(p, 64, l, nfields, field);
+        uint64_t hi = gather_bits(p + 64, 64, l, nfields, field);
+        *reinterpret_cast<ulonglong2 *>(payload + cb) = make_ulonglong2(lo, hi);
+      }
     } else {
       for (int j = 0; j < 16; ++j) {
         uint64_t g = cb + j;
@@ -191,8 +228,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         siy += (u128)y * i;
         if (CODEC == kPoly2) sqy += (u128)y * ((uint64_t)i * i);
       }
-      sy = group_reduce<0, G>(sy, sm.red);
-      siy = group_reduce<0, G>(siy, sm.red);
+      group_reduce2<0, 0, G>(sy, siy, sm.red);
       if (CODEC == kPoly2) sqy = group_reduce<0, G>(sqy, sm.red);
       const double md = __uint2double_rn(len);
       if (CODEC == kLinear) {
@@ -218,18 +254,24 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
     if (CODEC == kLinear) {
       // ---- midpoint shift (piecewise_fix_integer_template.h:36-46) -----------
       int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
+      const bool fast = model_in_range(m0, m1, 0.0, len);
       for (uint32_t i = tid; i < len; i += nt) {
-        int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)f2i_x86(pred_linear(m0, m1, i)));
+        const double p = pred_linear(m0, m1, i);
+        const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
+        int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)pr);
         dmax = d > dmax ? d : dmax;
         dmin = d < dmin ? d : dmin;
       }
-      dmax = (int64_t)(uint64_t)group_reduce<3, G>((u128)(uint64_t)dmax, sm.red);
-      dmin = (int64_t)(uint64_t)group_reduce<4, G>((u128)(uint64_t)dmin, sm.red);
+      u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
+      group_reduce2<3, 4, G>(rmx, rmn, sm.red);
+      dmax = (int64_t)(uint64_t)rmx;
+      dmin = (int64_t)(uint64_t)rmn;
       const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
       m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
     }
     // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
     uint64_t rmax = 0;
+    const bool fast = model_in_range(m0, m1, CODEC == kPoly2 ? m2 : 0.0, len);
     for (uint32_t i0 = 0; i0 < len; i0 += nt) {
       const uint32_t i = i0 + tid;
       bool pos = false;
@@ -237,11 +279,13 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         const uint64_t y = (uint64_t)sm.vals[i];
         uint64_t r;
         if (CODEC == kLinear) {
-          const int64_t pred = f2i_x86(pred_linear(m0, m1, i));
+          const double p = pred_linear(m0, m1, i);
+          const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
           pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
           r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
         } else {
-          const int64_t pred = f2i_x86(pred_poly2(m0, m1, m2, __uint2double_rn(i)));
+          const double p = pred_poly2(m0, m1, m2, __uint2double_rn(i));
+          const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
           pos = (int64_t)y > pred;
           r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
         }
@@ -263,8 +307,10 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       mn = y < mn ? y : mn;
       mx = y > mx ? y : mx;
     }
-    mn = (uint64_t)group_reduce<2, G>((u128)mn, sm.red);
-    mx = (uint64_t)group_reduce<1, G>((u128)mx, sm.red);
+    u128 rmn = (u128)mn, rmx = (u128)mx;
+    group_reduce2<2, 1, G>(rmn, rmx, sm.red);
+    mn = (uint64_t)rmn;
+    mx = (uint64_t)rmx;
     fbase = mn;
     m1 = __longlong_as_double((long long)mx);
     l = bits_of(mx - mn);
