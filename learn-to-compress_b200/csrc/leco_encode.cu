@@ -46,6 +46,76 @@ __global__ void __launch_bounds__(256) encode_kernel_warp(EncodeArgs a, uint32_t
   encode_block<T, CODEC, 32>(a, b, smem_raw + (size_t)w * slice);
 }
 
+// Sequential reference fits, one warp per 32 blocks: each step the warp loads a
+// 32 x 32 tile (32 consecutive values of each of its 32 blocks, coalesced) into
+// shared memory while the next tile is already in flight to registers; lane j
+// then adds the 32 values of block j to its running sums in order, exactly the
+// reference's loop (lr.h:72-77; Y sums of polynomial_regression_internals.hpp:129-137).
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(128) seq_fit_tiled_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs,
+                                                            uint64_t nb, PolyX px, double *__restrict__ models) {
+  __shared__ T tile[4][32][33];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t b0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+  if (b0 >= nb) return;
+  const uint64_t mine = b0 + lane;
+  const uint32_t len = mine < nb ? (uint32_t)umin64(bs, n - mine * bs) : 0;
+  T nxt[32];
+  // value i of row r exists when block b0 + r exists and i < its length
+  auto fetch = [&](uint32_t t0) {
+    const uint32_t i = t0 + lane;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const uint64_t g = (b0 + r) * bs + i;
+      nxt[r] = (b0 + r < nb && i < bs && g < n) ? __ldg(values + g) : (T)0;
+    }
+  };
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;  // linear: sumx sumy sumxx sumxy; poly: Y0 Y1 Y2
+  uint32_t maxlen = len;
+  for (int m = 16; m; m >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
+  fetch(0);
+  for (uint32_t t0 = 0; t0 < maxlen; t0 += 32) {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) tile[w][r][lane] = nxt[r];
+    __syncwarp();
+    if (t0 + 32 < maxlen) fetch(t0 + 32);
+    const uint32_t cnt = len > t0 ? (len - t0 < 32 ? len - t0 : 32) : 0;
+    for (uint32_t c = 0; c < cnt; ++c) {
+      const uint32_t i = t0 + c;
+      const double di = __uint2double_rn(i), yi = to_double<T>(tile[w][lane][c]);
+      if (CODEC == kLinear) {
+        s0 = __dadd_rn(s0, di);
+        s1 = __dadd_rn(s1, yi);
+        s2 = __dadd_rn(s2, __dmul_rn(di, di));
+        s3 = __dadd_rn(s3, __dmul_rn(di, yi));
+      } else {
+        s0 = __dadd_rn(s0, __dmul_rn(1.0, yi));
+        s1 = __dadd_rn(s1, __dmul_rn(di, yi));
+        s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yi));
+      }
+    }
+    __syncwarp();
+  }
+  if (!len) return;
+  double *m = models + mine * 3;
+  if (CODEC == kLinear) {
+    const double md = __uint2double_rn(len);
+    const double ccc = __dsub_rn(__dmul_rn(s3, md), __dmul_rn(s0, s1));
+    const double xxx = __dsub_rn(__dmul_rn(s2, md), __dmul_rn(s0, s0));
+    const double t1 = __ddiv_rn(ccc, xxx);
+    m[0] = __ddiv_rn(__dsub_rn(s1, __dmul_rn(t1, s0)), md);
+    m[1] = t1;
+    m[2] = 0.0;
+  } else {
+    const double *X = px.x + (len == bs ? 0 : 5);
+    double Y[3] = {s0, s1, s2}, c[3];
+    poly2_solve(X, Y, c);
+    m[0] = c[0];
+    m[1] = c[1];
+    m[2] = c[2];
+  }
+}
+
 template <typename T, int CODEC>
 __global__ void __launch_bounds__(128) seq_fit_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t nb,
                                                        PolyX px, double *__restrict__ models) {
@@ -64,8 +134,8 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
   PolyX px;
   for (int i = 0; i < 10; ++i) a.polyX[i] = px.x[i] = L.polyX[i];
   if (L.seq_models && (CODEC == kLinear || CODEC == kPoly2)) {
-    const int tpb = 128;
-    seq_fit_kernel<T, CODEC><<<(unsigned)((L.nb + tpb - 1) / tpb), tpb, 0, st>>>(
+    // four warps per CTA, 32 blocks per warp
+    seq_fit_tiled_kernel<T, CODEC><<<(unsigned)((L.nb + 127) / 128), 128, 0, st>>>(
         reinterpret_cast<const T *>(L.values), L.n, L.bs, L.nb, px, L.seq_models);
     a.seq_models = L.seq_models;
   }
