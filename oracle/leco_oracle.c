@@ -608,3 +608,251 @@ uint64_t oracle_column_sum(int codec, const uint8_t *payload, const uint64_t *of
   for (size_t i = 0; i < n; i++) acc += ld(scratch, s, i);
   return acc;
 }
+
+/* ---- predicate pushdown ------------------------------------------------- */
+
+/* (int)x as x86-64 compiles it (32-bit CVTTSD2SI): NaN and values outside the
+ * int range give INT_MIN.  The filters store their FP64 index thresholds in
+ * int (piecewise_fix_integer_template.h:226,275-276). */
+static int32_t x86_f2i32(double x) {
+  if (x > -2147483649.0 && x < 2147483648.0) return (int32_t)x;
+  return INT32_MIN;
+}
+/* std::max(a, b) = (a < b) ? b : a and std::min(a, b) = (b < a) ? b : a, as
+ * the filters call them (a NaN first argument passes through). */
+static double std_max(double a, double b) { return a < b ? b : a; }
+static double std_min(double a, double b) { return b < a ? b : a; }
+
+/* Comparisons of a decoded value with a filter bound of type T: for T =
+ * uint64_t the reference compares int64_t with T, i.e. unsigned; for T =
+ * uint32_t the bound is promoted to int64_t and the comparison is signed
+ * (bit_read.h:421,477; piecewise_fix_integer_template.h:241,286). */
+static int cmp_gt(uint64_t v, uint64_t f, int s) { return s == 8 ? v > f : (int64_t)v > (int64_t)f; }
+static int cmp_lt(uint64_t v, uint64_t f, int s) { return s == 8 ? v < f : (int64_t)v < (int64_t)f; }
+
+/* Value k of a packed LeCo block as the filter readers compute it:
+ * (long long)(theta0 + k*theta1) minus or plus the field's magnitude, in
+ * wrapping 64-bit arithmetic (bit_read.h:409-420,465-476); l == 0: the
+ * prediction alone (piecewise_fix_integer_template.h:240,285). */
+static uint64_t leco_filter_value(const uint8_t *body, unsigned l, double t0, double t1, int64_t k) {
+  uint64_t v = (uint64_t)x86_f2i(t0 + (double)k * t1);
+  if (!l) return v;
+  uint64_t f = get_field(body, (uint64_t)k * l, l);
+  uint64_t mag = f & ((1ull << (l - 1)) - 1);
+  return ((f >> (l - 1)) & 1) ? v + mag : v - mag;
+}
+
+/* 1L << (l-1), the model's residual bound (:221-224, :270-273). */
+static int64_t delta_interval(unsigned l) { return l ? (int64_t)1 << (l - 1) : 0; }
+
+/* (double)(filter + c) for a bound of type T plus an int64_t offset c: T =
+ * uint64_t wraps modulo 2^64 and converts as unsigned; T = uint32_t computes in
+ * int64_t (:226, :275-276).  plus_one adds the int 1 first, in T (:226). */
+static double bound_to_double(uint64_t filter, int plus_one, int64_t c, int s) {
+  if (s == 8) return (double)(filter + (uint64_t)plus_one + (uint64_t)c);
+  uint32_t f = (uint32_t)filter + (uint32_t)plus_one;
+  return (double)((int64_t)f + c);
+}
+
+/* Leco_int<T>::filter_range (piecewise_fix_integer_template.h:206-252) with
+ * read_all_bit_fix_range (bit_read.h:388-445): the indices block_start + k of
+ * the values above `filter`, scanned from the model's threshold
+ * thre = (int)max((filter + 1 - 2^(l-1) - theta0) / theta1, 0).  A raw block
+ * (l == 8s), which the reference does not recognise here (its result would
+ * come from shifts by the type width), is scanned as its stored values.
+ * Returns the count. */
+size_t oracle_leco_filter(const uint8_t *in, int s, size_t n, uint64_t filter, uint32_t block_start, uint32_t *out) {
+  unsigned l = in[0];
+  size_t c = 0;
+  filter &= tmask(s);
+  if (l == 8u * (unsigned)s) {
+    for (size_t k = 0; k < n; k++)
+      if (rdT(in + 1 + k * (size_t)s, s) > filter) out[c++] = block_start + (uint32_t)k;
+    return c;
+  }
+  double t0 = rdf64(in + 1), t1 = rdf64(in + 9);
+  int32_t thre = x86_f2i32(std_max((bound_to_double(filter, 1, -delta_interval(l), s) - t0) / t1, 0.));
+  if ((uint64_t)(int64_t)thre >= n) return 0; /* :227 compares int with size_t */
+  for (size_t k = (size_t)thre; k < n; k++)
+    if (cmp_gt(leco_filter_value(in + 17, l, t0, t1, (int64_t)k), filter, s)) out[c++] = block_start + (uint32_t)k;
+  return c;
+}
+
+/* Leco_int<T>::filter_range_close (piecewise_fix_integer_template.h:254-303)
+ * with read_all_bit_fix_range_close (bit_read.h:447-502): for the windows
+ * (filter1 + p*base, filter2 + p*base), p = 0, 1, ... (bounds wrap in T), the
+ * indices whose value lies strictly inside, scanned over the model's index range
+ * [thre1, thre2) per window ([thre1, thre2] for l == 0, :281) until
+ * thre1 >= length or thre2 <= 0.
+ * overwrite = 1 reproduces the reference's output pointer exactly: for l > 0
+ * every window's indices are written from out[0] again (the reader is passed
+ * `out`, not the advanced position, :280), so earlier windows' indices are
+ * overwritten; overwrite = 0 writes them one after another.  The count is the
+ * same.  Raw blocks: every stored value is counted once when it lies in some
+ * window.  max_periods bounds the window loop (0 = unbounded); returns the
+ * count, or SIZE_MAX when the bound was reached. */
+size_t oracle_leco_filter_close(const uint8_t *in, int s, size_t n, uint64_t filter1, uint64_t filter2, int32_t base,
+                                uint32_t block_start, uint32_t *out, int overwrite, uint64_t max_periods) {
+  unsigned l = in[0];
+  size_t c = 0;
+  const uint64_t mask = tmask(s);
+  filter1 &= mask;
+  filter2 &= mask;
+  if (l == 8u * (unsigned)s) {
+    const uint64_t b = (uint64_t)(int64_t)base & mask;
+    for (size_t k = 0; k < n; k++) {
+      uint64_t v = rdT(in + 1 + k * (size_t)s, s);
+      if (v <= filter1 || filter2 <= filter1 || b == 0) continue;
+      uint64_t m = (v - filter1 - 1) % b; /* the largest window start below v is v - m - 1 */
+      if (m + 1 < filter2 - filter1) out[c++] = block_start + (uint32_t)k;
+    }
+    return c;
+  }
+  double t0 = rdf64(in + 1), t1 = rdf64(in + 9);
+  const int64_t di = delta_interval(l);
+  const uint64_t step = (uint64_t)(int64_t)base & mask; /* filter += base in T (:290-291) */
+  uint64_t p = 0;
+  for (;;) {
+    int32_t thre1 = x86_f2i32(std_max((bound_to_double(filter1, 0, -di, s) - t0) / t1 - 1, 0.));
+    int32_t thre2 = x86_f2i32(std_min((bound_to_double(filter2, 0, di, s) - t0) / t1 + 1, (double)n));
+    if (!((uint64_t)(int64_t)thre1 < n && thre2 > 0)) break;
+    if (max_periods && p == max_periods) return (size_t)-1;
+    uint32_t *o = (overwrite && l) ? out : out + c;
+    size_t pc = 0;
+    int64_t hi = l ? (int64_t)thre2 : (int64_t)thre2 + 1;
+    for (int64_t k = thre1; k < hi; k++) {
+      uint64_t v = leco_filter_value(in + 17, l, t0, t1, k);
+      if (cmp_gt(v, filter1, s) && cmp_lt(v, filter2, s)) o[pc++] = block_start + (uint32_t)k;
+    }
+    c += pc;
+    filter1 = (filter1 + step) & mask;
+    filter2 = (filter2 + step) & mask;
+    p++;
+  }
+  return c;
+}
+
+/* FOR_int<T>::filter_range (FOR_integer_template.h:115-160) with
+ * filter_read_all_bit_FOR (bit_read.h:1417-1459): values above `filter`; the
+ * header maximum rejects a block unread (:143).  Raw iff l == 8s (the
+ * reference's `l >= 8s-1` test reads an l == 8s-1 packed block as raw). */
+size_t oracle_for_filter(const uint8_t *in, int s, size_t n, uint64_t filter, uint32_t block_start, uint32_t *out) {
+  unsigned l = in[0];
+  size_t c = 0;
+  filter &= tmask(s);
+  if (l == 8u * (unsigned)s) {
+    for (size_t k = 0; k < n; k++)
+      if (rdT(in + 1 + k * (size_t)s, s) > filter) out[c++] = block_start + (uint32_t)k;
+    return c;
+  }
+  uint64_t m = rdT(in + 1, s), M = rdT(in + 1 + s, s);
+  if (M <= filter) return 0;
+  for (size_t k = 0; k < n; k++) {
+    uint64_t v = l ? (m + get_field(in + 1 + 2 * s, (uint64_t)k * l, l)) & tmask(s) : m;
+    if (v > filter) out[c++] = block_start + (uint32_t)k;
+  }
+  return c;
+}
+
+/* FOR_int<T>::filter_range_close (FOR_integer_template.h:166-215) with
+ * filter_read_all_bit_FOR_close (bit_read.h:1462-1505): values v with
+ * filter1 < v % base < filter2 (base converted to T). */
+size_t oracle_for_filter_close(const uint8_t *in, int s, size_t n, uint64_t filter1, uint64_t filter2, int32_t base,
+                               uint32_t block_start, uint32_t *out) {
+  unsigned l = in[0];
+  size_t c = 0;
+  const uint64_t mask = tmask(s), b = (uint64_t)(int64_t)base & mask;
+  filter1 &= mask;
+  filter2 &= mask;
+  if (b == 0) return 0;
+  int raw = l == 8u * (unsigned)s;
+  uint64_t m = raw ? 0 : rdT(in + 1, s);
+  for (size_t k = 0; k < n; k++) {
+    uint64_t v = raw ? rdT(in + 1 + k * (size_t)s, s) : (l ? (m + get_field(in + 1 + 2 * s, (uint64_t)k * l, l)) & mask : m);
+    uint64_t r = v % b;
+    if (r > filter1 && r < filter2) out[c++] = block_start + (uint32_t)k;
+  }
+  return c;
+}
+
+/* Per-block minimum and maximum of a column's decoded values (the filter
+ * experiments' zone map, experiments/leco_int_fix_template.cpp:219-239). */
+void oracle_column_zonemap(int codec, const uint8_t *payload, const uint64_t *offsets, int s, size_t n, uint32_t bs,
+                           void *scratch, uint64_t *zmin, uint64_t *zmax) {
+  oracle_column_decode(codec, payload, offsets, s, n, bs, scratch);
+  size_t nb = (n + bs - 1) / bs;
+  for (size_t b = 0; b < nb; b++) {
+    size_t len = n - b * bs < bs ? n - b * bs : bs;
+    uint64_t lo = ~0ull, hi = 0;
+    for (size_t k = 0; k < len; k++) {
+      uint64_t v = ld(scratch, s, b * bs + k);
+      if (v < lo) lo = v;
+      if (v > hi) hi = v;
+    }
+    zmin[b] = lo;
+    zmax[b] = hi;
+  }
+}
+
+/* The filter experiment's loop (experiments/leco_int_fix_template.cpp:244-256,
+ * FOR_int_fix_template.cpp:254-266): blocks in order, results appended; with a
+ * zone map, blocks whose maximum is <= filter are skipped.  Returns the count. */
+size_t oracle_column_filter(int codec, const uint8_t *payload, const uint64_t *offsets, int s, size_t n, uint32_t bs,
+                            uint64_t filter, const uint64_t *zmax, uint32_t *out) {
+  size_t nb = (n + bs - 1) / bs, c = 0;
+  for (size_t b = 0; b < nb; b++) {
+    if (zmax && zmax[b] <= filter) continue;
+    size_t len = n - b * bs < bs ? n - b * bs : bs;
+    const uint8_t *in = payload + offsets[b];
+    uint32_t start = (uint32_t)(b * bs);
+    c += codec == 0 ? oracle_leco_filter(in, s, len, filter, start, out + c) : oracle_for_filter(in, s, len, filter, start, out + c);
+  }
+  return c;
+}
+
+/* Window start of one block in the LeCo close-range experiment
+ * (experiments/leco_int_fix_template.cpp:299-304): the first
+ * filter1 + j*base at or above the block minimum, one window earlier when the
+ * minimum itself lies inside a window; all in T and FP64 as written there
+ * (base is the driver's T). */
+void oracle_close_window_start(uint64_t zmin, uint64_t filter1, uint64_t filter2, uint64_t base, int s,
+                               uint64_t *f1_out, uint64_t *f2_out) {
+  const uint64_t mask = tmask(s);
+  double q = __builtin_ceil((double)((zmin - filter1) & mask) / (double)base);
+  uint64_t a = f2T(q * (double)base + (double)filter1, s);
+  uint64_t b = f2T(q * (double)base + (double)filter2, s);
+  uint64_t r = zmin % base;
+  if (r < filter2 && r > filter1) {
+    a = (a - base) & mask;
+    b = (b - base) & mask;
+  }
+  *f1_out = a;
+  *f2_out = b;
+}
+
+/* The close-range experiment's loop (leco_int_fix_template.cpp:290-322 for
+ * LeCo, FOR_int_fix_template.cpp:303-322 for FOR): LeCo blocks get their own
+ * window start from the zone-map minimum (or filter1/filter2 as given when zmin
+ * is NULL); FOR blocks take filter1, filter2, base as given.  base is passed to
+ * the codec as int (:310).  overwrite as in oracle_leco_filter_close.  Returns
+ * the count, or SIZE_MAX when a block reached max_periods windows. */
+size_t oracle_column_filter_close(int codec, const uint8_t *payload, const uint64_t *offsets, int s, size_t n, uint32_t bs,
+                                  uint64_t filter1, uint64_t filter2, uint64_t base, const uint64_t *zmin, uint32_t *out,
+                                  int overwrite, uint64_t max_periods) {
+  size_t nb = (n + bs - 1) / bs, c = 0;
+  for (size_t b = 0; b < nb; b++) {
+    size_t len = n - b * bs < bs ? n - b * bs : bs;
+    const uint8_t *in = payload + offsets[b];
+    uint32_t start = (uint32_t)(b * bs);
+    if (codec == 0) {
+      uint64_t f1 = filter1, f2 = filter2;
+      if (zmin) oracle_close_window_start(zmin[b], filter1, filter2, base, s, &f1, &f2);
+      size_t k = oracle_leco_filter_close(in, s, len, f1, f2, (int32_t)base, start, out + c, overwrite, max_periods);
+      if (k == (size_t)-1) return k;
+      c += k;
+    } else {
+      c += oracle_for_filter_close(in, s, len, filter1, filter2, (int32_t)base, start, out + c);
+    }
+  }
+  return c;
+}

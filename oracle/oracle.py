@@ -86,6 +86,26 @@ class Oracle:
         L.oracle_lr_fit.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, _P]
         L.oracle_poly2_fit.restype = None
         L.oracle_poly2_fit.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
+        L.oracle_leco_filter.restype = _SZ
+        L.oracle_leco_filter.argtypes = [_P, ctypes.c_int, _SZ, ctypes.c_uint64, ctypes.c_uint32, _P]
+        L.oracle_for_filter.restype = _SZ
+        L.oracle_for_filter.argtypes = [_P, ctypes.c_int, _SZ, ctypes.c_uint64, ctypes.c_uint32, _P]
+        L.oracle_leco_filter_close.restype = _SZ
+        L.oracle_leco_filter_close.argtypes = [_P, ctypes.c_int, _SZ, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32,
+                                               ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_uint64]
+        L.oracle_for_filter_close.restype = _SZ
+        L.oracle_for_filter_close.argtypes = [_P, ctypes.c_int, _SZ, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32,
+                                              ctypes.c_uint32, _P]
+        L.oracle_close_window_start.restype = None
+        L.oracle_close_window_start.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                                ctypes.c_int, _P, _P]
+        L.oracle_column_zonemap.restype = None
+        L.oracle_column_zonemap.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, _P, _P, _P]
+        L.oracle_column_filter.restype = _SZ
+        L.oracle_column_filter.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, ctypes.c_uint64, _P, _P]
+        L.oracle_column_filter_close.restype = _SZ
+        L.oracle_column_filter_close.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, ctypes.c_uint64,
+                                                 ctypes.c_uint64, ctypes.c_uint64, _P, _P, ctypes.c_int, ctypes.c_uint64]
 
     _ENC = ("oracle_leco_encode", "oracle_for_encode", "oracle_delta_encode", "oracle_poly2_encode")
     _DEC = ("oracle_leco_decode", "oracle_for_decode", "oracle_delta_decode", "oracle_poly2_decode")
@@ -142,6 +162,62 @@ class Oracle:
         self.L.oracle_column_random(codec, _ptr(pay), _ptr(offsets), s, bs, _ptr(idx), len(idx), _ptr(out))
         return out
 
+    # -- predicate pushdown ------------------------------------------------
+    def zonemap(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int):
+        """Per-block (min, max) of the decoded values, as uint64 arrays."""
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        nb = (n + bs - 1) // bs
+        scratch = np.zeros(max(n, 1), _dtype(s))
+        zmin, zmax = np.zeros(nb, np.uint64), np.zeros(nb, np.uint64)
+        self.L.oracle_column_zonemap(codec, _ptr(pay), _ptr(offsets), s, n, bs, _ptr(scratch), _ptr(zmin), _ptr(zmax))
+        return zmin, zmax
+
+    def block_filter(self, codec: int, block: bytes, n: int, s: int, filt: int, block_start: int = 0) -> np.ndarray:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(n + 1, np.uint32)
+        fn = self.L.oracle_leco_filter if codec == LECO else self.L.oracle_for_filter
+        c = fn(_ptr(buf), s, n, filt, block_start, _ptr(out))
+        return out[:c].copy()
+
+    def block_filter_close(self, codec: int, block: bytes, n: int, s: int, f1: int, f2: int, base: int,
+                           block_start: int = 0, overwrite: bool = False, max_periods: int = 0, out_len: int | None = None):
+        """(count, out buffer); count -1 when max_periods windows were reached."""
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(out_len if out_len is not None else 4 * n + 2, np.uint32)
+        if codec == LECO:
+            c = self.L.oracle_leco_filter_close(_ptr(buf), s, n, f1, f2, base, block_start, _ptr(out), int(overwrite), max_periods)
+        else:
+            c = self.L.oracle_for_filter_close(_ptr(buf), s, n, f1, f2, base, block_start, _ptr(out))
+        return (-1 if c == 2**64 - 1 else c), out
+
+    def close_window_start(self, zmin: int, f1: int, f2: int, base: int, s: int):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self.L.oracle_close_window_start(zmin, f1, f2, base, s, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def filter_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int,
+                      filt: int, zmax: np.ndarray | None = None) -> np.ndarray:
+        """Indices (uint32) of the values above `filt`, blocks in order."""
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        out = np.zeros(n + 1, np.uint32)
+        zp = _ptr(np.ascontiguousarray(zmax, np.uint64)) if zmax is not None else None
+        c = self.L.oracle_column_filter(codec, _ptr(pay), _ptr(offsets), s, n, bs, filt, zp, _ptr(out))
+        return out[:c].copy()
+
+    def filter_close_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int,
+                            f1: int, f2: int, base: int, zmin: np.ndarray | None = None, overwrite: bool = False,
+                            max_periods: int = 0, out_len: int | None = None):
+        """(count, out buffer) of the close-range filter; out_len sizes the
+        buffer (default 4n + nblocks + 1).  count is -1 when a block reached
+        max_periods windows."""
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        nb = (n + bs - 1) // bs
+        out = np.zeros(out_len if out_len is not None else 4 * n + nb + 1, np.uint32)
+        zm = np.ascontiguousarray(zmin, np.uint64) if zmin is not None else None
+        c = self.L.oracle_column_filter_close(codec, _ptr(pay), _ptr(offsets), s, n, bs, f1, f2, base,
+                                              _ptr(zm) if zm is not None else None, _ptr(out), int(overwrite), max_periods)
+        return (-1 if c == 2**64 - 1 else c), out
+
     # -- variable-length segments ----------------------------------------
     def varseg_encode(self, array: np.ndarray, start: int, end: int) -> bytes:
         out = np.zeros((end - start + 1) * 8 + 64, np.uint8)
@@ -186,6 +262,17 @@ class Reference:
         L.ref_varlen_random.argtypes = [_P, _P, _SZ, _P]
         L.ref_varlen_free.restype = None
         L.ref_varlen_free.argtypes = [_P]
+        for t, ct in (("u32", ctypes.c_uint32), ("u64", ctypes.c_uint64)):
+            f = getattr(L, f"ref_column_filter_{t}"); f.restype = _SZ
+            f.argtypes = [ctypes.c_int, _P, _P, _SZ, ctypes.c_uint32, ct, _P, _P]
+            f = getattr(L, f"ref_column_filter_close_{t}"); f.restype = _SZ
+            f.argtypes = [ctypes.c_int, _P, _P, _SZ, ctypes.c_uint32, ct, ct, ct, _P, _P]
+            f = getattr(L, f"ref_block_filter_{t}"); f.restype = _SZ
+            f.argtypes = [ctypes.c_int, _P, _SZ, ctypes.c_uint32, ctypes.c_int, ct, _P]
+            f = getattr(L, f"ref_block_filter_close_{t}"); f.restype = _SZ
+            f.argtypes = [ctypes.c_int, _P, _SZ, ctypes.c_uint32, ctypes.c_int, ct, ct, ctypes.c_int, _P]
+            f = getattr(L, f"ref_close_window_start_{t}"); f.restype = None
+            f.argtypes = [ct, ct, ct, ct, _P, _P]
 
     @staticmethod
     def _t(s):
@@ -229,6 +316,47 @@ class Reference:
         out = np.zeros(len(idx), _dtype(s))
         getattr(self.L, f"ref_column_random_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), bs, _ptr(idx), len(idx), _ptr(out), threads)
         return out
+
+    # -- predicate pushdown (the filter experiments' loops) -----------------
+    def filter_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int,
+                      filt: int, zmax: np.ndarray | None = None) -> np.ndarray:
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        out = np.zeros(n + 64, np.uint32)
+        zp = _ptr(np.ascontiguousarray(zmax, np.uint64)) if zmax is not None else None
+        c = getattr(self.L, f"ref_column_filter_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), n, bs, filt, zp, _ptr(out))
+        return out[:c].copy()
+
+    def block_filter(self, codec: int, block: bytes, n: int, s: int, filt: int, bs: int, block_id: int):
+        """(count, out buffer) of one block's filter_range."""
+        buf = np.frombuffer(block + b"\0" * 64, np.uint8).copy()
+        out = np.zeros(n + 64, np.uint32)
+        c = getattr(self.L, f"ref_block_filter_{self._t(s)}")(codec, _ptr(buf), n, bs, block_id, filt, _ptr(out))
+        return c, out
+
+    def block_filter_close(self, codec: int, block: bytes, n: int, s: int, f1: int, f2: int, base: int, bs: int,
+                           block_id: int):
+        """(count, out buffer) of one block's filter_range_close."""
+        buf = np.frombuffer(block + b"\0" * 64, np.uint8).copy()
+        out = np.zeros(4 * n + 64, np.uint32)
+        c = getattr(self.L, f"ref_block_filter_close_{self._t(s)}")(codec, _ptr(buf), n, bs, block_id, f1, f2, base, _ptr(out))
+        return c, out
+
+    def close_window_start(self, zmin: int, f1: int, f2: int, base: int, s: int):
+        ct = ctypes.c_uint64 if s == 8 else ctypes.c_uint32
+        a, b = ct(), ct()
+        getattr(self.L, f"ref_close_window_start_{self._t(s)}")(zmin, f1, f2, base, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def filter_close_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int,
+                            f1: int, f2: int, base: int, zmin: np.ndarray | None = None, out_len: int | None = None):
+        """(count, out buffer) exactly as the reference leaves them."""
+        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+        nb = (n + bs - 1) // bs
+        out = np.zeros(out_len if out_len is not None else 4 * n + nb + 1, np.uint32)
+        zm = np.ascontiguousarray(zmin, np.uint64) if zmin is not None else None
+        c = getattr(self.L, f"ref_column_filter_close_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), n, bs, f1, f2, base,
+                                                                      _ptr(zm) if zm is not None else None, _ptr(out))
+        return c, out
 
     # -- variable-length (u64) ---------------------------------------------
     def varlen_encode(self, data: np.ndarray, blocks: int, delta: int):

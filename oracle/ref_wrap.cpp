@@ -181,3 +181,104 @@ void ref_varlen_free(void *h) {
 }
 
 }  // extern "C"
+
+// ---- predicate pushdown ----------------------------------------------------
+// The filter experiments' loops (experiments/leco_int_fix_template.cpp:244-256 and
+// :290-322, FOR_int_fix_template.cpp:254-266 and :303-322) around the codecs'
+// filter_range / filter_range_close.  zmax / zmin: the zone map (per-block maximum
+// / minimum); zmax may be null (no skipping).  For LeCo close-range, zmin null
+// passes filter1/filter2 to every block unchanged.  Returns the count; `out`
+// is what the codec methods left there.
+namespace {
+template <typename T>
+size_t col_filter(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, T filter, const uint64_t *zmax,
+                  uint32_t *out) {
+  size_t nb = (n + bs - 1) / bs;
+  Leco_int<T> lc;
+  FOR_int<T> fc;
+  lc.init((int)nb, (int)bs);
+  fc.init((int)nb, (int)bs);
+  size_t total = 0;
+  for (size_t i = 0; i < nb; ++i) {
+    if (zmax && (T)zmax[i] <= filter) continue;
+    size_t len = std::min<size_t>(bs, n - i * bs);
+    uint8_t *in = const_cast<uint8_t *>(p + off[i]);
+    total += codec == C_LECO ? lc.filter_range(in, len, filter, out + total, (int)i)
+                             : fc.filter_range(in, len, filter, out + total, i);
+  }
+  return total;
+}
+
+template <typename T>
+void window_start(T lo, T filter1, T filter2, T base, T *a, T *b) {
+  T f1 = ceil((double)(T)(lo - filter1) / (double)base) * base + filter1;
+  T f2 = ceil((double)(T)(lo - filter1) / (double)base) * base + filter2;
+  if (lo % base < filter2 && lo % base > filter1) {
+    f1 -= base;
+    f2 -= base;
+  }
+  *a = f1;
+  *b = f2;
+}
+template <typename T>
+size_t col_filter_close(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, T filter1, T filter2,
+                        T base, const uint64_t *zmin, uint32_t *out) {
+  size_t nb = (n + bs - 1) / bs;
+  Leco_int<T> lc;
+  FOR_int<T> fc;
+  lc.init((int)nb, (int)bs);
+  fc.init((int)nb, (int)bs);
+  size_t total = 0;
+  for (size_t i = 0; i < nb; ++i) {
+    size_t len = std::min<size_t>(bs, n - i * bs);
+    uint8_t *in = const_cast<uint8_t *>(p + off[i]);
+    if (codec == C_LECO) {
+      T f1 = filter1, f2 = filter2;
+      if (zmin) window_start<T>((T)zmin[i], filter1, filter2, base, &f1, &f2);
+      total += lc.filter_range_close(in, len, out + total, (int)i, f1, f2, (int)base);
+    } else {
+      total += fc.filter_range_close(in, len, out + total, i, filter1, filter2, (int)base);
+    }
+  }
+  return total;
+}
+}  // namespace
+
+extern "C" {
+size_t ref_column_filter_u32(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint32_t f, const uint64_t *zmax, uint32_t *out) { return col_filter<uint32_t>(codec, p, off, n, bs, f, zmax, out); }
+size_t ref_column_filter_u64(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint64_t f, const uint64_t *zmax, uint32_t *out) { return col_filter<uint64_t>(codec, p, off, n, bs, f, zmax, out); }
+size_t ref_column_filter_close_u32(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint32_t f1, uint32_t f2, uint32_t base, const uint64_t *zmin, uint32_t *out) { return col_filter_close<uint32_t>(codec, p, off, n, bs, f1, f2, base, zmin, out); }
+size_t ref_column_filter_close_u64(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint64_t f1, uint64_t f2, uint64_t base, const uint64_t *zmin, uint32_t *out) { return col_filter_close<uint64_t>(codec, p, off, n, bs, f1, f2, base, zmin, out); }
+}  // extern "C"
+
+// One block through <Codec>::filter_range / filter_range_close with the codec's
+// block_size = bs and the given block_id (the index base is block_id*bs).
+// ref_close_window_start_*: the LeCo close-range experiment's per-block window
+// start from the block minimum (experiments/leco_int_fix_template.cpp:299-304).
+namespace {
+template <typename T>
+size_t blk_filter(int codec, const uint8_t *in, size_t len, uint32_t bs, int block_id, T f, uint32_t *out) {
+  uint8_t *p = const_cast<uint8_t *>(in);
+  if (codec == C_LECO) { Leco_int<T> c; c.init(block_id + 1, (int)bs); return c.filter_range(p, len, f, out, block_id); }
+  FOR_int<T> c;
+  c.init(block_id + 1, (int)bs);
+  return c.filter_range(p, len, f, out, (size_t)block_id);
+}
+template <typename T>
+size_t blk_filter_close(int codec, const uint8_t *in, size_t len, uint32_t bs, int block_id, T f1, T f2, int base, uint32_t *out) {
+  uint8_t *p = const_cast<uint8_t *>(in);
+  if (codec == C_LECO) { Leco_int<T> c; c.init(block_id + 1, (int)bs); return c.filter_range_close(p, len, out, block_id, f1, f2, base); }
+  FOR_int<T> c;
+  c.init(block_id + 1, (int)bs);
+  return c.filter_range_close(p, len, out, (size_t)block_id, f1, f2, base);
+}
+}  // namespace
+
+extern "C" {
+size_t ref_block_filter_u32(int codec, const uint8_t *in, size_t len, uint32_t bs, int bid, uint32_t f, uint32_t *out) { return blk_filter<uint32_t>(codec, in, len, bs, bid, f, out); }
+size_t ref_block_filter_u64(int codec, const uint8_t *in, size_t len, uint32_t bs, int bid, uint64_t f, uint32_t *out) { return blk_filter<uint64_t>(codec, in, len, bs, bid, f, out); }
+size_t ref_block_filter_close_u32(int codec, const uint8_t *in, size_t len, uint32_t bs, int bid, uint32_t f1, uint32_t f2, int base, uint32_t *out) { return blk_filter_close<uint32_t>(codec, in, len, bs, bid, f1, f2, base, out); }
+size_t ref_block_filter_close_u64(int codec, const uint8_t *in, size_t len, uint32_t bs, int bid, uint64_t f1, uint64_t f2, int base, uint32_t *out) { return blk_filter_close<uint64_t>(codec, in, len, bs, bid, f1, f2, base, out); }
+void ref_close_window_start_u32(uint32_t lo, uint32_t f1, uint32_t f2, uint32_t base, uint32_t *a, uint32_t *b) { window_start<uint32_t>(lo, f1, f2, base, a, b); }
+void ref_close_window_start_u64(uint64_t lo, uint64_t f1, uint64_t f2, uint64_t base, uint64_t *a, uint64_t *b) { window_start<uint64_t>(lo, f1, f2, base, a, b); }
+}  // extern "C"
