@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen"],
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
@@ -467,6 +467,105 @@ def run_varlen(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_filter(args, world, rank, local):
+    """Predicate pushdown on the decode workload's column (200M sorted u64
+    keys, LeCo-fix, 4096-value blocks): filter_range at 50% and 1%
+    selectivity with the zone map, and a close-range filter, each timed on the
+    device; the reference's own filter loop (compiled headers) is timed on the
+    host cores over the first blocks, and the GPU's indices there are checked
+    against it."""
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    x = workloads.piecewise_linear_u64(n, seed=2 + rank, device=dev)
+    col = lc.encode(x, lc.LINEAR, BS, lc.FIT_REFERENCE)
+    zmin, zmax = col.zonemap()
+    xh = x.cpu().numpy().view(np.uint64)
+    pay, off = col.to_host()
+    stream = torch.cuda.current_stream()
+    out = torch.empty(n + col.nblocks, dtype=torch.int32, device=dev)
+    ws = torch.empty(int(lc.lib().leco_filter_workspace_bytes(n, BS)), dtype=torch.uint8, device=dev)
+    reps = max(3, args.steps // 4)
+
+    def ev_time(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    zmax_h = to_np_u64(zmax)
+    res = {}
+    with ClockSampler(local) as clk:
+        for q in (0.5, 0.99):
+            f = int(np.quantile(xh[:: max(1, n // 1_000_000)], q))
+            ms = ev_time(lambda: col.filter_range(f, zone_max=zmax, zone_min=zmin, out=out, ws=ws, sync=False))
+            _, c = col.filter_range(f, zone_max=zmax, zone_min=zmin, out=out, ws=ws)
+            live = zmax_h > np.uint64(f)  # blocks the zone map lets through: their images are read
+            read = int(np.sum((off[1:] - off[:-1])[live])) + 8 * col.nblocks
+            res[f"range_q{q}"] = {"filter": f, "matches": c, "ms": round(ms, 4),
+                                  "gvalues_s": round(n / ms / 1e6, 2),
+                                  "alg_gbs": round((read + 4 * c) / ms / 1e6, 1)}
+        f = res["range_q0.5"]["filter"]
+        ms = ev_time(lambda: col.filter_range(f, out=out, ws=ws, sync=False))
+        _, c = col.filter_range(f, out=out, ws=ws)
+        res["range_q0.5_no_zone_map"] = {"filter": f, "matches": c, "ms": round(ms, 4),
+                                         "gvalues_s": round(n / ms / 1e6, 2)}
+        base, f1, f2 = (1 << 31) - 1, 1 << 29, 1 << 30
+        ms = ev_time(lambda: col.filter_range_close(f1, f2, base, zone_min=zmin, out=out, ws=ws, sync=False))
+        _, c = col.filter_range_close(f1, f2, base, zone_min=zmin, out=out, ws=ws)
+        read = int(off[-1]) + 8 * col.nblocks
+        res["close"] = {"base": base, "f1": f1, "f2": f2, "matches": c, "ms": round(ms, 4),
+                        "gvalues_s": round(n / ms / 1e6, 2), "alg_gbs": round((read + 4 * c) / ms / 1e6, 1)}
+    lc.check()
+    # the reference's filter loop on the host, over the first blocks (bounded sample)
+    cpu = {}
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Reference
+
+        R = Reference()
+        nbs = min(col.nblocks, 4096)
+        ns = min(n, nbs * BS)
+        spay, soff = pay[: int(off[nbs])], off[: nbs + 1]
+        f = res["range_q0.5"]["filter"]
+        t0 = time.perf_counter()
+        want = R.filter_column(0, spay, soff, ns, 8, BS, f, zmax_h[:nbs])
+        t_cpu = time.perf_counter() - t0
+        got, c = col.filter_range(f, zone_max=zmax, zone_min=zmin, out=out, ws=ws)
+        g = got.cpu().numpy().view(np.uint32)
+        assert np.array_equal(g[: len(want)], want), "filter_range differs from the reference on the sample"
+        cpu = {"value": round(ns / t_cpu / 1e9, 4), "unit": "Gvalues/s", "cores": 1, "kind": "reference",
+               "sample": f"first {nbs} blocks ({ns} keys), filter_range at the median, zone map, 1 thread "
+                         "(the reference's loop is single-threaded)"}
+    except (FileNotFoundError, OSError) as e:
+        cpu = {"unavailable": str(e)}
+    if rank == 0:
+        head = res["range_q0.5"]
+        line = {"metric": "LeCo-fix predicate pushdown on 200M sorted u64 keys: filter_range Gvalues/s",
+                "value": head["gvalues_s"], "unit": "Gvalues/s", "n_gpus": world, "steps": reps,
+                "warmup": max(3, args.warmup), "ms_per_step": head["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"{n} u64 piecewise-linear keys, LeCo-fix blocks of {BS}, zone map",
+                           "keys": n, "compressed_bytes": int(off[-1])},
+                "clocks": clk.summary(), "cpu_baseline": cpu, **res}
+        print(json.dumps(line), flush=True)
+
+
+def to_np_u64(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -481,6 +580,9 @@ def main():
         return
     if args.workload == "varlen":
         run_varlen(args, world, rank, local)
+        return
+    if args.workload == "filter":
+        run_filter(args, world, rank, local)
         return
 
     import torch

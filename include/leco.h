@@ -160,6 +160,55 @@ uint64_t leco_sum_workspace_bytes(uint64_t n, uint32_t block_size);
 int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
              uint32_t block_size, uint64_t *d_sum, void *d_partials, leco_stream_t stream);
 
+/* ---- predicate pushdown ------------------------------------------------------
+ * Indices of the values that pass a filter, found without decoding the column to
+ * memory.  Output: uint32 global value indices b*block_size + k (the reference's
+ * uint32_t out), blocks in order, within a block in the order the reference's
+ * method emits them; at most out_cap are written and *d_count receives the full
+ * count.  Columns of LINEAR (Leco_int<T>) or FOR (FOR_int<T>) blocks, n < 2^32.
+ * d_ws: leco_filter_workspace_bytes() bytes of 8-byte aligned device scratch.
+ * A raw LINEAR block (l == 8*sizeof(T)), which the reference's filters read as a
+ * model, is filtered on its stored values here. */
+uint64_t leco_filter_workspace_bytes(uint64_t n, uint32_t block_size);
+
+/* Values above `filter`: Leco_int<T>::filter_range
+ * (piecewise_fix_integer_template.h:206-252: scan from the model's threshold index)
+ * or FOR_int<T>::filter_range (FOR_integer_template.h:115-160) on every block, as the
+ * filter experiment calls them (experiments/leco_int_fix_template.cpp:244-256).
+ * d_zone_min / d_zone_max (each nullable): per-block minima / maxima (leco_zonemap).
+ * Blocks whose maximum is <= filter are skipped unread, as the experiment's zone map
+ * does (:247-249); blocks whose minimum is above it match from the threshold index on
+ * without their fields being read (the same indices the reference emits). */
+int leco_filter_range(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                      uint32_t block_size, uint64_t filter, const uint64_t *d_zone_min, const uint64_t *d_zone_max,
+                      uint32_t *d_out, uint64_t out_cap, uint64_t *d_count, void *d_ws, uint64_t ws_bytes,
+                      leco_stream_t stream);
+
+/* Close-range filter: filter_range_close (piecewise_fix_integer_template.h:254-303,
+ * FOR_integer_template.h:166-215) on every block, as the close-range experiments call
+ * it (leco_int_fix_template.cpp:290-322, FOR_int_fix_template.cpp:303-322).
+ * FOR: values v with filter1 < v % base < filter2.  LINEAR: for the windows
+ * (filter1 + p*base, filter2 + p*base), p = 0, 1, ..., the values inside each window
+ * among the indices the block's model allows, windows in order; with d_zone_min
+ * (per-block minima) each block's first window is derived from its minimum as the
+ * experiment does (:299-304), without it every block starts at (filter1, filter2).
+ * 1 <= base <= INT32_MAX (the codecs take it as int).  The reference appends each
+ * window's indices after the previous ones only for l == 0 blocks (for l > 0 it
+ * writes every window from the block's first output slot again, :280); here they
+ * are always appended, and the count is the reference's.  A LINEAR block that
+ * needs more than 65536 windows sets the error word (leco_check returns
+ * LECO_ERR_UNSUPPORTED); the reference's loop costs windows x block length there. */
+int leco_filter_range_close(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                            uint32_t block_size, uint64_t filter1, uint64_t filter2, uint64_t base,
+                            const uint64_t *d_zone_min, uint32_t *d_out, uint64_t out_cap, uint64_t *d_count,
+                            void *d_ws, uint64_t ws_bytes, leco_stream_t stream);
+
+/* Per-block minimum and maximum of the decoded values, as uint64 (the filter
+ * experiments' zone map, experiments/leco_int_fix_template.cpp:219-239, built there
+ * from the raw column; here from the compressed one).  Any fixed-block codec. */
+int leco_zonemap(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                 uint32_t block_size, uint64_t *d_min, uint64_t *d_max, leco_stream_t stream);
+
 /* ---- variable-length segments (Leco_cost_merge_double_wo_round<uint64_t>) ----
  * headers/piecewise_cost_merge_integer_template_double_wo_round.h:18-700.  A column is
  * payload (segment images back to back), offsets[nseg + 1] and starts[nseg] (value

@@ -68,6 +68,10 @@ SIGNATURES = [
     ("leco_gather", _I, [_I, _I, _P, _P, _P, _U64, _U32, _P, _U64, _P, _P]),
     ("leco_sum_workspace_bytes", _U64, [_U64, _U32]),
     ("leco_sum", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P, _P]),
+    ("leco_filter_workspace_bytes", _U64, [_U64, _U32]),
+    ("leco_filter_range", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _P, _P, _P, _U64, _P, _P, _U64, _P]),
+    ("leco_filter_range_close", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _U64, _U64, _P, _P, _U64, _P, _P, _U64, _P]),
+    ("leco_zonemap", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P, _P]),
     ("leco_encode_host", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P]),
     ("leco_decode_host", _I, [_I, _I, _P, _P, _U64, _U32, _P]),
     ("leco_gather_host", _I, [_I, _I, _P, _P, _U64, _U32, _P, _U64, _P]),
@@ -314,6 +318,62 @@ class Column:
         _check(lib().leco_sum(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n, self.block_size,
                               _tptr(out), None, _stream_ptr(stream)), "leco_sum")
         return int(out.item()) & 0xFFFFFFFFFFFFFFFF
+
+    # -- predicate pushdown (Leco_int / FOR_int filter_range, filter_range_close) --
+    def zonemap(self, stream=None):
+        """(min, max) of every block's decoded values, as int64 tensors holding
+        the uint64 bit patterns."""
+        torch = _torch()
+        zmin = torch.empty(self.nblocks, dtype=torch.int64, device=self.payload.device)
+        zmax = torch.empty_like(zmin)
+        _check(lib().leco_zonemap(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n,
+                                  self.block_size, _tptr(zmin), _tptr(zmax), _stream_ptr(stream)), "leco_zonemap")
+        return zmin, zmax
+
+    def _filter_buffers(self, out, out_cap, ws):
+        torch = _torch()
+        dev = self.payload.device
+        if out is None:
+            out_cap = self.n + self.nblocks if out_cap is None else out_cap
+            out = torch.empty(max(out_cap, 1), dtype=torch.int32, device=dev)
+        elif out_cap is None:
+            out_cap = out.numel()
+        need = int(lib().leco_filter_workspace_bytes(self.n, self.block_size))
+        if ws is None or ws.numel() < need:
+            ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        count = torch.empty(1, dtype=torch.int64, device=dev)
+        return out, out_cap, ws, count
+
+    def filter_range(self, filt: int, zone_max=None, zone_min=None, out=None, out_cap=None, ws=None, stream=None,
+                     sync: bool = True):
+        """Indices (int32 tensor holding uint32) of the values above `filt`;
+        returns (indices, count).  sync=False returns the device count tensor
+        and the full output buffer without waiting."""
+        out, out_cap, ws, count = self._filter_buffers(out, out_cap, ws)
+        _check(lib().leco_filter_range(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n,
+                                       self.block_size, int(filt) & 0xFFFFFFFFFFFFFFFF, _tptr(zone_min),
+                                       _tptr(zone_max), _tptr(out),
+                                       out_cap, _tptr(count), _tptr(ws), ws.numel(), _stream_ptr(stream)),
+               "leco_filter_range")
+        if not sync:
+            return out, count
+        c = int(count.item())
+        return out[:min(c, out_cap)], c
+
+    def filter_range_close(self, f1: int, f2: int, base: int, zone_min=None, out=None, out_cap=None, ws=None,
+                           stream=None, sync: bool = True):
+        """Close-range filter (windows (f1 + p*base, f2 + p*base) for LeCo,
+        residues f1 < v % base < f2 for FOR); returns (indices, count)."""
+        out, out_cap, ws, count = self._filter_buffers(out, out_cap, ws)
+        _check(lib().leco_filter_range_close(self.codec, self.dtype, _tptr(self.payload), _tptr(self.offsets), self.n,
+                                             self.block_size, int(f1) & 0xFFFFFFFFFFFFFFFF, int(f2) & 0xFFFFFFFFFFFFFFFF,
+                                             base, _tptr(zone_min), _tptr(out), out_cap, _tptr(count), _tptr(ws),
+                                             ws.numel(), _stream_ptr(stream)), "leco_filter_range_close")
+        if not sync:
+            return out, count
+        c = int(count.item())
+        _check(lib().leco_check(_stream_ptr(stream)), "leco_filter_range_close")
+        return out[:min(c, out_cap)], c
 
     def build_directory(self, stream=None):
         torch = _torch()

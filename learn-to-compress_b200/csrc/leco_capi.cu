@@ -245,6 +245,95 @@ int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_o
   return LECO_OK;
 }
 
+// ---- predicate pushdown -------------------------------------------------------------
+
+uint64_t leco_filter_workspace_bytes(uint64_t n, uint32_t block_size) {
+  return leco_num_blocks(n, block_size) * 8 + 64;
+}
+
+static int filter_setup(const char *fn, int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets,
+                        uint64_t n, uint32_t block_size, uint32_t *d_out, uint64_t out_cap, uint64_t *d_count,
+                        void *d_ws, uint64_t ws_bytes, cudaStream_t st, FilterLaunch &L) {
+  int rc = check_column(fn, codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (codec != kLinear && codec != kFor)
+    return fail(LECO_ERR_UNSUPPORTED, std::string(fn) + ": the reference filters LINEAR and FOR columns only");
+  if (n >= (1ull << 32)) return fail(LECO_ERR_ARG, std::string(fn) + ": output indices are uint32 (n < 2^32)");
+  if (!d_count || (out_cap && !d_out)) return fail(LECO_ERR_ARG, std::string(fn) + ": null output");
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  if (!d_ws || ws_bytes < leco_filter_workspace_bytes(n, block_size) || (reinterpret_cast<uintptr_t>(d_ws) & 7))
+    return fail(LECO_ERR_ARG, std::string(fn) + ": workspace must be leco_filter_workspace_bytes() bytes, 8-byte aligned");
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  L = FilterLaunch{};
+  L.payload = d_payload;
+  L.offsets = d_offsets;
+  L.n = n;
+  L.bs = block_size;
+  L.nb = nb;
+  L.out = d_out;
+  L.cap = d_out ? out_cap : 0;
+  L.count = d_count;
+  L.status = reinterpret_cast<uint64_t *>(d_ws);
+  L.ticket = reinterpret_cast<uint32_t *>(L.status + nb);
+  L.error = err;
+  L.max_windows = 65536;
+  L.stage = (reinterpret_cast<uintptr_t>(d_payload) & 15) == 0;
+  LECO_CUDA(cudaMemsetAsync(d_ws, 0, nb * 8 + 8, st));
+  if (!nb) LECO_CUDA(cudaMemsetAsync(d_count, 0, 8, st));
+  return LECO_OK;
+}
+
+int leco_filter_range(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                      uint32_t block_size, uint64_t filter, const uint64_t *d_zone_min, const uint64_t *d_zone_max,
+                      uint32_t *d_out, uint64_t out_cap, uint64_t *d_count, void *d_ws, uint64_t ws_bytes,
+                      leco_stream_t stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  FilterLaunch L;
+  int rc = filter_setup("leco_filter_range", codec, dtype, d_payload, d_offsets, n, block_size, d_out, out_cap, d_count,
+                        d_ws, ws_bytes, st, L);
+  if (rc) return rc;
+  L.f1 = filter;
+  L.zone = d_zone_max;
+  L.zone_lo = d_zone_min;
+  if (launch_filter(codec, dtype, L, 0, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range: no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+int leco_filter_range_close(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                            uint32_t block_size, uint64_t filter1, uint64_t filter2, uint64_t base,
+                            const uint64_t *d_zone_min, uint32_t *d_out, uint64_t out_cap, uint64_t *d_count,
+                            void *d_ws, uint64_t ws_bytes, leco_stream_t stream) {
+  if (base < 1 || base > 0x7fffffffull) return fail(LECO_ERR_ARG, "leco_filter_range_close: base must be in 1..INT32_MAX");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  FilterLaunch L;
+  int rc = filter_setup("leco_filter_range_close", codec, dtype, d_payload, d_offsets, n, block_size, d_out, out_cap,
+                        d_count, d_ws, ws_bytes, st, L);
+  if (rc) return rc;
+  L.f1 = filter1;
+  L.f2 = filter2;
+  L.base = base;
+  L.zone = codec == kLinear ? d_zone_min : nullptr;
+  if (launch_filter(codec, dtype, L, 1, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range_close: no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
+int leco_zonemap(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets, uint64_t n,
+                 uint32_t block_size, uint64_t *d_min, uint64_t *d_max, leco_stream_t stream) {
+  int rc = check_column("leco_zonemap", codec, dtype, d_payload, d_offsets, block_size);
+  if (rc) return rc;
+  if (!d_min || !d_max) return fail(LECO_ERR_ARG, "leco_zonemap: null output");
+  uint32_t *err = nullptr;
+  if ((rc = error_ptr(&err))) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  DecodeLaunch L{d_payload, d_offsets, n, block_size, 0, n, nullptr, err};
+  if (launch_zonemap(codec, dtype, L, d_min, d_max, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_zonemap: no kernel");
+  LECO_CUDA(cudaGetLastError());
+  return LECO_OK;
+}
+
 int leco_check(leco_stream_t stream) {
   uint32_t *err = nullptr;
   int rc = error_ptr(&err);
@@ -259,6 +348,7 @@ int leco_check(leco_stream_t stream) {
   if (h & kErrCapacity) return fail(LECO_ERR_CAPACITY, "payload buffer smaller than the encoded column");
   if (h & kErrBadHeader) return fail(LECO_ERR_CORRUPT, "invalid block header");
   if (h & kErrBadIndex) return fail(LECO_ERR_CORRUPT, "index outside the column");
+  if (h & kErrLimit) return fail(LECO_ERR_UNSUPPORTED, "close-range filter: a block needs more than 65536 windows");
   return LECO_OK;
 }
 

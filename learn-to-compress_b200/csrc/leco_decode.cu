@@ -14,6 +14,7 @@
 // rule).  The reference's bulk decoders also call l == 8*sizeof(T)-1 raw, which
 // mis-decodes such packed blocks; this decoder reads them correctly.
 #include "leco_decode.cuh"
+#include "leco_stage.cuh"
 
 #include <cstdlib>
 
@@ -33,43 +34,6 @@ __global__ void __launch_bounds__(256) decode_kernel_warp(DecodeLaunch a, uint64
 }
 
 // ---- TMA-staged persistent decode --------------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t tx) {
-  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(tx) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bulk (non-tensor) TMA copy global -> this CTA's shared memory, completion
-// counted on `bar`.  dst/src 16-byte aligned, bytes a multiple of 16.  No
-// multicast: the source is always this GPU's own payload.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-// Bounded wait on a staging barrier (about a second at most).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (uint32_t spins = 0; spins < (1u << 24); ++spins)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
 struct StageMeta {
   uint64_t gbase;   // 16-byte aligned global byte address of the staged copy
   uint32_t hoff;    // block header offset inside the staged copy

@@ -23,7 +23,7 @@ constexpr int kLinear = 0, kFor = 1, kDelta = 2, kPoly2 = 3, kVarlen = 4;
 constexpr uint32_t kWarpBlock = 512;
 
 // Error word bits (device error word, read by leco_check).
-constexpr uint32_t kErrBadIndex = 1u, kErrBadHeader = 2u, kErrTimeout = 4u, kErrCapacity = 8u;
+constexpr uint32_t kErrBadIndex = 1u, kErrBadHeader = 2u, kErrTimeout = 4u, kErrCapacity = 8u, kErrLimit = 16u;
 
 // (int64_t)x as x86-64 CVTTSD2SI computes it: truncation toward zero, and
 // INT64_MIN for NaN or |x| >= 2^63 (reference: e.g. piecewise_fix_integer_template.h:54,

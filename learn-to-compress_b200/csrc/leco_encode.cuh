@@ -13,7 +13,7 @@
 namespace leco {
 
 constexpr uint64_t kFlagAgg = 1ull << 62, kFlagIncl = 2ull << 62, kValMask = (1ull << 62) - 1;
-constexpr uint32_t kSpinLimit = 1u << 22;  // x ~64-512 ns backoff: far above any real wait
+constexpr uint32_t kSpinLimit = 1u << 22;  // x ~32-256 ns backoff: far above any real wait
 
 // Per-block model scratch: the sequential reference fit writes 3 doubles per block.
 struct EncodeArgs {
@@ -57,9 +57,12 @@ __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
   return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + bs * s;
 }
 
-// Decoupled look-back (single-pass prefix sum over block image sizes).  Run by
-// warp 0.  Returns the exclusive prefix; on a wait that exceeds the spin limit
-// sets kErrTimeout and returns ~0.
+// Decoupled look-back (single-pass prefix sum over per-block totals).  Run by
+// one full warp.  Publishes this block's total, then walks back over the
+// predecessors 32 at a time (lane i reads block j - i): it needs every block from
+// the nearest one down to the first with an inclusive prefix, and waits only
+// while one of those has published nothing.  Returns the exclusive prefix; on a
+// wait that exceeds the spin limit sets kErrTimeout and returns ~0.
 __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error,
                                                     uint32_t spin_limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
@@ -71,27 +74,26 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
   uint64_t excl = 0;
   int64_t j = (int64_t)b - 1;
   for (;;) {
-    int64_t idx = j - lane;
+    const int64_t idx = j - lane;
     uint64_t v = kFlagIncl;  // lanes before block 0 read as "inclusive 0"
-    uint32_t spins = 0, ns = 64;
+    uint32_t spins = 0, ns = 32;
+    uint32_t incl;
+    int last;  // the farthest lane this round needs
     for (;;) {
       if (idx >= 0) v = ld_relaxed(&status[idx]);
-      if (__all_sync(0xffffffffu, (v >> 62) != 0)) break;
+      incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+      last = incl ? __ffs(incl) - 1 : 31;
+      const uint32_t need = last == 31 ? 0xffffffffu : ((2u << last) - 1u);
+      if (!(__ballot_sync(0xffffffffu, (v >> 62) == 0) & need)) break;
       if (++spins > spin_limit) {
         if (lane == 0) atomicOr(error, kErrTimeout);
         return ~0ull;
       }
       __nanosleep(ns);
-      if (ns < 512) ns <<= 1;
+      if (ns < 256) ns <<= 1;
     }
-    uint32_t incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
-    if (incl) {
-      int first = __ffs(incl) - 1;  // nearest predecessor with an inclusive prefix
-      uint64_t x = lane <= first ? (v & kValMask) : 0;
-      excl += warp_sum_u64(x);
-      break;
-    }
-    excl += warp_sum_u64(v & kValMask);
+    excl += warp_sum_u64(lane <= last ? (v & kValMask) : 0);
+    if (incl) break;
     j -= 32;
   }
   if (lane == 0) st_relaxed(&status[b], kFlagIncl | (excl + my));

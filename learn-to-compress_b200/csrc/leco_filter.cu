@@ -1,0 +1,468 @@
+// leco_filter.cu -- predicate pushdown on compressed columns: the indices of the
+// values that pass a filter, found without decoding the column to memory.
+//
+// Semantics are those of the reference's per-block filters, called block after
+// block as its filter experiments do:
+//   range (values above f):  Leco_int<T>::filter_range   piecewise_fix_integer_template.h:206-252
+//                            FOR_int<T>::filter_range    FOR_integer_template.h:115-160
+//   close range (windows):   Leco_int<T>::filter_range_close  piecewise_fix_integer_template.h:254-303
+//                            FOR_int<T>::filter_range_close   FOR_integer_template.h:166-215
+//   column loops:            experiments/leco_int_fix_template.cpp:244-256, :290-322
+//                            experiments/FOR_int_fix_template.cpp:254-266, :303-322
+// The output is uint32 global indices b*block_size + k, blocks in order, each
+// block's indices in the order the reference emits them.
+//
+// One warp per block, blocks taken in ticket order; the output offset of a
+// block is the exclusive prefix of the match counts, found by decoupled
+// look-back (the single-pass scan the encoder uses for byte offsets).  Before
+// reading any field, a block (or window) is classified from its model's value
+// bounds, its FOR header or the zone map: all indices match, none do, or the
+// values must be read.  Read blocks are evaluated twice: a counting pass that
+// keeps the match bitmap in shared memory and, once the offset is known, a
+// writing pass (bitmap read back, or the windows evaluated again from
+// L1-resident fields).
+#include "leco_decode.cuh"
+#include "leco_encode.cuh"
+
+namespace leco {
+
+constexpr int kFT = 256;                              // threads per CTA
+constexpr int kFU = 4;                                // 32-item groups per lane per step
+
+// (int)x as x86-64 compiles it (32-bit CVTTSD2SI): NaN and values outside the
+// int range give INT_MIN.  The filters keep their index thresholds in int
+// (piecewise_fix_integer_template.h:226,275-276).
+__device__ __forceinline__ int32_t f2i32_x86(double x) {
+  return (x > -2147483649.0 && x < 2147483648.0) ? __double2int_rz(x) : (int32_t)0x80000000;
+}
+// std::max / std::min as the filters use them: (a < b) ? b : a, (b < a) ? b : a.
+__device__ __forceinline__ double std_max(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double std_min(double a, double b) { return b < a ? b : a; }
+
+// A decoded value against a bound of type T: uint64_t compares unsigned; for
+// uint32_t the bound is promoted to int64_t and the comparison is signed
+// (bit_read.h:421,477).
+template <int S>
+__device__ __forceinline__ bool cmp_gt(uint64_t v, uint64_t f) { return S == 8 ? v > f : (int64_t)v > (int64_t)f; }
+template <int S>
+__device__ __forceinline__ bool cmp_lt(uint64_t v, uint64_t f) { return S == 8 ? v < f : (int64_t)v < (int64_t)f; }
+
+// (double)(f + c) for f of type T and an int64_t offset c: T = uint64_t wraps
+// modulo 2^64 and converts unsigned; T = uint32_t is widened to int64_t first.
+template <int S>
+__device__ __forceinline__ double bound_plus(uint64_t f, int64_t c) {
+  if (S == 8) return __ull2double_rn(f + (uint64_t)c);
+  return __ll2double_rn((int64_t)(uint32_t)f + c);
+}
+
+// Value k of a block as the filter readers compute it: raw values as stored,
+// FOR min + offset, LeCo (long long)(theta0 + k*theta1) -/+ the magnitude in
+// wrapping 64-bit arithmetic (bit_read.h:409-420; l == 0: the prediction).
+template <int S, int CODEC>
+__device__ __forceinline__ uint64_t filter_value(const uint64_t *__restrict__ words, const BlockHdr &h, bool raw, uint32_t k) {
+  constexpr uint32_t TB = 8u * S;
+  if (raw) return load_field(words, h.body_bit + (uint64_t)k * TB, TB);
+  if (CODEC == kFor) {
+    const uint64_t v = h.l ? h.base + load_field(words, h.body_bit + (uint64_t)k * h.l, h.l) : h.base;
+    return S == 8 ? v : (v & 0xffffffffull);
+  }
+  uint64_t v = (uint64_t)f2i_x86(pred_linear(h.a0, h.a1, k));
+  if (h.l) v = apply_signed(v, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+  return v;
+}
+
+// What one block evaluates.
+enum : int {
+  kPredAbove = 0,   // v > f1
+  kPredModulo = 1,  // f1 < v % base < f2 (FOR close range)
+  kPredAnyWin = 2,  // raw LeCo block, close range: v in some window (f1 + p*base, f2 + p*base)
+  kPredWindows = 3  // packed LeCo block, close range: the reference's window loop
+};
+
+template <int S>
+__device__ __forceinline__ bool single_pred(int pred, uint64_t v, uint64_t f1, uint64_t f2, uint64_t base) {
+  if (pred == kPredAbove) return cmp_gt<S>(v, f1);
+  if (pred == kPredModulo) {
+    const uint64_t r = v % base;
+    return r > f1 && r < f2;
+  }
+  // kPredAnyWin: the largest window start below v is v - ((v - f1 - 1) % base) - 1
+  return v > f1 && f2 > f1 && ((v - f1 - 1) % base) + 1 < f2 - f1;
+}
+
+// One warp per block.  A CTA takes kFB consecutive blocks by one ticket; its
+// warps are then independent: each counts its block, finds its output offset by
+// look-back (the CTA's earlier warps and earlier CTAs are all resident or done,
+// so every wait ends) and writes; no CTA barrier after the ticket.
+constexpr int kFB = kFT / 32;            // warps (blocks in flight) per CTA
+constexpr uint32_t kFWin = 32;           // windows per chunk (close range), one per lane
+
+// How a window's values relate to its bounds, decided from the block model
+// (or header / zone map) before any field is read.
+enum : int { kNone = 0, kAll = 1, kEval = 2 };
+
+// Per-warp plan of one block.
+struct BlockPlan {
+  BlockHdr h;
+  uint64_t vbase;
+  uint32_t len, lo, hi;
+  int pred;
+  int mode;       // single window: kNone / kAll / kEval
+  bool raw;
+  bool bounded;   // LeCo: every prediction of the block lies inside (-2^62, 2^62) and l <= 61
+  uint64_t f1, f2;
+};
+
+// Bounds of the values of a packed LeCo block at indices [k0, k1] (k0 <= k1):
+// the predictions are monotone in k when every one lies inside (-2^62, 2^62),
+// and a value differs from its prediction by at most 2^(l-1) - 1.
+__device__ __forceinline__ void leco_value_bounds(const BlockHdr &h, uint32_t k0, uint32_t k1, int64_t &vmin, int64_t &vmax) {
+  const int64_t pa = __double2ll_rz(pred_linear(h.a0, h.a1, k0)), pb = __double2ll_rz(pred_linear(h.a0, h.a1, k1));
+  const int64_t m = h.l ? (((int64_t)1 << (h.l - 1)) - 1) : 0;
+  vmin = (pa < pb ? pa : pb) - m;
+  vmax = (pa < pb ? pb : pa) + m;
+}
+
+// Window classification against (w1, w2) (w2 = none: range filter v > w1) in
+// the comparison domain of T.  For T = uint64_t a negative int64 value wraps
+// to a huge unsigned one, so only blocks whose values are all non-negative are
+// classified.
+template <int S>
+__device__ __forceinline__ int classify(int64_t vmin, int64_t vmax, uint64_t w1, uint64_t w2, bool two_sided) {
+  if (S == 8 && vmin < 0) return kEval;
+  const bool gt_all = S == 8 ? (uint64_t)vmin > w1 : vmin > (int64_t)w1;
+  const bool gt_none = S == 8 ? (uint64_t)vmax <= w1 : vmax <= (int64_t)w1;
+  if (!two_sided) return gt_all ? kAll : (gt_none ? kNone : kEval);
+  const bool lt_all = S == 8 ? (uint64_t)vmax < w2 : vmax < (int64_t)w2;
+  const bool lt_none = S == 8 ? (uint64_t)vmin >= w2 : vmin >= (int64_t)w2;
+  if (gt_none || lt_none) return kNone;
+  return gt_all && lt_all ? kAll : kEval;
+}
+
+template <int S, int CODEC>
+__device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t b, int close) {
+  constexpr uint32_t TB = 8u * S;
+  constexpr uint64_t TM = S == 8 ? ~0ull : 0xffffffffull;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  BlockPlan p;
+  p.vbase = b * a.bs;
+  p.len = (uint32_t)umin64((uint64_t)a.bs, a.n - p.vbase);
+  const uint64_t off = __ldg(a.offsets + b);
+  p.h = parse_header<CODEC, S>(a.payload, off);
+  p.raw = p.h.l == TB;
+  p.pred = kPredAbove;
+  p.mode = kEval;
+  p.lo = p.hi = 0;
+  p.f1 = a.f1 & TM;
+  p.f2 = a.f2 & TM;
+  p.bounded = CODEC == kLinear && !p.raw && p.h.l <= 61 && pred_in_range<kLinear>(p.h, p.len + 1);
+  const uint64_t step = a.base & TM;
+  if (p.h.l > TB) {  // sentinel or corrupt header: no case in the reference's filters
+    if ((threadIdx.x & 31) == 0) atomicOr(a.error, kErrBadHeader);
+    p.mode = kNone;
+    return p;
+  }
+  if (!close) {
+    p.hi = p.len;
+    if (a.zone && __ldg(a.zone + b) <= p.f1) {  // the experiment's zone-map skip (:247-249)
+      p.mode = kNone;
+    } else if (!p.raw && CODEC == kFor) {
+      const uint64_t mx = load_u64_at(words, off + 1 + S) & TM;  // header maximum (FOR_integer_template.h:143)
+      if (mx <= p.f1) p.mode = kNone;
+      else if (p.h.base > p.f1) p.mode = kAll;                   // the header minimum is above the filter
+    } else if (!p.raw) {  // the model's threshold index (piecewise_fix_integer_template.h:221-230)
+      const int64_t di = p.h.l ? (int64_t)1 << (p.h.l - 1) : 0;
+      const double q = __ddiv_rn(__dsub_rn(bound_plus<S>((p.f1 + 1) & TM, -di), p.h.a0), p.h.a1);
+      const int32_t thre = f2i32_x86(std_max(q, 0.));
+      if ((uint64_t)(int64_t)thre >= p.len) {
+        p.mode = kNone;
+      } else {
+        p.lo = (uint32_t)thre;
+        if (a.zone_lo && __ldg(a.zone_lo + b) > p.f1) {
+          p.mode = kAll;  // every value is above the filter: indices [thre, len)
+        } else if (p.bounded) {
+          int64_t vmin, vmax;
+          leco_value_bounds(p.h, p.lo, p.hi - 1, vmin, vmax);
+          p.mode = classify<S>(vmin, vmax, p.f1, 0, false);
+        }
+      }
+    }
+    if (p.mode == kNone) p.hi = p.lo;
+    return p;
+  }
+  p.hi = p.len;
+  if (CODEC == kFor) {
+    p.pred = kPredModulo;
+    return p;
+  }
+  if (a.zone) {  // first window from the block minimum (leco_int_fix_template.cpp:299-304)
+    const uint64_t zmin = __ldg(a.zone + b) & TM;
+    const double db = __ull2double_rn(step);
+    const double qb = __dmul_rn(ceil(__ddiv_rn(__ull2double_rn((zmin - p.f1) & TM), db)), db);
+    uint64_t w1 = f2T_x86<S>(__dadd_rn(qb, __ull2double_rn(p.f1)));
+    uint64_t w2 = f2T_x86<S>(__dadd_rn(qb, __ull2double_rn(p.f2)));
+    const uint64_t r = zmin % step;
+    if (r < p.f2 && r > p.f1) {
+      w1 = (w1 - step) & TM;
+      w2 = (w2 - step) & TM;
+    }
+    p.f1 = w1;
+    p.f2 = w2;
+  }
+  p.pred = p.raw ? kPredAnyWin : kPredWindows;
+  return p;
+}
+
+// Close range on a packed LeCo block, by one warp: the reference's window loop
+// (piecewise_fix_integer_template.h:275-298), windows in chunks of 32 (one per
+// lane).  Window p = (f1 + p*base, f2 + p*base) (bounds wrap in T) covers
+// indices [thre1, thre2) ([thre1, thre2] for l == 0); the loop ends at the
+// first window with thre1 >= len or thre2 <= 0.  A window whose value bounds lie
+// inside (outside) its bounds matches every (no) index without reading fields;
+// the others are evaluated 32 indices at a time.  Counts, or (write) stores the
+// matches from out position `run` on.
+template <int S, int CODEC, bool WRITE>
+__device__ uint64_t window_loop(const FilterLaunch &a, const BlockPlan &p, uint64_t run) {
+  constexpr uint64_t TM = S == 8 ? ~0ull : 0xffffffffull;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const uint64_t step = a.base & TM;
+  const int64_t di = p.h.l ? (int64_t)1 << (p.h.l - 1) : 0;
+  const double dlen = __uint2double_rn(p.len);
+  uint64_t total = 0;
+  for (uint32_t q0 = 0;; q0 += kFWin) {
+    const uint64_t q = q0 + lane;
+    const uint64_t w1 = (p.f1 + q * step) & TM, w2 = (p.f2 + q * step) & TM;
+    const int32_t t1 = f2i32_x86(std_max(__dsub_rn(__ddiv_rn(__dsub_rn(bound_plus<S>(w1, -di), p.h.a0), p.h.a1), 1.0), 0.));
+    const int32_t t2 = f2i32_x86(std_min(__dadd_rn(__ddiv_rn(__dsub_rn(bound_plus<S>(w2, di), p.h.a0), p.h.a1), 1.0), dlen));
+    const bool ok = (uint64_t)(int64_t)t1 < p.len && t2 > 0;
+    const uint32_t fails = __ballot_sync(0xffffffffu, !ok);
+    const uint32_t nwin = fails ? (uint32_t)(__ffs(fails) - 1) : kFWin;
+    if (q0 >= a.max_windows) {  // the loop would go on past the window limit
+      if (nwin && lane == 0 && !WRITE) atomicOr(a.error, kErrLimit);
+      break;
+    }
+    uint32_t size = 0;
+    int mode = kEval;
+    if (lane < nwin) {
+      const int32_t e = p.h.l ? t2 : t2 + 1;  // one past the window's last index
+      size = e > t1 ? (uint32_t)(e - t1) : 0u;
+      if (size && p.bounded) {
+        int64_t vmin, vmax;
+        leco_value_bounds(p.h, (uint32_t)t1, (uint32_t)(e - 1), vmin, vmax);
+        mode = classify<S>(vmin, vmax, w1, w2, true);
+      }
+    }
+    for (uint32_t w = 0; w < nwin; ++w) {
+      const uint32_t sz = __shfl_sync(0xffffffffu, size, w);
+      const int md = __shfl_sync(0xffffffffu, mode, w);
+      if (!sz || md == kNone) continue;
+      const uint32_t k0 = (uint32_t)__shfl_sync(0xffffffffu, t1, w);
+      if (md == kAll) {
+        if (WRITE)
+          for (uint32_t j = lane; j < sz; j += 32) {
+            const uint64_t pos = run + total + j;
+            if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + k0 + j);
+          }
+        total += sz;
+        continue;
+      }
+      const uint64_t lo1 = __shfl_sync(0xffffffffu, w1, w), hi2 = __shfl_sync(0xffffffffu, w2, w);
+      for (uint32_t j0 = 0; j0 < sz; j0 += 32) {
+        const uint32_t k = k0 + j0 + lane;
+        bool fl = false;
+        if (j0 + lane < sz) {
+          const uint64_t v = filter_value<S, CODEC>(words, p.h, false, k);
+          fl = cmp_gt<S>(v, lo1) && cmp_lt<S>(v, hi2);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, fl);
+        if (WRITE && fl) {
+          const uint64_t pos = run + total + __popc(m & ((1u << lane) - 1u));
+          if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + k);
+        }
+        total += __popc(m);
+      }
+    }
+    if (nwin < kFWin) break;
+  }
+  return total;
+}
+
+template <int S, int CODEC>
+__global__ void __launch_bounds__(kFT, 4) filter_kernel(FilterLaunch a, int close) {
+  extern __shared__ __align__(16) uint32_t fmask[];
+  __shared__ uint32_t cta_ticket;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *mask = fmask + (size_t)warp * a.mask_words;
+  if (threadIdx.x == 0) cta_ticket = atomicAdd(a.ticket, 1u);  // one ticket per CTA: kFB consecutive blocks
+  __syncthreads();  // the only CTA barrier: warps are independent from here on
+  const uint64_t b = (uint64_t)cta_ticket * kFB + warp;
+  if (b >= a.nb) return;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+
+  // ---- counting -----------------------------------------------------------------
+  const BlockPlan p = plan_block<S, CODEC>(a, b, close);
+  uint64_t cnt = 0;
+  if (p.pred == kPredWindows) {
+    cnt = window_loop<S, CODEC, false>(a, p, 0);
+  } else if (p.mode == kAll) {
+    cnt = p.hi - p.lo;
+  } else if (p.mode == kEval) {
+    const uint64_t step = a.base & (S == 8 ? ~0ull : 0xffffffffull);
+    for (uint32_t s0 = p.lo; s0 < p.hi; s0 += 32 * kFU) {
+      uint32_t m[kFU];
+#pragma unroll
+      for (int u = 0; u < kFU; ++u) {
+        const uint32_t k = s0 + u * 32 + lane;
+        bool fl = false;
+        if (k < p.hi) fl = single_pred<S>(p.pred, filter_value<S, CODEC>(words, p.h, p.raw, k), p.f1, p.f2, step);
+        m[u] = __ballot_sync(0xffffffffu, fl);
+      }
+#pragma unroll
+      for (int u = 0; u < kFU; ++u) {
+        if (lane == u) mask[((s0 - p.lo) >> 5) + u] = m[u];
+        cnt += __popc(m[u]);
+      }
+    }
+  }
+
+  // ---- output offset by look-back -------------------------------------------------
+  const uint64_t excl = lookback_prefix(a.status, b, cnt, a.error);
+  if (excl == ~0ull) return;  // a predecessor never published: error word set
+  if (b == a.nb - 1 && lane == 0) *a.count = excl + cnt;
+  if (!cnt) return;
+  __syncwarp();  // bitmap words written by other lanes
+
+  // ---- writing ------------------------------------------------------------------
+  if (p.pred == kPredWindows) {
+    window_loop<S, CODEC, true>(a, p, excl);
+    return;
+  }
+  if (p.mode == kAll) {
+    const uint32_t c = p.hi - p.lo;
+    for (uint32_t j = lane; j < c; j += 32) {
+      const uint64_t pos = excl + j;
+      if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + p.lo + j);
+    }
+    return;
+  }
+  uint64_t run = excl;
+  const uint32_t nwords = (p.hi - p.lo + 31) >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t w0 = 0; w0 < nwords; w0 += kFU) {
+    uint32_t m[kFU];
+#pragma unroll
+    for (int u = 0; u < kFU; ++u) m[u] = w0 + u < nwords ? mask[w0 + u] : 0u;
+#pragma unroll
+    for (int u = 0; u < kFU; ++u) {
+      if ((m[u] >> lane) & 1u) {
+        const uint64_t pos = run + __popc(m[u] & lt);
+        if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + p.lo + (w0 + u) * 32 + lane);
+      }
+      run += __popc(m[u]);
+    }
+  }
+}
+
+// ---- zone map: per-block minimum and maximum of the decoded values -------------------
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256) zonemap_kernel(DecodeLaunch a, uint64_t *zmin, uint64_t *zmax) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  constexpr uint64_t TM = S == 8 ? ~0ull : 0xffffffffull;
+  __shared__ u128 red[66];
+  const uint64_t b = blockIdx.x;
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const uint64_t off = __ldg(a.offsets + b);
+  const BlockHdr h = parse_header<CODEC, S>(a.payload, off);
+  if (h.l == 126 || h.l == 127 || h.l > TB) {
+    if (threadIdx.x == 0) {
+      atomicOr(a.error, kErrBadHeader);
+      zmin[b] = 0;
+      zmax[b] = 0;
+    }
+    return;
+  }
+  const bool raw = h.l == TB;
+  if (CODEC == kFor && !raw) {  // the header holds both
+    if (threadIdx.x == 0) {
+      zmin[b] = h.base;
+      zmax[b] = load_u64_at(words, off + 1 + S) & TM;
+    }
+    return;
+  }
+  uint64_t mn = ~0ull, mx = 0;
+  if (CODEC == kDelta && !raw) {
+    const DeltaChunk c = delta_chunk_start<256>(words, h, len);
+    uint64_t run = c.run;
+    for (uint32_t k = c.k0; k < c.k1; ++k) {
+      const uint64_t v = run & TM;
+      mn = v < mn ? v : mn;
+      mx = v > mx ? v : mx;
+      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+    }
+  } else {
+    const uint32_t l = raw ? TB : h.l;
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+      const uint64_t f = l ? load_field(words, h.body_bit + (uint64_t)k * l, l) : 0;
+      const uint64_t v = (raw ? f : value_from_field<CODEC, S>(h, k, f)) & TM;
+      mn = v < mn ? v : mn;
+      mx = v > mx ? v : mx;
+    }
+  }
+  u128 A = mn, B = mx;
+  block_reduce2<2, 1>(A, B, red);
+  if (threadIdx.x == 0) {
+    zmin[b] = (uint64_t)A;
+    zmax[b] = (uint64_t)B;
+  }
+}
+
+template <int S, int CODEC>
+static int run_filter(FilterLaunch L, int close, cudaStream_t st) {
+  L.mask_words = (L.bs + 127) / 128 * 4;
+  const int smem = (int)(kFB * L.mask_words * 4);
+  if (cudaFuncSetAttribute(filter_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
+  filter_kernel<S, CODEC><<<(unsigned)((L.nb + kFB - 1) / kFB), kFT, smem, st>>>(L, close);
+  return 0;
+}
+
+int launch_filter(int codec, int s, const FilterLaunch &L, int close, cudaStream_t st) {
+  if (!L.nb) return 0;
+  if (s == 4) {
+    if (codec == kLinear) return run_filter<4, kLinear>(L, close, st);
+    if (codec == kFor) return run_filter<4, kFor>(L, close, st);
+  } else {
+    if (codec == kLinear) return run_filter<8, kLinear>(L, close, st);
+    if (codec == kFor) return run_filter<8, kFor>(L, close, st);
+  }
+  return 1;
+}
+
+template <typename T, int CODEC>
+static void run_zonemap(const DecodeLaunch &L, uint64_t nb, uint64_t *zmin, uint64_t *zmax, cudaStream_t st) {
+  if (nb) zonemap_kernel<T, CODEC><<<(unsigned)nb, 256, 0, st>>>(L, zmin, zmax);
+}
+int launch_zonemap(int codec, int s, const DecodeLaunch &L, uint64_t *zmin, uint64_t *zmax, cudaStream_t st) {
+  const uint64_t nb = (L.n + L.bs - 1) / L.bs;
+  if (s == 4) {
+    switch (codec) {
+      case kLinear: run_zonemap<uint32_t, kLinear>(L, nb, zmin, zmax, st); return 0;
+      case kFor: run_zonemap<uint32_t, kFor>(L, nb, zmin, zmax, st); return 0;
+      case kDelta: run_zonemap<uint32_t, kDelta>(L, nb, zmin, zmax, st); return 0;
+      case kPoly2: run_zonemap<uint32_t, kPoly2>(L, nb, zmin, zmax, st); return 0;
+    }
+  } else {
+    switch (codec) {
+      case kLinear: run_zonemap<uint64_t, kLinear>(L, nb, zmin, zmax, st); return 0;
+      case kFor: run_zonemap<uint64_t, kFor>(L, nb, zmin, zmax, st); return 0;
+      case kDelta: run_zonemap<uint64_t, kDelta>(L, nb, zmin, zmax, st); return 0;
+      case kPoly2: run_zonemap<uint64_t, kPoly2>(L, nb, zmin, zmax, st); return 0;
+    }
+  }
+  return 1;
+}
+
+}  // namespace leco

@@ -46,7 +46,31 @@ struct GatherLaunch {
   uint32_t *error;
 };
 
+// Predicate pushdown over a column (leco_filter.cu).
+struct FilterLaunch {
+  const uint8_t *payload;
+  const uint64_t *offsets;
+  uint64_t n;
+  uint32_t bs;
+  uint64_t nb;
+  uint64_t f1, f2;       // range: f1 = the filter; close range: the window (LeCo) or residue (FOR) bounds
+  uint64_t base;         // close range: window step (LeCo) / modulus (FOR), 1..INT32_MAX
+  const uint64_t *zone;  // range: per-block maxima (nullable); close-range LeCo: per-block minima (nullable)
+  const uint64_t *zone_lo;  // range: per-block minima (nullable)
+  uint32_t *out;
+  uint64_t cap;
+  uint64_t *count;
+  uint64_t *status;      // look-back words, nb of them, zeroed
+  uint32_t *ticket;      // zeroed
+  uint32_t *error;
+  uint32_t max_windows;  // close-range LeCo: windows per block before kErrLimit (a multiple of 32)
+  uint32_t mask_words;   // per-block match bitmap words (set by the launcher)
+  int stage;             // payload is 16-byte aligned: fields may be staged by bulk copies
+};
+
 int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st);
+int launch_filter(int codec, int s, const FilterLaunch &L, int close, cudaStream_t st);
+int launch_zonemap(int codec, int s, const DecodeLaunch &L, uint64_t *zmin, uint64_t *zmax, cudaStream_t st);
 int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st);
 int launch_gather(int codec, int s, const GatherLaunch &L, cudaStream_t st);
 int launch_sum(int codec, int s, const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st);
