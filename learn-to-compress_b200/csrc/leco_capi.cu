@@ -278,7 +278,7 @@ static int filter_setup(const char *fn, int codec, int dtype, const uint8_t *d_p
   L.ticket = reinterpret_cast<uint32_t *>(L.status + nb);
   L.error = err;
   L.max_windows = 65536;
-  L.stage = (reinterpret_cast<uintptr_t>(d_payload) & 15) == 0;
+  L.vec_out = (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
   LECO_CUDA(cudaMemsetAsync(d_ws, 0, nb * 8 + 8, st));
   if (!nb) LECO_CUDA(cudaMemsetAsync(d_count, 0, 8, st));
   return LECO_OK;

@@ -21,6 +21,8 @@
 // keeps the match bitmap in shared memory and, once the offset is known, a
 // writing pass (bitmap read back, or the windows evaluated again from
 // L1-resident fields).
+#include <algorithm>
+
 #include "leco_decode.cuh"
 #include "leco_encode.cuh"
 
@@ -139,6 +141,47 @@ __device__ __forceinline__ int classify(int64_t vmin, int64_t vmax, uint64_t w1,
   return gt_all && lt_all ? kAll : kEval;
 }
 
+// Per-index forms of the window classification for a bounded packed LeCo
+// block: every value at k is above w1 (resp. below w2).  Monotone in k because
+// the predictions are.
+template <int S>
+__device__ __forceinline__ bool surely_above(const BlockHdr &h, int64_t m, uint32_t k, uint64_t w1) {
+  const int64_t v = __double2ll_rz(pred_linear(h.a0, h.a1, k)) - m;
+  return S == 8 ? (v >= 0 && (uint64_t)v > w1) : v > (int64_t)w1;
+}
+template <int S>
+__device__ __forceinline__ bool surely_below(const BlockHdr &h, int64_t m, uint32_t k, uint64_t w2) {
+  const int64_t v = __double2ll_rz(pred_linear(h.a0, h.a1, k)) + m;
+  return S == 8 ? (w2 > 0x7fffffffffffffffull || v < (int64_t)w2) : v < (int64_t)w2;
+}
+// First k in [lo, hi) where a monotone predicate changes from `from` to its
+// opposite (hi when it never does).
+template <typename P>
+__device__ __forceinline__ uint32_t first_change(uint32_t lo, uint32_t hi, bool from, P pred) {
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (pred(mid) == from) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+// The indices [ia, ib) of window [k0, k1) whose values all lie inside
+// (w1, w2); the rest of the window must be read.  ia == ib: none.
+template <int S>
+__device__ __forceinline__ void surely_inside(const BlockHdr &h, uint32_t k0, uint32_t k1, uint64_t w1, uint64_t w2,
+                                              uint32_t &ia, uint32_t &ib) {
+  const int64_t m = h.l ? (((int64_t)1 << (h.l - 1)) - 1) : 0;
+  auto above = [&](uint32_t k) { return surely_above<S>(h, m, k, w1); };
+  auto below = [&](uint32_t k) { return surely_below<S>(h, m, k, w2); };
+  if (h.a1 >= 0) {  // predictions non-decreasing: above turns true, below turns false
+    ia = first_change(k0, k1, false, above);
+    ib = first_change(ia, k1, true, below);
+  } else {          // non-increasing: below turns true, above turns false
+    ia = first_change(k0, k1, false, below);
+    ib = first_change(ia, k1, true, above);
+  }
+}
+
 template <int S, int CODEC>
 __device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t b, int close) {
   constexpr uint32_t TB = 8u * S;
@@ -213,6 +256,38 @@ __device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t 
   return p;
 }
 
+// Writes the consecutive indices idx0 .. idx0+cnt-1 to out[pos ...] (positions
+// at or past cap are dropped), by one warp: 16-byte stores once pos is aligned
+// when the output buffer itself is 16-byte aligned.
+__device__ __forceinline__ void write_run(const FilterLaunch &a, uint64_t pos, uint32_t idx0, uint32_t cnt) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t head = cnt;
+  if (a.vec_out) head = min(cnt, (uint32_t)((4u - (uint32_t)(pos & 3)) & 3u));
+  for (uint32_t j = lane; j < head; j += 32)
+    if (pos + j < a.cap) a.out[pos + j] = idx0 + j;
+  if (head == cnt) return;
+  pos += head;
+  idx0 += head;
+  cnt -= head;
+  const uint32_t nvec = cnt >> 2;
+  uint4 *o4 = reinterpret_cast<uint4 *>(a.out + pos);
+  for (uint32_t v = lane; v < nvec; v += 32) {
+    const uint64_t q = pos + 4ull * v;
+    const uint32_t x = idx0 + 4 * v;
+    if (q + 4 <= a.cap) {
+      __stcs(o4 + v, make_uint4(x, x + 1, x + 2, x + 3));
+    } else {
+      for (uint32_t t = 0; t < 4; ++t)
+        if (q + t < a.cap) a.out[q + t] = x + t;
+    }
+  }
+  const uint32_t rem = cnt & 3;
+  if (lane < rem) {
+    const uint64_t q = pos + 4ull * nvec + lane;
+    if (q < a.cap) a.out[q] = idx0 + 4 * nvec + lane;
+  }
+}
+
 // Close range on a packed LeCo block, by one warp: the reference's window loop
 // (piecewise_fix_integer_template.h:275-298), windows in chunks of 32 (one per
 // lane).  Window p = (f1 + p*base, f2 + p*base) (bounds wrap in T) covers
@@ -242,45 +317,54 @@ __device__ uint64_t window_loop(const FilterLaunch &a, const BlockPlan &p, uint6
       if (nwin && lane == 0 && !WRITE) atomicOr(a.error, kErrLimit);
       break;
     }
-    uint32_t size = 0;
-    int mode = kEval;
+    // window [k0, e): read [k0, ia) and [ib, e), all of [ia, ib) matches
+    uint32_t k0 = 0, e = 0, ia = 0, ib = 0;
     if (lane < nwin) {
-      const int32_t e = p.h.l ? t2 : t2 + 1;  // one past the window's last index
-      size = e > t1 ? (uint32_t)(e - t1) : 0u;
-      if (size && p.bounded) {
-        int64_t vmin, vmax;
-        leco_value_bounds(p.h, (uint32_t)t1, (uint32_t)(e - 1), vmin, vmax);
-        mode = classify<S>(vmin, vmax, w1, w2, true);
+      const int32_t ee = p.h.l ? t2 : t2 + 1;  // one past the window's last index
+      if (ee > t1) {
+        k0 = (uint32_t)t1;
+        e = (uint32_t)ee;
+        ia = ib = e;  // undecided: read everything
+        if (p.bounded) {
+          int64_t vmin, vmax;
+          leco_value_bounds(p.h, k0, e - 1, vmin, vmax);
+          const int mode = classify<S>(vmin, vmax, w1, w2, true);
+          if (mode == kNone) e = ia = ib = k0;
+          else if (mode == kAll) ia = k0;
+          else surely_inside<S>(p.h, k0, e, w1, w2, ia, ib);
+          if (ib <= ia) ia = ib = e;
+        }
       }
     }
     for (uint32_t w = 0; w < nwin; ++w) {
-      const uint32_t sz = __shfl_sync(0xffffffffu, size, w);
-      const int md = __shfl_sync(0xffffffffu, mode, w);
-      if (!sz || md == kNone) continue;
-      const uint32_t k0 = (uint32_t)__shfl_sync(0xffffffffu, t1, w);
-      if (md == kAll) {
-        if (WRITE)
-          for (uint32_t j = lane; j < sz; j += 32) {
-            const uint64_t pos = run + total + j;
-            if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + k0 + j);
-          }
-        total += sz;
-        continue;
-      }
+      const uint32_t wk0 = __shfl_sync(0xffffffffu, k0, w), we = __shfl_sync(0xffffffffu, e, w);
+      if (we <= wk0) continue;
+      const uint32_t wa = __shfl_sync(0xffffffffu, ia, w), wb = __shfl_sync(0xffffffffu, ib, w);
       const uint64_t lo1 = __shfl_sync(0xffffffffu, w1, w), hi2 = __shfl_sync(0xffffffffu, w2, w);
-      for (uint32_t j0 = 0; j0 < sz; j0 += 32) {
-        const uint32_t k = k0 + j0 + lane;
-        bool fl = false;
-        if (j0 + lane < sz) {
-          const uint64_t v = filter_value<S, CODEC>(words, p.h, false, k);
-          fl = cmp_gt<S>(v, lo1) && cmp_lt<S>(v, hi2);
+      // three runs in index order: read [wk0, wa), all of [wa, wb), read [wb, we)
+      for (int part = 0; part < 3; ++part) {
+        const uint32_t r0 = part == 0 ? wk0 : (part == 1 ? wa : wb);
+        const uint32_t r1 = part == 0 ? wa : (part == 1 ? wb : we);
+        if (r1 <= r0) continue;
+        if (part == 1) {
+          if (WRITE) write_run(a, run + total, (uint32_t)(p.vbase + r0), r1 - r0);
+          total += r1 - r0;
+          continue;
         }
-        const uint32_t m = __ballot_sync(0xffffffffu, fl);
-        if (WRITE && fl) {
-          const uint64_t pos = run + total + __popc(m & ((1u << lane) - 1u));
-          if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + k);
+        for (uint32_t k1 = r0; k1 < r1; k1 += 32) {
+          const uint32_t k = k1 + lane;
+          bool fl = false;
+          if (k < r1) {
+            const uint64_t v = filter_value<S, CODEC>(words, p.h, false, k);
+            fl = cmp_gt<S>(v, lo1) && cmp_lt<S>(v, hi2);
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, fl);
+          if (WRITE && fl) {
+            const uint64_t pos = run + total + __popc(m & ((1u << lane) - 1u));
+            if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + k);
+          }
+          total += __popc(m);
         }
-        total += __popc(m);
       }
     }
     if (nwin < kFWin) break;
@@ -288,65 +372,68 @@ __device__ uint64_t window_loop(const FilterLaunch &a, const BlockPlan &p, uint6
   return total;
 }
 
-template <int S, int CODEC>
-__global__ void __launch_bounds__(kFT, 4) filter_kernel(FilterLaunch a, int close) {
-  extern __shared__ __align__(16) uint32_t fmask[];
-  __shared__ uint32_t cta_ticket;
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t *mask = fmask + (size_t)warp * a.mask_words;
-  if (threadIdx.x == 0) cta_ticket = atomicAdd(a.ticket, 1u);  // one ticket per CTA: kFB consecutive blocks
-  __syncthreads();  // the only CTA barrier: warps are independent from here on
-  const uint64_t b = (uint64_t)cta_ticket * kFB + warp;
-  if (b >= a.nb) return;
-  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+__device__ __forceinline__ BlockPlan shfl_plan(const BlockPlan &q, int src) {
+  BlockPlan p;
+  p.h.body_bit = __shfl_sync(0xffffffffu, q.h.body_bit, src);
+  p.h.l = __shfl_sync(0xffffffffu, q.h.l, src);
+  p.h.a0 = __shfl_sync(0xffffffffu, q.h.a0, src);
+  p.h.a1 = __shfl_sync(0xffffffffu, q.h.a1, src);
+  p.h.a2 = 0;
+  p.h.base = __shfl_sync(0xffffffffu, q.h.base, src);
+  p.vbase = __shfl_sync(0xffffffffu, q.vbase, src);
+  p.len = __shfl_sync(0xffffffffu, q.len, src);
+  p.lo = __shfl_sync(0xffffffffu, q.lo, src);
+  p.hi = __shfl_sync(0xffffffffu, q.hi, src);
+  p.pred = __shfl_sync(0xffffffffu, q.pred, src);
+  p.mode = __shfl_sync(0xffffffffu, q.mode, src);
+  p.raw = __shfl_sync(0xffffffffu, (int)q.raw, src) != 0;
+  p.bounded = __shfl_sync(0xffffffffu, (int)q.bounded, src) != 0;
+  p.f1 = __shfl_sync(0xffffffffu, q.f1, src);
+  p.f2 = __shfl_sync(0xffffffffu, q.f2, src);
+  return p;
+}
 
-  // ---- counting -----------------------------------------------------------------
-  const BlockPlan p = plan_block<S, CODEC>(a, b, close);
+// Matches of one block (warp-uniform), keeping the match bitmap of a read
+// single-window block in `mask`.
+template <int S, int CODEC>
+__device__ __forceinline__ uint64_t count_block(const FilterLaunch &a, const BlockPlan &p, uint32_t *mask) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (p.pred == kPredWindows) return window_loop<S, CODEC, false>(a, p, 0);
+  if (p.mode == kAll) return p.hi - p.lo;
+  if (p.mode != kEval) return 0;
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const uint64_t step = a.base & (S == 8 ? ~0ull : 0xffffffffull);
   uint64_t cnt = 0;
-  if (p.pred == kPredWindows) {
-    cnt = window_loop<S, CODEC, false>(a, p, 0);
-  } else if (p.mode == kAll) {
-    cnt = p.hi - p.lo;
-  } else if (p.mode == kEval) {
-    const uint64_t step = a.base & (S == 8 ? ~0ull : 0xffffffffull);
-    for (uint32_t s0 = p.lo; s0 < p.hi; s0 += 32 * kFU) {
-      uint32_t m[kFU];
+  for (uint32_t s0 = p.lo; s0 < p.hi; s0 += 32 * kFU) {
+    uint32_t m[kFU];
 #pragma unroll
-      for (int u = 0; u < kFU; ++u) {
-        const uint32_t k = s0 + u * 32 + lane;
-        bool fl = false;
-        if (k < p.hi) fl = single_pred<S>(p.pred, filter_value<S, CODEC>(words, p.h, p.raw, k), p.f1, p.f2, step);
-        m[u] = __ballot_sync(0xffffffffu, fl);
-      }
+    for (int u = 0; u < kFU; ++u) {
+      const uint32_t k = s0 + u * 32 + lane;
+      bool fl = false;
+      if (k < p.hi) fl = single_pred<S>(p.pred, filter_value<S, CODEC>(words, p.h, p.raw, k), p.f1, p.f2, step);
+      m[u] = __ballot_sync(0xffffffffu, fl);
+    }
 #pragma unroll
-      for (int u = 0; u < kFU; ++u) {
-        if (lane == u) mask[((s0 - p.lo) >> 5) + u] = m[u];
-        cnt += __popc(m[u]);
-      }
+    for (int u = 0; u < kFU; ++u) {
+      if (lane == u) mask[((s0 - p.lo) >> 5) + u] = m[u];
+      cnt += __popc(m[u]);
     }
   }
+  return cnt;
+}
 
-  // ---- output offset by look-back -------------------------------------------------
-  const uint64_t excl = lookback_prefix(a.status, b, cnt, a.error);
-  if (excl == ~0ull) return;  // a predecessor never published: error word set
-  if (b == a.nb - 1 && lane == 0) *a.count = excl + cnt;
-  if (!cnt) return;
-  __syncwarp();  // bitmap words written by other lanes
-
-  // ---- writing ------------------------------------------------------------------
+// Writes the matches of one block from output position `run` on.
+template <int S, int CODEC>
+__device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPlan &p, const uint32_t *mask, uint64_t run) {
+  const uint32_t lane = threadIdx.x & 31;
   if (p.pred == kPredWindows) {
-    window_loop<S, CODEC, true>(a, p, excl);
+    window_loop<S, CODEC, true>(a, p, run);
     return;
   }
   if (p.mode == kAll) {
-    const uint32_t c = p.hi - p.lo;
-    for (uint32_t j = lane; j < c; j += 32) {
-      const uint64_t pos = excl + j;
-      if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + p.lo + j);
-    }
+    write_run(a, run, (uint32_t)(p.vbase + p.lo), p.hi - p.lo);
     return;
   }
-  uint64_t run = excl;
   const uint32_t nwords = (p.hi - p.lo + 31) >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t w0 = 0; w0 < nwords; w0 += kFU) {
@@ -361,6 +448,57 @@ __global__ void __launch_bounds__(kFT, 4) filter_kernel(FilterLaunch a, int clos
       }
       run += __popc(m[u]);
     }
+  }
+}
+
+// One warp per group of a.group consecutive blocks (at most 32).  A CTA takes
+// kFB groups by one ticket; its warps are then independent: lane j plans block
+// j of the group (all header, offset and zone-map loads of the group in flight
+// at once), the warp counts the blocks one after another, finds the group's
+// output offset by look-back (the CTA's earlier warps and earlier CTAs are all
+// resident or done, so every wait ends) and writes.
+template <int S, int CODEC>
+__global__ void __launch_bounds__(kFT, 3) filter_kernel(FilterLaunch a, int close) {
+  extern __shared__ __align__(16) uint32_t fmask[];
+  __shared__ uint32_t cta_ticket;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *mask = fmask + (size_t)warp * a.group * a.mask_words;
+  if (threadIdx.x == 0) cta_ticket = atomicAdd(a.ticket, 1u);
+  __syncthreads();  // the only CTA barrier: warps are independent from here on
+  const uint64_t grp = (uint64_t)cta_ticket * kFB + warp;
+  const uint64_t b0 = grp * a.group;
+  if (b0 >= a.nb) return;
+  const uint32_t nblk = (uint32_t)umin64(a.group, a.nb - b0);
+
+  // ---- counting -----------------------------------------------------------------
+  BlockPlan mine;
+  if (lane < nblk) mine = plan_block<S, CODEC>(a, b0 + lane, close);
+  uint64_t mycnt = 0;
+  for (uint32_t j = 0; j < nblk; ++j) {
+    const BlockPlan p = shfl_plan(mine, j);
+    const uint64_t c = count_block<S, CODEC>(a, p, mask + j * a.mask_words);
+    if (lane == j) mycnt = c;
+  }
+
+  // ---- output offset by look-back -------------------------------------------------
+  const uint64_t tot = warp_sum_u64(mycnt);
+  const uint64_t excl = lookback_prefix(a.status, grp, tot, a.error);
+  if (excl == ~0ull) return;  // a predecessor never published: error word set
+  if (b0 + nblk == a.nb && lane == 0) *a.count = excl + tot;
+  if (!tot) return;
+  uint64_t inc = mycnt;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= (uint32_t)d) inc += y;
+  }
+  const uint64_t myoff = excl + inc - mycnt;
+  __syncwarp();  // bitmap words written by other lanes
+
+  // ---- writing ------------------------------------------------------------------
+  for (uint32_t j = 0; j < nblk; ++j) {
+    if (!__shfl_sync(0xffffffffu, mycnt, j)) continue;
+    const BlockPlan p = shfl_plan(mine, j);
+    write_block<S, CODEC>(a, p, mask + j * a.mask_words, __shfl_sync(0xffffffffu, myoff, j));
   }
 }
 
@@ -423,9 +561,11 @@ __global__ void __launch_bounds__(256) zonemap_kernel(DecodeLaunch a, uint64_t *
 template <int S, int CODEC>
 static int run_filter(FilterLaunch L, int close, cudaStream_t st) {
   L.mask_words = (L.bs + 127) / 128 * 4;
-  const int smem = (int)(kFB * L.mask_words * 4);
+  L.group = std::max(1u, std::min(32u, 1024u / L.mask_words));  // 4 KB of bitmaps per warp
+  const int smem = (int)(kFB * L.group * L.mask_words * 4);
   if (cudaFuncSetAttribute(filter_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
-  filter_kernel<S, CODEC><<<(unsigned)((L.nb + kFB - 1) / kFB), kFT, smem, st>>>(L, close);
+  const uint64_t groups = (L.nb + L.group - 1) / L.group;
+  filter_kernel<S, CODEC><<<(unsigned)((groups + kFB - 1) / kFB), kFT, smem, st>>>(L, close);
   return 0;
 }
 

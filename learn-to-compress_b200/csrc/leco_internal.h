@@ -65,7 +65,8 @@ struct FilterLaunch {
   uint32_t *error;
   uint32_t max_windows;  // close-range LeCo: windows per block before kErrLimit (a multiple of 32)
   uint32_t mask_words;   // per-block match bitmap words (set by the launcher)
-  int stage;             // payload is 16-byte aligned: fields may be staged by bulk copies
+  uint32_t group;        // blocks per warp (set by the launcher)
+  int vec_out;           // out is 16-byte aligned: runs of indices are written with 16-byte stores
 };
 
 int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st);

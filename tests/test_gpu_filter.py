@@ -121,6 +121,12 @@ def test_output_capacity_and_empty_column(lc, orc, dev):
     assert c == len(x) - 4  # values 12, 15, ... are above 10
     assert np.array_equal(_idx(got, 64), np.arange(4, 68, dtype=np.uint32))
     assert np.all(out[64:].cpu().numpy() == -1)  # nothing past out_cap
+    # an output buffer that is not 16-byte aligned, and a cap inside a 4-index run
+    out2 = torch.full((200,), -1, dtype=torch.int32, device=dev)
+    got, c = col.filter_range(10, out=out2[1:], out_cap=63)
+    assert c == len(x) - 4
+    assert np.array_equal(_idx(got, 63), np.arange(4, 67, dtype=np.uint32))
+    assert out2[0].item() == -1 and np.all(out2[64:].cpu().numpy() == -1)
     empty = lc.Column(0, 8, 0, 1000, col.payload, col.offsets)
     got, c = empty.filter_range(0)
     assert c == 0
