@@ -356,6 +356,16 @@ int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_byt
 int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
                       uint32_t to_find, void *h_value);
 
+/* Leco_int<T> / FOR_int<T>::filter_range(in, length, filter, out, block_id)
+ * (close = 0; piecewise_fix_integer_template.h:206-252, FOR_integer_template.h:115-160) or
+ * filter_range_close(in, length, out, block_id, filter1, filter2, base)
+ * (close = 1; :254-303, :166-215) on one block image: indices block_start + k into h_out
+ * (at most out_cap written).  Returns the count (which may exceed out_cap) or a negative
+ * status.  block_start = block_id * block_size, as the reference computes it. */
+int64_t leco_block_filter(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
+                          uint32_t block_start, int close, uint64_t filter1, uint64_t filter2, uint64_t base,
+                          uint32_t *h_out, uint64_t out_cap);
+
 /* ---- validation / errors ------------------------------------------------ */
 
 /* Host-side validation of an imported column before any launch: offsets

@@ -83,6 +83,21 @@ class LecoBlockCodec {
     return v;
   }
 
+  // Indices block_id*block_size + k of the values above `filter` (Leco_int / FOR_int
+  // only; piecewise_fix_integer_template.h:206-252, FOR_integer_template.h:115-160).
+  // Like the reference, `out` must have room for every match; returns the count.
+  int filter_range(uint8_t *in, const size_t length, T filter, uint32_t *out, size_t block_id) {
+    return run_filter(in, length, out, block_id, 0, (uint64_t)filter, 0, 0);
+  }
+  // Close range: windows (filter1 + p*base, filter2 + p*base) for Leco_int, residues
+  // filter1 < v % base < filter2 for FOR_int (:254-303, FOR :166-215).  Indices of every
+  // window are appended (the reference overwrites earlier windows' for l > 0); the count
+  // is the reference's.
+  int filter_range_close(uint8_t *in, const size_t length, uint32_t *out, size_t block_id, T filter1, T filter2,
+                         int base) {
+    return run_filter(in, length, out, block_id, 1, (uint64_t)filter1, (uint64_t)filter2, (uint64_t)(int64_t)base);
+  }
+
   // ---- column extensions (one launch per column) -------------------------------------
   // Encodes data[0..n) in blocks of block_size: payload = concatenated block images,
   // offsets[b] = byte offset of block b, offsets[nblocks] = total.
@@ -101,6 +116,21 @@ class LecoBlockCodec {
   }
   void gather(const uint8_t *payload, const uint64_t *offsets, size_t n, const uint64_t *idx, size_t m, T *out) const {
     leco_detail::check(leco_gather_host(CODEC, (int)sizeof(T), payload, offsets, n, (uint32_t)block_size, idx, m, out), "gather");
+  }
+
+ private:
+  int run_filter(const uint8_t *in, size_t length, uint32_t *out, size_t block_id, int close, uint64_t f1, uint64_t f2,
+                 uint64_t base) {
+    const uint64_t bytes = leco_detail::image_bytes(CODEC, (int)sizeof(T), in, (uint32_t)length);
+    const uint32_t start = (uint32_t)(block_id * (size_t)block_size);
+    uint64_t cap = length + 1;  // every index once, plus the l == 0 window end
+    int64_t c = leco_block_filter(CODEC, (int)sizeof(T), in, bytes, (uint32_t)length, start, close, f1, f2, base, out, cap);
+    leco_detail::check(c, close ? "filter_range_close" : "filter_range");
+    if ((uint64_t)c > cap) {  // overlapping windows counted an index more than once
+      c = leco_block_filter(CODEC, (int)sizeof(T), in, bytes, (uint32_t)length, start, close, f1, f2, base, out, (uint64_t)c);
+      leco_detail::check(c, "filter_range_close");
+    }
+    return (int)c;
   }
 };
 

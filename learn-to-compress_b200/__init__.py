@@ -72,6 +72,7 @@ SIGNATURES = [
     ("leco_filter_range", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _P, _P, _P, _U64, _P, _P, _U64, _P]),
     ("leco_filter_range_close", _I, [_I, _I, _P, _P, _U64, _U32, _U64, _U64, _U64, _P, _P, _U64, _P, _P, _U64, _P]),
     ("leco_zonemap", _I, [_I, _I, _P, _P, _U64, _U32, _P, _P, _P]),
+    ("leco_block_filter", ctypes.c_int64, [_I, _I, _P, _U64, _U32, _U32, _I, _U64, _U64, _U64, _P, _U64]),
     ("leco_encode_host", _I, [_I, _I, _P, _U64, _U32, _I, _P, _U64, _P, _P]),
     ("leco_decode_host", _I, [_I, _I, _P, _P, _U64, _U32, _P]),
     ("leco_gather_host", _I, [_I, _I, _P, _P, _U64, _U32, _P, _U64, _P]),
@@ -211,12 +212,42 @@ class _BlockCodec:
         return int(v[0])
 
 
-class Leco_int(_BlockCodec):
+class _FilterCodec(_BlockCodec):
+    """The two reference classes with predicate pushdown: ``filter_range(in_,
+    length, filter, out, block_id)`` and ``filter_range_close(in_, length, out,
+    block_id, filter1, filter2, base)`` write indices block_id*block_size + k
+    into the uint32 array ``out`` and return the count."""
+
+    def _filter(self, in_, length, out, block_id, close, f1, f2, base):
+        buf = np.frombuffer(bytes(in_), np.uint8).copy()
+        s = self.dtype.itemsize
+        start = block_id * self.block_size
+        m = 1 << (8 * s)
+        cap = length + 1
+        while True:
+            tmp = np.zeros(cap, np.uint32)
+            c = _check(lib().leco_block_filter(self.CODEC, s, _np_ptr(buf), len(buf), length, start, close, int(f1) % m,
+                                               int(f2) % m, base, _np_ptr(tmp), cap), "filter")
+            if c <= cap:
+                break
+            cap = c
+        out[:c] = tmp[:c]
+        return c
+
+    def filter_range(self, in_, length: int, filt: int, out: np.ndarray, block_id: int = 0) -> int:
+        return self._filter(in_, length, out, block_id, 0, filt, 0, 0)
+
+    def filter_range_close(self, in_, length: int, out: np.ndarray, block_id: int, filter1: int, filter2: int,
+                           base: int) -> int:
+        return self._filter(in_, length, out, block_id, 1, filter1, filter2, base)
+
+
+class Leco_int(_FilterCodec):
     """Mirror of ``Codecset::Leco_int<T>`` (piecewise_fix_integer_template.h:14-338)."""
     CODEC = LINEAR
 
 
-class FOR_int(_BlockCodec):
+class FOR_int(_FilterCodec):
     """Mirror of ``Codecset::FOR_int<T>`` (FOR_integer_template.h:14-249)."""
     CODEC = FOR
 

@@ -553,6 +553,56 @@ int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_byt
   return leco_decode_host(codec, dtype, tmp.data(), off, length, length, h_out);
 }
 
+int64_t leco_block_filter(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
+                          uint32_t block_start, int close, uint64_t filter1, uint64_t filter2, uint64_t base,
+                          uint32_t *h_out, uint64_t out_cap) {
+  if (!h_in || !in_bytes || !length || length > LECO_MAX_BLOCK || (out_cap && !h_out))
+    return fail(LECO_ERR_ARG, "leco_block_filter: bad argument");
+  cudaStream_t st;
+  LECO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int64_t rc = 0;
+  {
+    std::vector<uint8_t> tmp(in_bytes + LECO_PAYLOAD_SLACK, 0);
+    memcpy(tmp.data(), h_in, in_bytes);
+    const uint64_t off[2] = {0, in_bytes};
+    const uint64_t wsb = leco_filter_workspace_bytes(length, length);
+    DevBuf pay, doff, out, cnt, ws;
+    if (pay.alloc(tmp.size(), st) || doff.alloc(16, st) || out.alloc(out_cap * 4, st) || cnt.alloc(8, st) ||
+        ws.alloc(wsb, st)) {
+      rc = fail(LECO_ERR_NOMEM, "leco_block_filter: device allocation failed");
+    } else {
+      cudaMemcpyAsync(pay.p, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(doff.p, off, 16, cudaMemcpyHostToDevice, st);
+      const leco_stream_t ls = reinterpret_cast<leco_stream_t>(st);
+      rc = close ? leco_filter_range_close(codec, dtype, (const uint8_t *)pay.p, (const uint64_t *)doff.p, length, length,
+                                           filter1, filter2, base, nullptr, (uint32_t *)out.p, out_cap,
+                                           (uint64_t *)cnt.p, ws.p, wsb, ls)
+                 : leco_filter_range(codec, dtype, (const uint8_t *)pay.p, (const uint64_t *)doff.p, length, length,
+                                     filter1, nullptr, nullptr, (uint32_t *)out.p, out_cap, (uint64_t *)cnt.p, ws.p,
+                                     wsb, ls);
+      uint64_t c = 0;
+      if (!rc) {
+        cudaMemcpyAsync(&c, cnt.p, 8, cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "leco_block_filter");
+      }
+      if (!rc && (rc = leco_check(ls)) == 0) {
+        const uint64_t w = std::min<uint64_t>(c, out_cap);
+        if (w) {
+          cudaMemcpyAsync(h_out, out.p, w * 4, cudaMemcpyDeviceToHost, st);
+          cudaError_t e = cudaStreamSynchronize(st);
+          if (e != cudaSuccess) rc = cuda_fail(e, "leco_block_filter");
+          for (uint64_t i = 0; i < w && !rc; ++i) h_out[i] += block_start;
+        }
+        if (!rc) rc = (int64_t)c;
+      }
+    }
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return rc;
+}
+
 int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
                       uint32_t to_find, void *h_value) {
   if (!h_in || !h_value || to_find >= length) return fail(LECO_ERR_ARG, "leco_block_random: bad argument");

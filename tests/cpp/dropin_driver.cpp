@@ -3,6 +3,8 @@
 // every block, random-access sampled positions, check everything against the input), run on
 // the GPU codec.  Writes the concatenated block images to argv[1] for the pytest that compares
 // them with the oracle.  Exit status 0 = every self-check passed.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -50,8 +52,64 @@ static int run(const char *name, std::vector<T> &data, int blocks, FILE *out) {
   return bad;
 }
 
+// The reference's filter experiments (experiments/leco_int_fix_template.cpp:216-326,
+// FOR_int_fix_template.cpp:226-322) on the drop-in classes: zone map from the data, the
+// filter_range loop with its zone-map skip, the close-range loop with LeCo's per-block window
+// start.  Writes (count, indices) of both loops to `out` for the pytest to compare with the
+// oracle.
+template <typename Codec>
+static void filter_experiment(const std::vector<uint64_t> &data, int blocks, uint64_t filter1, uint64_t filter2,
+                              uint64_t base, bool leco, FILE *out) {
+  Codec codec;
+  const int N = (int)data.size();
+  int block_size = N / blocks;
+  blocks = N / block_size;
+  if (blocks * block_size < N) blocks++;
+  codec.init(blocks, block_size);
+  std::vector<uint8_t *> block_start_vec;
+  std::vector<std::pair<uint64_t, uint64_t>> zonemap;
+  for (int i = 0; i < blocks; i++) {
+    int len = (i == blocks - 1) ? N - (blocks - 1) * block_size : block_size;
+    uint8_t *descriptor = (uint8_t *)malloc((size_t)len * 8 * 4 + 64);
+    codec.encodeArray8_int(data.data() + (size_t)i * block_size, len, descriptor, i);
+    block_start_vec.push_back(descriptor);
+    uint64_t lo = UINT64_MAX, hi = 0;
+    for (int j = 0; j < len; j++) {
+      lo = std::min(lo, data[(size_t)i * block_size + j]);
+      hi = std::max(hi, data[(size_t)i * block_size + j]);
+    }
+    zonemap.emplace_back(lo, hi);
+  }
+  std::vector<uint32_t> bit_pos(data.size() + blocks);
+  int total_counter = 0;
+  for (int i = 0; i < blocks; i++) {
+    if (zonemap[i].second <= filter1) continue;
+    int len = (i == blocks - 1) ? N - (blocks - 1) * block_size : block_size;
+    total_counter += codec.filter_range(block_start_vec[i], len, filter1, bit_pos.data() + total_counter, i);
+  }
+  fwrite(&total_counter, 4, 1, out);
+  fwrite(bit_pos.data(), 4, total_counter, out);
+  total_counter = 0;
+  for (int i = 0; i < blocks && base; i++) {
+    int len = (i == blocks - 1) ? N - (blocks - 1) * block_size : block_size;
+    uint64_t f1 = filter1, f2 = filter2;
+    if (leco) {
+      f1 = ceil((double)(zonemap[i].first - filter1) / (double)base) * base + filter1;
+      f2 = ceil((double)(zonemap[i].first - filter1) / (double)base) * base + filter2;
+      if (zonemap[i].first % base < filter2 && zonemap[i].first % base > filter1) {
+        f1 -= base;
+        f2 -= base;
+      }
+    }
+    total_counter += codec.filter_range_close(block_start_vec[i], len, bit_pos.data() + total_counter, i, f1, f2, (int)base);
+  }
+  fwrite(&total_counter, 4, 1, out);
+  fwrite(bit_pos.data(), 4, total_counter, out);
+  for (auto *p : block_start_vec) free(p);
+}
+
 int main(int argc, char **argv) {
-  if (argc < 2) return 2;
+  if (argc < 3) return 2;
   FILE *out = fopen(argv[1], "wb");
   if (!out) return 2;
   const int N = 200000;
@@ -82,6 +140,13 @@ int main(int argc, char **argv) {
   col.gather(payload.data(), offsets.data(), N, idx.data(), idx.size(), got.data());
   for (size_t i = 0; i < idx.size(); i++) bad += got[i] != k64[idx[i]];
   fclose(out);
+  FILE *fout = fopen(argv[2], "wb");
+  if (!fout) return 2;
+  const uint64_t median = k64[N / 2];
+  filter_experiment<Codecset::Leco_int<uint64_t>>(k64, 49, median, median, 0, true, fout);
+  filter_experiment<Codecset::Leco_int<uint64_t>>(k64, 49, 1ull << 28, 1ull << 29, 1ull << 30, true, fout);
+  filter_experiment<Codecset::FOR_int<uint64_t>>(k64, 49, 1000, 40000, 65536, false, fout);
+  fclose(fout);
   printf("total mismatches %d\n", bad);
   return bad ? 1 : 0;
 }

@@ -34,7 +34,8 @@ def test_cpp_dropin_driver(tmp_path, orc, lc):
                            os.path.join(ROOT, "tests", "cpp", "dropin_driver.cpp"), "-L", lib_dir, "-lleco_b200",
                            f"-Wl,-rpath,{lib_dir}", "-o", str(exe)])
     out = tmp_path / "blocks.bin"
-    r = subprocess.run([str(exe), str(out)], capture_output=True, text=True, timeout=600)
+    fout = tmp_path / "filters.bin"
+    r = subprocess.run([str(exe), str(out), str(fout)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     k32, k64 = _keys()
     data = out.read_bytes()
@@ -55,3 +56,27 @@ def test_cpp_dropin_driver(tmp_path, orc, lc):
                 img = mask_delta_last_fields(np.frombuffer(img, np.uint8), off, s, m, m).tobytes()
                 ref = mask_delta_last_fields(np.frombuffer(ref, np.uint8), np.array([0, len(ref)], np.uint64), s, m, m).tobytes()
             assert img == ref, (codec, b)
+
+    # the filter experiments through the drop-in classes == the oracle's column loops
+    fdata = fout.read_bytes()
+    fpos = 0
+
+    def take():
+        nonlocal fpos
+        c = struct.unpack_from("<i", fdata, fpos)[0]
+        idx = np.frombuffer(fdata, np.uint32, c, fpos + 4)
+        fpos += 4 + 4 * c
+        return idx
+
+    bs = len(k64) // 49
+    med = int(k64[len(k64) // 2])
+    for codec, f1, f2, base in ((0, med, med, 0), (0, 1 << 28, 1 << 29, 1 << 30), (1, 1000, 40000, 65536)):
+        pay, off = orc.encode_column(codec, k64, bs)
+        zmin = np.array([k64[i:i + bs].min() for i in range(0, len(k64), bs)], np.uint64)
+        zmax = np.array([k64[i:i + bs].max() for i in range(0, len(k64), bs)], np.uint64)
+        got = take()
+        assert np.array_equal(got, orc.filter_column(codec, pay, off, len(k64), 8, bs, f1, zmax)), (codec, "range")
+        got = take()
+        if base:
+            c, want = orc.filter_close_column(codec, pay, off, len(k64), 8, bs, f1, f2, base, zmin if codec == 0 else None)
+            assert len(got) == c and np.array_equal(got, want[:c]), (codec, "close")

@@ -178,3 +178,39 @@ def test_large_sorted_column_counts(lc, orc, dev):
         want = orc.filter_column(0, pay, off, n, 8, bs, f)
         assert c == len(want) and np.array_equal(_idx(got, c), want)
         assert np.array_equal(want, np.nonzero(x > f)[0].astype(np.uint32))
+
+
+def test_block_mirror_matches_reference_fixture(lc, orc):
+    """Leco_int / FOR_int .filter_range / .filter_range_close one block at a
+    time (the reference's call shape) against the reference's own per-block
+    results stored in the fixtures (count always; indices where the
+    reference's buffer is defined, i.e. not for l > 0 LeCo close range)."""
+    fx = np.load(FIX)
+    checked = 0
+    for key, s, codec, bs, n, x, pay, off, filters in _fixture_columns():
+        cls = lc.Leco_int if codec == 0 else lc.FOR_int
+        c_ = cls(np.uint64 if s == 8 else np.uint32)
+        c_.init(len(off) - 1, bs)
+        for j, (kind, a, b, base) in enumerate(filters):
+            counts, outs = fx[f"{key}__f{j}__counts"], fx[f"{key}__f{j}__out"]
+            pos = 0
+            for blk in range(len(off) - 1):
+                img = pay[off[blk]:off[blk + 1]].tobytes()
+                ln = min(bs, n - blk * bs)
+                cr = int(counts[blk])
+                ref = outs[pos:pos + max(cr, 0)]
+                pos += max(cr, 0)
+                if cr < 0 or (codec == 1 and img[0] == 8 * s - 1):
+                    continue  # undefined in the reference (checked against the oracle elsewhere)
+                buf = np.zeros(4 * ln + 8, np.uint32)
+                if kind == 0:
+                    c = c_.filter_range(img, ln, a, buf, blk)
+                    assert c == cr and np.array_equal(buf[:c], ref), (key, j, blk)
+                else:
+                    f1, f2 = (int(fx[f"{key}__f{j}__w1"][blk]), int(fx[f"{key}__f{j}__w2"][blk])) if codec == 0 else (a, b)
+                    c = c_.filter_range_close(img, ln, buf, blk, f1, f2, base)
+                    assert c == cr, (key, j, blk)
+                    if codec == 1 or img[0] == 0:
+                        assert np.array_equal(buf[:c], ref), (key, j, blk)
+                checked += 1
+    assert checked > 1500
