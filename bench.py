@@ -423,6 +423,11 @@ def run_varlen(args, world, rank, local):
     t0 = time.perf_counter()
     starts = lc.varlen_partition(xh, n // 2000, 12)
     t_part = time.perf_counter() - t0
+    pws = torch.empty(int(lc.lib().leco_varlen_partition_workspace_bytes(n, n // 2000)), dtype=torch.uint8, device=dev)
+    dstarts = lc.varlen_partition_device(x, n // 2000, 12, ws=pws)
+    assert np.array_equal(dstarts.cpu().numpy().view(np.uint64), starts), "GPU partition differs from the host's"
+    t_part_dev = ev_time(lambda: lc.varlen_partition_device(x, n // 2000, 12, ws=pws), reps=3)
+    del dstarts, pws
     vc = lc.varlen_encode(x, starts, lc.FIT_REFERENCE)
     out = torch.empty_like(x)
     idx = torch.randint(0, n, (RA_BATCH,), device=dev)
@@ -430,6 +435,7 @@ def run_varlen(args, world, rank, local):
     res = {}
     res["varlen"] = {
         "segments": int(len(starts)), "partition_host_s": round(t_part, 3), "host_threads": os.cpu_count(),
+        "partition_gpu_ms": round(t_part_dev, 2),
         "encode_ms": round(ev_time(lambda: lc.varlen_encode(x, vc.starts, lc.FIT_REFERENCE,
                                                             max_segment_len=vc.max_segment_len)), 3),
         "decode_ms": round(ev_time(lambda: vc.decode(out=out)), 3),

@@ -221,6 +221,17 @@ int leco_zonemap(int codec, int dtype, const uint8_t *d_payload, const uint64_t 
  * *nseg.  threads <= 0: all host cores. */
 int leco_varlen_partition(const uint64_t *h_values, uint64_t n, uint32_t coarse_blocks, int64_t delta,
                           uint64_t *h_starts, uint64_t starts_cap, uint64_t *nseg, int threads);
+/* The same partitioner on the GPU (same segment starts bit for bit): one thread per
+ * coarse block, each with a private scratch slot in d_ws (the segment list of the
+ * split/merge phase, then the segment starts and sizes of the pairwise passes).
+ * d_values on the device; writes d_starts (<= starts_cap; the error word records an
+ * overflow) and *d_nseg on the device.  d_ws: leco_varlen_partition_workspace_bytes()
+ * bytes, 256-byte aligned (about 56 bytes per value of the coarse block size per
+ * resident thread, plus 4 bytes per value). */
+uint64_t leco_varlen_partition_workspace_bytes(uint64_t n, uint32_t coarse_blocks);
+int leco_varlen_partition_device(const uint64_t *d_values, uint64_t n, uint32_t coarse_blocks, int64_t delta,
+                                 uint64_t *d_starts, uint64_t starts_cap, uint64_t *d_nseg, void *d_ws, uint64_t ws_bytes,
+                                 leco_stream_t stream);
 uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg);
 uint64_t leco_varlen_workspace_bytes(uint64_t nseg);
 /* Longest segment leco_varlen_encode accepts (values). */

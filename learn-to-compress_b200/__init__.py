@@ -96,6 +96,8 @@ SIGNATURES = [
     ("leco_server_reset_stats", _I, [_P]),
     ("leco_server_destroy", _I, [_P]),
     ("leco_varlen_partition", _I, [_P, _U64, _U32, ctypes.c_int64, _P, _U64, _P, _I]),
+    ("leco_varlen_partition_workspace_bytes", _U64, [_U64, _U32]),
+    ("leco_varlen_partition_device", _I, [_P, _U64, _U32, ctypes.c_int64, _P, _U64, _P, _P, _U64, _P]),
     ("leco_varlen_max_payload_bytes", _U64, [_U64, _U64]),
     ("leco_varlen_workspace_bytes", _U64, [_U64]),
     ("leco_varlen_max_segment", _U64, []),
@@ -658,6 +660,23 @@ def varlen_partition(values: np.ndarray, coarse_blocks: int, delta: int, threads
     _check(lib().leco_varlen_partition(_np_ptr(values), len(values), coarse_blocks, delta, _np_ptr(out), len(out),
                                        ctypes.byref(ns), threads), "leco_varlen_partition")
     return out[: ns.value].copy()
+
+
+def varlen_partition_device(values, coarse_blocks: int, delta: int, ws=None, stream=None):
+    """Segment starts (int64 CUDA tensor holding uint64) of a uint64 column
+    already on the device (int64 tensor), computed on the GPU."""
+    torch = _torch()
+    n = values.numel()
+    need = int(lib().leco_varlen_partition_workspace_bytes(n, coarse_blocks))
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=values.device)
+    starts = torch.empty(n, dtype=torch.int64, device=values.device)
+    nseg = torch.zeros(1, dtype=torch.int64, device=values.device)
+    _check(lib().leco_varlen_partition_device(_tptr(values), n, coarse_blocks, delta, _tptr(starts), n, _tptr(nseg),
+                                              _tptr(ws), ws.numel(), _stream_ptr(stream)), "leco_varlen_partition_device")
+    k = int(nseg.item())
+    _check(lib().leco_check(_stream_ptr(stream)), "leco_varlen_partition_device")
+    return starts[:k]
 
 
 @dataclass

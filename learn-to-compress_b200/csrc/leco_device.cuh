@@ -46,6 +46,18 @@ __device__ __forceinline__ uint64_t f2T_x86(double x) {
   return (uint64_t)(uint32_t)f2i_x86(x);
 }
 
+// (__int128)x: truncation toward zero (gcc's __fixdfti) for |x| < 2^127; used where
+// the variable-length codec converts its prediction to a 128-bit integer
+// (piecewise_cost_merge_integer_template_double_wo_round.h:92,158).
+__device__ __forceinline__ i128 f2i128(double x) {
+  if (fabs(x) < 9223372036854775808.0) return (i128)__double2ll_rz(x);
+  const uint64_t bits = (uint64_t)__double_as_longlong(x);
+  const int e = (int)((bits >> 52) & 0x7ff) - 1075;
+  const uint64_t m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+  const i128 v = e >= 0 ? ((i128)m << e) : (i128)(m >> (-e));
+  return x < 0 ? -v : v;
+}
+
 template <typename T>
 __device__ __forceinline__ double to_double(T v);
 template <>

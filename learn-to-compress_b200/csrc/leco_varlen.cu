@@ -20,16 +20,6 @@ namespace leco {
 
 constexpr uint32_t kVarlenMaxSeg = 16384;  // values per segment the encoder stages in shared memory
 
-__device__ __forceinline__ i128 f2i128(double x) {
-  // truncation toward zero (__fixdfti) for |x| < 2^127
-  if (fabs(x) < 9223372036854775808.0) return (i128)__double2ll_rz(x);
-  const uint64_t bits = (uint64_t)__double_as_longlong(x);
-  const int e = (int)((bits >> 52) & 0x7ff) - 1075;
-  const uint64_t m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
-  const i128 v = e >= 0 ? ((i128)m << e) : (i128)(m >> (-e));
-  return x < 0 ? -v : v;
-}
-
 struct VarArgs {
   const uint64_t *values;
   uint64_t n;

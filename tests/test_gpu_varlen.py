@@ -72,3 +72,48 @@ def test_varlen_short_and_raw_segments(lc, orc, dev):
     idx = torch.arange(n, device=dev)
     assert torch.equal(col.gather(idx), xd)
     lc.check()
+
+
+def _starts(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+def test_device_partition_golden(lc, golden, dev):
+    """The GPU partitioner on the reference fixture's column gives the
+    reference's segment starts."""
+    x = golden["varlen__values"]
+    st = lc.varlen_partition_device(_dev(x, dev), 10, 20)
+    assert np.array_equal(_starts(st), golden["varlen__starts"].astype(np.uint64))
+
+
+def test_device_partition_matches_host(lc, dev):
+    """GPU partitioner == host partitioner (which the CPU tier pins to the
+    reference) over the value families, coarse block counts and merge
+    penalties of the reference comparison, ragged and one-value tail blocks
+    included."""
+    rng = np.random.default_rng(5)
+    checked = 0
+    for trial in range(40):
+        n = int(rng.choice([2, 3, 1000, 5000, 20011, 100000, 400_003]))
+        x = _gen(rng, n, trial % 4)
+        blocks = int(rng.choice([1, 3, 10, 50, 200]))
+        blocks = max(1, min(blocks, n // 2))
+        delta = int(rng.choice([0, 2, 12, 64]))
+        want = lc.varlen_partition(x, blocks, delta, threads=8)
+        got = _starts(lc.varlen_partition_device(_dev(x, dev), blocks, delta))
+        assert np.array_equal(got, want), (trial, n, blocks, delta)
+        checked += 1
+    assert checked == 40
+
+
+def test_device_partition_large(lc, dev):
+    """20M keys of the regime-switching generator in coarse blocks of 2000
+    values, merge penalty 12 bits (the variable-length benchmark's settings)."""
+    from leco_b200 import workloads
+
+    n = 20_000_000
+    x = workloads.regime_switching_u64(n, seed=11, device=dev)
+    xh = x.cpu().numpy().view(np.uint64)
+    got = _starts(lc.varlen_partition_device(x, n // 2000, 12))
+    want = lc.varlen_partition(xh, n // 2000, 12)
+    assert np.array_equal(got, want)
