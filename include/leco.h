@@ -377,6 +377,44 @@ int64_t leco_block_filter(int codec, int dtype, const uint8_t *h_in, uint64_t in
                           uint32_t block_start, int close, uint64_t filter1, uint64_t filter2, uint64_t base,
                           uint32_t *h_out, uint64_t out_cap);
 
+/* ---- container file, import / export ------------------------------------
+ * The reference has no file format: its drivers hold each block as a separate
+ * malloc'ed byte string (experiments/leco_int_fix_template.cpp:108-127).  A column
+ * container stores payload + offsets (+ segment starts) behind a 64-byte header
+ * with a checksum; reading checks the header, the offsets, the checksum and every
+ * block header before anything reaches a kernel (LECO_ERR_CORRUPT otherwise). */
+typedef struct leco_container_info {
+  int codec;            /* enum leco_codec                                   */
+  int dtype;            /* LECO_U32 / LECO_U64                               */
+  uint32_t block_size;  /* fixed-block codecs; 0 for variable-length          */
+  uint64_t n;           /* values                                            */
+  uint64_t nunits;      /* blocks or segments                                */
+  uint64_t payload_bytes;
+  int has_starts;       /* variable-length: segment starts stored            */
+} leco_container_info;
+
+/* Writes a column from host buffers (atomically: a temporary file renamed). */
+int leco_container_write(const char *path, const leco_container_info *info, const uint8_t *h_payload,
+                         const uint64_t *h_offsets, const uint64_t *h_starts);
+/* Reads the header (and checks offsets/starts) without the payload. */
+int leco_container_info_read(const char *path, leco_container_info *info);
+/* Reads a column into host buffers (payload_cap >= payload_bytes). */
+int leco_container_read(const char *path, uint8_t *h_payload, uint64_t payload_cap, uint64_t *h_offsets,
+                        uint64_t *h_starts);
+/* Device-buffer forms (synchronous; staged through host memory).  load: payload_cap >=
+ * payload_bytes + LECO_PAYLOAD_SLACK (the slack is zero-filled). */
+int leco_container_save_device(const char *path, const leco_container_info *info, const uint8_t *d_payload,
+                               const uint64_t *d_offsets, const uint64_t *d_starts, leco_stream_t stream);
+int leco_container_load_device(const char *path, uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets,
+                               uint64_t *d_starts, leco_stream_t stream);
+/* The reference drivers' per-block byte strings (block_start_vec[i], sizes) <-> a
+ * column's payload + offsets, byte for byte.  export: h_blocks may be NULL to get the
+ * sizes only; otherwise each h_blocks[i] must hold h_sizes[i] bytes. */
+int leco_import_blocks(const uint8_t *const *h_blocks, const uint64_t *h_sizes, uint64_t nblocks, uint8_t *h_payload,
+                       uint64_t payload_cap, uint64_t *h_offsets);
+int leco_export_blocks(const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t nblocks, uint8_t *const *h_blocks,
+                       uint64_t *h_sizes);
+
 /* ---- validation / errors ------------------------------------------------ */
 
 /* Host-side validation of an imported column before any launch: offsets

@@ -80,6 +80,13 @@ SIGNATURES = [
     ("leco_block_decode", _I, [_I, _I, _P, _U64, _U32, _P]),
     ("leco_block_random", _I, [_I, _I, _P, _U64, _U32, _U32, _P]),
     ("leco_validate_host", _I, [_I, _I, _P, _U64, _P, _U64, _U32, _P]),
+    ("leco_container_write", _I, [ctypes.c_char_p, _P, _P, _P, _P]),
+    ("leco_container_info_read", _I, [ctypes.c_char_p, _P]),
+    ("leco_container_read", _I, [ctypes.c_char_p, _P, _U64, _P, _P]),
+    ("leco_container_save_device", _I, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
+    ("leco_container_load_device", _I, [ctypes.c_char_p, _P, _U64, _P, _P, _P]),
+    ("leco_import_blocks", _I, [_P, _P, _U64, _P, _U64, _P]),
+    ("leco_export_blocks", _I, [_P, _P, _U64, _P, _P]),
     ("leco_batch_create", _I, [_P, _U32, _I, _P]),
     ("leco_batch_destroy", _I, [_P]),
     ("leco_batch_total_blocks", _U64, [_P]),
@@ -265,6 +272,72 @@ class Leco_int_poly(_BlockCodec):
 
 
 # ---------------------------------------------------------------------------
+# Container files and the reference's per-block byte strings.
+# ---------------------------------------------------------------------------
+
+class ContainerInfo(ctypes.Structure):
+    _fields_ = [("codec", ctypes.c_int), ("dtype", ctypes.c_int), ("block_size", ctypes.c_uint32),
+                ("n", ctypes.c_uint64), ("nunits", ctypes.c_uint64), ("payload_bytes", ctypes.c_uint64),
+                ("has_starts", ctypes.c_int)]
+
+
+def container_write(path: str, codec: int, dtype: int, block_size: int, n: int, payload: np.ndarray,
+                    offsets: np.ndarray, starts: Optional[np.ndarray] = None) -> None:
+    """Writes a column (host arrays) to a container file."""
+    payload = np.ascontiguousarray(payload, np.uint8)
+    offsets = np.ascontiguousarray(offsets, np.uint64)
+    info = ContainerInfo(codec, dtype, block_size, n, len(offsets) - 1, int(offsets[-1]), int(starts is not None))
+    st = np.ascontiguousarray(starts, np.uint64) if starts is not None else None
+    _check(lib().leco_container_write(os.fsencode(path), ctypes.byref(info), _np_ptr(payload), _np_ptr(offsets),
+                                      _np_ptr(st) if st is not None else None), "leco_container_write")
+
+
+def container_info(path: str) -> dict:
+    info = ContainerInfo()
+    _check(lib().leco_container_info_read(os.fsencode(path), ctypes.byref(info)), "leco_container_info_read")
+    return {f: getattr(info, f) for f, _ in ContainerInfo._fields_}
+
+
+def container_read(path: str):
+    """(info dict, payload uint8, offsets uint64, starts uint64 or None) of a
+    container file, checked (header, offsets, checksum, block headers)."""
+    info = container_info(path)
+    pay = np.zeros(info["payload_bytes"], np.uint8)
+    off = np.zeros(info["nunits"] + 1, np.uint64)
+    st = np.zeros(info["nunits"], np.uint64) if info["has_starts"] else None
+    _check(lib().leco_container_read(os.fsencode(path), _np_ptr(pay), len(pay), _np_ptr(off),
+                                     _np_ptr(st) if st is not None else None), "leco_container_read")
+    return info, pay, off, st
+
+
+def import_blocks(blocks) -> tuple:
+    """The reference drivers' per-block byte strings -> (payload, offsets)."""
+    blocks = [bytes(b) for b in blocks]
+    bufs = [np.frombuffer(b, np.uint8) for b in blocks]
+    ptrs = (ctypes.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+    sizes = np.array([len(b) for b in blocks], np.uint64)
+    pay = np.zeros(int(sizes.sum()), np.uint8)
+    off = np.zeros(len(blocks) + 1, np.uint64)
+    _check(lib().leco_import_blocks(ptrs, _np_ptr(sizes), len(blocks), _np_ptr(pay), len(pay), _np_ptr(off)),
+           "leco_import_blocks")
+    return pay, off
+
+
+def export_blocks(payload: np.ndarray, offsets: np.ndarray) -> list:
+    """(payload, offsets) -> the per-block byte strings, as the reference's
+    encodeArray8_int returned them."""
+    payload = np.ascontiguousarray(payload, np.uint8)
+    offsets = np.ascontiguousarray(offsets, np.uint64)
+    nb = len(offsets) - 1
+    sizes = np.zeros(nb, np.uint64)
+    _check(lib().leco_export_blocks(_np_ptr(payload), _np_ptr(offsets), nb, None, _np_ptr(sizes)), "leco_export_blocks")
+    bufs = [np.zeros(int(z), np.uint8) for z in sizes]
+    ptrs = (ctypes.c_void_p * nb)(*[b.ctypes.data for b in bufs])
+    _check(lib().leco_export_blocks(_np_ptr(payload), _np_ptr(offsets), nb, ptrs, _np_ptr(sizes)), "leco_export_blocks")
+    return [b.tobytes() for b in bufs]
+
+
+# ---------------------------------------------------------------------------
 # Device-resident columns.
 # ---------------------------------------------------------------------------
 
@@ -433,6 +506,28 @@ class Column:
         off = self.offsets.cpu().numpy().view(np.uint64)
         pay = self.payload[: int(off[-1])].cpu().numpy()
         return pay, off
+
+    def save(self, path: str, stream=None) -> None:
+        """Writes the column to a container file (leco_container_save_device)."""
+        info = ContainerInfo(self.codec, self.dtype, self.block_size, self.n, self.nblocks, self.nbytes, 0)
+        _check(lib().leco_container_save_device(os.fsencode(path), ctypes.byref(info), _tptr(self.payload),
+                                                _tptr(self.offsets), None, _stream_ptr(stream)), "leco_container_save_device")
+
+    @classmethod
+    def load(cls, path: str, device="cuda", stream=None) -> "Column":
+        """A column read from a container file into device memory (checked
+        before it reaches a kernel), with its random-access directory."""
+        torch = _torch()
+        info = container_info(path)
+        if info["codec"] == VARLEN:
+            raise LecoError(-1, "a variable-length container: use VarlenColumn.load")
+        pay = torch.empty(info["payload_bytes"] + PAYLOAD_SLACK, dtype=torch.uint8, device=device)
+        off = torch.empty(info["nunits"] + 1, dtype=torch.int64, device=device)
+        _check(lib().leco_container_load_device(os.fsencode(path), _tptr(pay), pay.numel(), _tptr(off), None,
+                                                _stream_ptr(stream)), "leco_container_load_device")
+        col = cls(info["codec"], info["dtype"], info["n"], info["block_size"], pay, off)
+        col.build_directory()
+        return col
 
     @classmethod
     def from_host(cls, codec: int, dtype: int, n: int, block_size: int, payload: np.ndarray, offsets: np.ndarray,
@@ -606,6 +701,8 @@ class Server:
                 c.build_directory()
             descs[i] = ColumnDesc(c.codec, c.dtype, c.block_size, 0, c.n, None, None, c.payload.data_ptr(),
                                   c.payload.numel(), c.offsets.data_ptr(), c.dir.data_ptr())
+        self.options = dict(slots=slots, max_requests_per_batch=max_requests_per_batch,
+                            hbm_budget_bytes=hbm_budget_bytes, max_items_per_batch=max_items_per_batch)
         opt = ServerOptions(slots, max_requests_per_batch, max_items_per_batch, 0, hbm_budget_bytes)
         h = _P()
         _check(L.leco_server_create(descs, len(self.columns), ctypes.byref(opt), ctypes.byref(h)), "leco_server_create")
@@ -635,6 +732,35 @@ class Server:
 
     def reset_stats(self):
         _check(lib().leco_server_reset_stats(self._h), "leco_server_reset_stats")
+
+    def checkpoint(self, directory: str) -> None:
+        """Saves the resident columns (one container file each) and the server
+        options (manifest.json) after draining the requests in flight."""
+        import json
+
+        self.drain()
+        os.makedirs(directory, exist_ok=True)
+        names = []
+        for i, c in enumerate(self.columns):
+            name = f"column_{i:05d}.leco"
+            c.save(os.path.join(directory, name))
+            names.append(name)
+        tmp = os.path.join(directory, "manifest.json.tmp")
+        with open(tmp, "w") as f:
+            json.dump({"format": "leco-server-checkpoint-1", "columns": names, "options": self.options}, f)
+        os.replace(tmp, os.path.join(directory, "manifest.json"))
+
+    @classmethod
+    def resume(cls, directory: str, device="cuda") -> "Server":
+        """A server over the columns of a checkpoint, with its options."""
+        import json
+
+        with open(os.path.join(directory, "manifest.json")) as f:
+            m = json.load(f)
+        if m.get("format") != "leco-server-checkpoint-1":
+            raise LecoError(-3, f"{directory}: not a server checkpoint")
+        cols = [Column.load(os.path.join(directory, name), device=device) for name in m["columns"]]
+        return cls(cols, **m["options"])
 
     def close(self):
         if getattr(self, "_h", None):
@@ -720,6 +846,25 @@ class VarlenColumn:
     def to_host(self):
         off = self.offsets.cpu().numpy().view(np.uint64)
         return self.payload[: int(off[-1])].cpu().numpy(), off, self.starts.cpu().numpy().view(np.uint64)
+
+    def save(self, path: str, stream=None) -> None:
+        info = ContainerInfo(VARLEN, 8, 0, self.n, self.nseg, self.nbytes, 1)
+        _check(lib().leco_container_save_device(os.fsencode(path), ctypes.byref(info), _tptr(self.payload),
+                                                _tptr(self.offsets), _tptr(self.starts), _stream_ptr(stream)),
+               "leco_container_save_device")
+
+    @classmethod
+    def load(cls, path: str, device="cuda", stream=None) -> "VarlenColumn":
+        torch = _torch()
+        info = container_info(path)
+        if info["codec"] != VARLEN:
+            raise LecoError(-1, "a fixed-block container: use Column.load")
+        pay = torch.empty(info["payload_bytes"] + PAYLOAD_SLACK, dtype=torch.uint8, device=device)
+        off = torch.empty(info["nunits"] + 1, dtype=torch.int64, device=device)
+        st = torch.empty(info["nunits"], dtype=torch.int64, device=device)
+        _check(lib().leco_container_load_device(os.fsencode(path), _tptr(pay), pay.numel(), _tptr(off), _tptr(st),
+                                                _stream_ptr(stream)), "leco_container_load_device")
+        return cls(info["n"], st, pay, off)
 
 
 def varlen_encode(values, starts, fit_mode: int = FIT_REFERENCE, stream=None, max_segment_len: int = 0) -> VarlenColumn:
