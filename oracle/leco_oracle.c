@@ -856,3 +856,107 @@ size_t oracle_column_filter_close(int codec, const uint8_t *payload, const uint6
   }
   return c;
 }
+
+/* ---- legacy u32 format: piecewise_fix_op_max ------------------------------ */
+
+/* piecewise_fix_op_max::encodeArray8 (piecewise_fix_op_minimize_maxerror.h:45-119):
+ * lr_int fit (lr.h:89-111, the same sums as lr_int_T), slope stored as float, the
+ * midpoint shift in int arithmetic, int residuals against (long long)(theta0 +
+ * theta1*i), width bits(max |r|) + 1; header [u8 l][f64 theta0][f32 theta1]; body
+ * packed with write_delta_T (bit_write.h:186-245, pad (32-l)/8 bytes) for l <= 30,
+ * the values as u32 (write_delta_default, :395-410) for l >= 31.
+ * diff_plus / diff_minus (nullable, n bytes each) receive the encoder's
+ * mul_add_diff_set / mul_add_diff_set_minus flags (:79-84): where the prediction
+ * accumulated by addition is below / above the multiplied one.  Returns bytes. */
+size_t oracle_legacy_encode(const uint32_t *in, size_t n, uint8_t *out, uint8_t *diff_plus, uint8_t *diff_minus) {
+  double t0, t1d;
+  oracle_lr_fit(in, 4, (int)n, &t0, &t1d);
+  const float t1 = (float)t1d;
+  int32_t mx = INT32_MIN, mn = INT32_MAX;
+  for (size_t i = 0; i < n; i++) {
+    int32_t d = (int32_t)((int64_t)in[i] - x86_f2i(t0 + (double)t1 * (double)i));
+    if (d > mx) mx = d;
+    if (d < mn) mn = d;
+  }
+  t0 += (double)(int32_t)((uint32_t)mx + (uint32_t)mn) / 2.0;
+  double pred = t0;
+  uint32_t maxe = 0;
+  int32_t *delta = (int32_t *)__builtin_alloca(n * sizeof(int32_t) + 4);
+  for (size_t i = 0; i < n; i++) {
+    const int64_t pm = x86_f2i(t0 + (double)t1 * (double)i), pa = x86_f2i(pred);
+    if (diff_plus) diff_plus[i] = pm > pa;
+    if (diff_minus) diff_minus[i] = pm < pa;
+    pred += (double)t1;
+    const int32_t d = (int32_t)((int64_t)in[i] - pm);
+    delta[i] = d;
+    const uint32_t a = d < 0 ? (uint32_t)(-(int64_t)d) : (uint32_t)d;
+    if (a > maxe) maxe = a;
+  }
+  const unsigned l = maxe ? (unsigned)oracle_bits(maxe) + 1 : 0;
+  out[0] = (uint8_t)l;
+  memcpy(out + 1, &t0, 8);
+  memcpy(out + 9, &t1, 4);
+  if (!l) return 13;
+  if (l >= 31) {
+    memcpy(out + 13, in, n * 4);
+    return 13 + n * 4;
+  }
+  const size_t nb = oracle_body_bytes_for(l, n); /* end + 1 + (32-l)/8 */
+  uint8_t *body = out + 13;
+  memset(body, 0, nb);
+  for (size_t i = 0; i < n; i++) {
+    const int32_t d = delta[i];
+    const uint64_t mag = d <= 0 ? (uint64_t)(-(int64_t)d) : (uint64_t)d;
+    put_field(body, (uint64_t)i * l, l, (mag & ((1ull << (l - 1)) - 1)) | ((uint64_t)(d > 0) << (l - 1)));
+  }
+  return 13 + nb;
+}
+
+/* Bulk decode.  add_pred = 1: piecewise_fix_op_max::decodeArray8 (:121-158) as
+ * written -- the prediction accumulated by repeated addition (read_all_bit_fix_add,
+ * bit_read.h:559-605; the l == 0 loop :148-153), which the reference's drivers then
+ * correct with the encoder's difference lists (experiments/fix_int.cpp:110-117);
+ * add_pred = 0: the multiplied prediction the encoder and the random access use,
+ * i.e. the stored values. */
+void oracle_legacy_decode(const uint8_t *in, size_t n, uint32_t *out, int add_pred) {
+  const unsigned l = in[0];
+  double t0;
+  float t1;
+  memcpy(&t0, in + 1, 8);
+  memcpy(&t1, in + 9, 4);
+  if (l >= 31) {
+    memcpy(out, in + 13, n * 4);
+    return;
+  }
+  double pred = t0;
+  for (size_t k = 0; k < n; k++) {
+    int64_t p = add_pred ? x86_f2i(pred) : x86_f2i(t0 + (double)t1 * (double)k);
+    pred += (double)t1;
+    if (l) {
+      const uint64_t f = get_field(in + 13, (uint64_t)k * l, l);
+      const int64_t mag = (int64_t)(f & ((1ull << (l - 1)) - 1));
+      p = ((f >> (l - 1)) & 1) ? p + mag : p - mag;
+    }
+    out[k] = (uint32_t)p;
+  }
+}
+
+/* piecewise_fix_op_max::randomdecodeArray8 (:160-186) with read_bit_fix_T
+ * (bit_read.h:1107-1133) / read_bit_default (:61-74). */
+uint32_t oracle_legacy_random(const uint8_t *in, int k) {
+  const unsigned l = in[0];
+  double t0;
+  float t1;
+  memcpy(&t0, in + 1, 8);
+  memcpy(&t1, in + 9, 4);
+  if (l >= 31) {
+    uint32_t v;
+    memcpy(&v, in + 13 + 4 * (size_t)k, 4);
+    return v;
+  }
+  const int64_t p = x86_f2i(t0 + (double)k * (double)t1);
+  if (!l) return (uint32_t)p;
+  const uint64_t f = get_field(in + 13, (uint64_t)k * l, l);
+  const int64_t mag = (int64_t)(f & ((1ull << (l - 1)) - 1));
+  return (uint32_t)(((f >> (l - 1)) & 1) ? p + mag : p - mag);
+}

@@ -99,6 +99,12 @@ class Oracle:
         L.oracle_close_window_start.restype = None
         L.oracle_close_window_start.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                                 ctypes.c_int, _P, _P]
+        L.oracle_legacy_encode.restype = _SZ
+        L.oracle_legacy_encode.argtypes = [_P, _SZ, _P, _P, _P]
+        L.oracle_legacy_decode.restype = None
+        L.oracle_legacy_decode.argtypes = [_P, _SZ, _P, ctypes.c_int]
+        L.oracle_legacy_random.restype = ctypes.c_uint32
+        L.oracle_legacy_random.argtypes = [_P, ctypes.c_int]
         L.oracle_column_zonemap.restype = None
         L.oracle_column_zonemap.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, _SZ, ctypes.c_uint32, _P, _P, _P]
         L.oracle_column_filter.restype = _SZ
@@ -161,6 +167,25 @@ class Oracle:
         out = np.zeros(len(idx), _dtype(s))
         self.L.oracle_column_random(codec, _ptr(pay), _ptr(offsets), s, bs, _ptr(idx), len(idx), _ptr(out))
         return out
+
+    # -- legacy u32 format (piecewise_fix_op_max) ---------------------------
+    def legacy_encode_block(self, data: np.ndarray):
+        """(image bytes, diff_plus bool[n], diff_minus bool[n])."""
+        data = np.ascontiguousarray(data, np.uint32)
+        out = np.zeros(len(data) * 4 + 64, np.uint8)
+        dp, dm = np.zeros(len(data), np.uint8), np.zeros(len(data), np.uint8)
+        nb = self.L.oracle_legacy_encode(_ptr(data), len(data), _ptr(out), _ptr(dp), _ptr(dm))
+        return out[:nb].tobytes(), dp.astype(bool), dm.astype(bool)
+
+    def legacy_decode_block(self, block: bytes, n: int, add_pred: bool = False) -> np.ndarray:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        out = np.zeros(max(n, 1), np.uint32)
+        self.L.oracle_legacy_decode(_ptr(buf), n, _ptr(out), int(add_pred))
+        return out[:n]
+
+    def legacy_random(self, block: bytes, k: int) -> int:
+        buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
+        return int(self.L.oracle_legacy_random(_ptr(buf), k))
 
     # -- predicate pushdown ------------------------------------------------
     def zonemap(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int):
@@ -262,6 +287,12 @@ class Reference:
         L.ref_varlen_random.argtypes = [_P, _P, _SZ, _P]
         L.ref_varlen_free.restype = None
         L.ref_varlen_free.argtypes = [_P]
+        L.ref_legacy_encode_block.restype = _SZ
+        L.ref_legacy_encode_block.argtypes = [_P, _SZ, _P, _P, _P]
+        L.ref_legacy_decode_block.restype = None
+        L.ref_legacy_decode_block.argtypes = [_P, _SZ, _P]
+        L.ref_legacy_random.restype = ctypes.c_uint32
+        L.ref_legacy_random.argtypes = [_P, ctypes.c_int]
         for t, ct in (("u32", ctypes.c_uint32), ("u64", ctypes.c_uint64)):
             f = getattr(L, f"ref_column_filter_{t}"); f.restype = _SZ
             f.argtypes = [ctypes.c_int, _P, _P, _SZ, ctypes.c_uint32, ct, _P, _P]
@@ -316,6 +347,24 @@ class Reference:
         out = np.zeros(len(idx), _dtype(s))
         getattr(self.L, f"ref_column_random_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), bs, _ptr(idx), len(idx), _ptr(out), threads)
         return out
+
+    # -- legacy u32 format (piecewise_fix_op_max) ---------------------------
+    def legacy_encode_block(self, data: np.ndarray):
+        data = np.ascontiguousarray(data, np.uint32)
+        out = np.zeros(len(data) * 4 + 1000, np.uint8)
+        dp, dm = np.zeros(len(data), np.uint8), np.zeros(len(data), np.uint8)
+        nb = self.L.ref_legacy_encode_block(_ptr(data), len(data), _ptr(out), _ptr(dp), _ptr(dm))
+        return out[:nb].tobytes(), dp.astype(bool), dm.astype(bool)
+
+    def legacy_decode_block(self, block: bytes, n: int) -> np.ndarray:
+        buf = np.frombuffer(block + b"\0" * 64, np.uint8).copy()
+        out = np.zeros(n + 64, np.uint32)
+        self.L.ref_legacy_decode_block(_ptr(buf), n, _ptr(out))
+        return out[:n]
+
+    def legacy_random(self, block: bytes, k: int) -> int:
+        buf = np.frombuffer(block + b"\0" * 64, np.uint8).copy()
+        return int(self.L.ref_legacy_random(_ptr(buf), k))
 
     # -- predicate pushdown (the filter experiments' loops) -----------------
     def filter_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int,

@@ -282,3 +282,26 @@ size_t ref_block_filter_close_u64(int codec, const uint8_t *in, size_t len, uint
 void ref_close_window_start_u32(uint32_t lo, uint32_t f1, uint32_t f2, uint32_t base, uint32_t *a, uint32_t *b) { window_start<uint32_t>(lo, f1, f2, base, a, b); }
 void ref_close_window_start_u64(uint64_t lo, uint64_t f1, uint64_t f2, uint64_t base, uint64_t *a, uint64_t *b) { window_start<uint64_t>(lo, f1, f2, base, a, b); }
 }  // extern "C"
+
+// ---- legacy u32 codec piecewise_fix_op_max (piecewise_fix_op_minimize_maxerror.h) ----
+#include "piecewise_fix_op_minimize_maxerror.h"
+extern "C" {
+// encodeArray8 on one block; diff_plus/diff_minus (n bytes, nullable) get the block's
+// mul_add_diff_set / mul_add_diff_set_minus membership.  Returns bytes written.
+size_t ref_legacy_encode_block(const uint32_t *in, size_t n, uint8_t *out, uint8_t *diff_plus, uint8_t *diff_minus) {
+  piecewise_fix_op_max c;
+  c.init(1, (int)n, 0);
+  uint8_t *end = c.encodeArray8(const_cast<uint32_t *>(in), n, out, 0);
+  if (diff_plus) for (int i : c.mul_add_diff_set) diff_plus[i] = 1;
+  if (diff_minus) for (int i : c.mul_add_diff_set_minus) diff_minus[i] = 1;
+  return (size_t)(end - out);
+}
+void ref_legacy_decode_block(const uint8_t *in, size_t n, uint32_t *out) {
+  piecewise_fix_op_max c;
+  c.decodeArray8(const_cast<uint8_t *>(in), n, out, 0);
+}
+uint32_t ref_legacy_random(const uint8_t *in, int k) {
+  piecewise_fix_op_max c;
+  return c.randomdecodeArray8(const_cast<uint8_t *>(in), (size_t)k, nullptr, 0);
+}
+}  // extern "C"
