@@ -42,7 +42,12 @@ enum leco_codec {
   LECO_CODEC_FOR = 1,    /* FOR_int<T>: frame of reference, unsigned offsets        */
   LECO_CODEC_DELTA = 2,  /* Delta_int<T>: signed first differences                  */
   LECO_CODEC_POLY2 = 3,  /* Leco_int_poly<T,2>: degree-2 normal-equation fit        */
-  LECO_CODEC_VARLEN = 4  /* Leco_cost_merge_double_wo_round<uint64_t> segments      */
+  LECO_CODEC_VARLEN = 4, /* Leco_cost_merge_double_wo_round<uint64_t> segments      */
+  LECO_CODEC_LINEAR_F32 = 5 /* piecewise_fix_op_max (u32 only, legacy): f32 slope,
+                               13-byte header, raw u32 body when l >= 31
+                               (piecewise_fix_op_minimize_maxerror.h:45-186).  Read
+                               side only: decode, random access, sum, directory,
+                               zone map, validation; encode with the reference. */
 };
 
 /* Value type = bytes per value. */

@@ -143,6 +143,36 @@ class FOR_int : public LecoBlockCodec<T, LECO_CODEC_FOR> {};
 template <typename T>
 class Delta_int : public LecoBlockCodec<T, LECO_CODEC_DELTA> {};
 
+// The reference's legacy u32 codec (piecewise_fix_op_minimize_maxerror.h:20-186), read side.
+// decodeArray8 returns the stored values: the reference's own bulk decoder accumulates the
+// prediction by addition and its drivers then correct it with the encoder's difference lists
+// (experiments/fix_int.cpp:110-117), which this decoder does not need.  Encode with the reference.
+class piecewise_fix_op_max {
+ public:
+  std::vector<int> mul_add_diff_set, mul_add_diff_set_minus;  // always empty: nothing to correct
+  int block_num = 0;
+  int block_size = 0;
+  void init(int blocks, int blocksize, int /*extra*/) {
+    block_num = blocks;
+    block_size = blocksize;
+  }
+  uint8_t *encodeArray8(uint32_t *, const size_t, uint8_t *, size_t) {
+    throw std::runtime_error("piecewise_fix_op_max::encodeArray8: this library reads the legacy format only");
+  }
+  uint32_t *decodeArray8(uint8_t *in, const size_t length, uint32_t *out, size_t /*nvalue*/) {
+    const uint64_t bytes = leco_block_bytes(LECO_CODEC_LINEAR_F32, LECO_U32, in[0], (uint32_t)length);
+    leco_detail::check(leco_block_decode(LECO_CODEC_LINEAR_F32, LECO_U32, in, bytes, (uint32_t)length, out), "decodeArray8");
+    return out;
+  }
+  uint32_t randomdecodeArray8(uint8_t *in, const size_t l, uint32_t * /*out*/, size_t /*nvalue*/) {
+    const uint32_t n = (uint32_t)l + 1;
+    const uint64_t bytes = leco_block_bytes(LECO_CODEC_LINEAR_F32, LECO_U32, in[0], n);
+    uint32_t v = 0;
+    leco_detail::check(leco_block_random(LECO_CODEC_LINEAR_F32, LECO_U32, in, bytes, n, (uint32_t)l, &v), "randomdecodeArray8");
+    return v;
+  }
+};
+
 template <typename T, int degree>
 class Leco_int_poly : public LecoBlockCodec<T, LECO_CODEC_POLY2> {
   static_assert(degree == 2, "the B200 codec provides the degree-2 polynomial model");

@@ -27,7 +27,7 @@ import numpy as np
 
 from . import build as _build
 
-LINEAR, FOR, DELTA, POLY2, VARLEN = 0, 1, 2, 3, 4
+LINEAR, FOR, DELTA, POLY2, VARLEN, LINEAR_F32 = 0, 1, 2, 3, 4, 5
 U32, U64 = 4, 8
 FIT_REFERENCE, FIT_EXACT = 0, 1
 PAYLOAD_SLACK = 64
@@ -264,6 +264,37 @@ class FOR_int(_FilterCodec):
 class Delta_int(_BlockCodec):
     """Mirror of ``Codecset::Delta_int<T>`` (delta_integer_template.h:14-158)."""
     CODEC = DELTA
+
+
+class piecewise_fix_op_max:
+    """Mirror of the reference's legacy u32 codec ``Codecset::piecewise_fix_op_max``
+    (piecewise_fix_op_minimize_maxerror.h:20-186), read side: ``decodeArray8``
+    returns the stored values (the reference's own bulk decoder accumulates the
+    prediction by addition and its drivers correct the difference afterwards,
+    experiments/fix_int.cpp:110-117); ``randomdecodeArray8`` is the reference's.
+    Encoding stays with the reference."""
+
+    CODEC = LINEAR_F32
+
+    def init(self, blocks: int, blocksize: int, extra: int = 0) -> None:
+        self.block_num, self.block_size = blocks, blocksize
+
+    def decodeArray8(self, in_, length: int, out: Optional[np.ndarray] = None, nvalue: int = 0) -> np.ndarray:
+        buf = np.frombuffer(bytes(in_), np.uint8).copy()
+        o = np.zeros(length, np.uint32)
+        _check(lib().leco_block_decode(LINEAR_F32, 4, _np_ptr(buf), len(buf), length, _np_ptr(o)), "decodeArray8")
+        if out is None:
+            return o
+        out[:length] = o
+        return out
+
+    def randomdecodeArray8(self, in_, l: int, out=None, nvalue: int = 0, length: Optional[int] = None) -> int:
+        buf = np.frombuffer(bytes(in_), np.uint8).copy()
+        n = length if length is not None else l + 1
+        nbytes = int(lib().leco_block_bytes(LINEAR_F32, 4, int(buf[0]), n))  # the image prefix that holds value l
+        v = np.zeros(1, np.uint32)
+        _check(lib().leco_block_random(LINEAR_F32, 4, _np_ptr(buf), nbytes, n, l, _np_ptr(v)), "randomdecodeArray8")
+        return int(v[0])
 
 
 class Leco_int_poly(_BlockCodec):

@@ -47,6 +47,8 @@ static int error_ptr(uint32_t **p) {
 int device_error_word(uint32_t **p) { return error_ptr(p); }
 
 static bool codec_ok(int codec) { return codec >= kLinear && codec <= kPoly2; }
+// Codecs the read side (decode, random access, sum, directory, zone map, validation) accepts.
+static bool codec_read_ok(int codec, int dtype) { return codec_ok(codec) || (codec == kLegacy && dtype == LECO_U32); }
 static bool dtype_ok(int dtype) { return dtype == LECO_U32 || dtype == LECO_U64; }
 
 void poly2_x_sums(uint32_t N, double X[5]) {
@@ -101,6 +103,7 @@ uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues) {
       case kFor: return block_bytes<kFor, 4>(l, nvalues);
       case kDelta: return block_bytes<kDelta, 4>(l, nvalues);
       case kPoly2: return block_bytes<kPoly2, 4>(l, nvalues);
+      case kLegacy: return block_bytes<kLegacy, 4>(l, nvalues);
     }
   } else if (dtype == LECO_U64) {
     switch (codec) {
@@ -167,7 +170,8 @@ int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t
 }
 
 static int check_column(const char *fn, int codec, int dtype, const void *payload, const void *offsets, uint32_t bs) {
-  if (!codec_ok(codec)) return fail(LECO_ERR_UNSUPPORTED, std::string(fn) + ": codec must be LINEAR, FOR, DELTA or POLY2");
+  if (!codec_read_ok(codec, dtype))
+    return fail(LECO_ERR_UNSUPPORTED, std::string(fn) + ": codec must be LINEAR, FOR, DELTA, POLY2 or LINEAR_F32 (u32)");
   if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, std::string(fn) + ": dtype must be LECO_U32 or LECO_U64");
   if (!bs || bs > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, std::string(fn) + ": block_size must be in 1..16384");
   if (!payload || !offsets) return fail(LECO_ERR_ARG, std::string(fn) + ": null pointer");
@@ -366,7 +370,7 @@ int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t 
     bool ok = o < e && e <= payload_bytes;
     if (ok) {
       const uint32_t l = h_payload[o];
-      bool sentinel = (l == 126 || l == 127) && codec != kFor;
+      bool sentinel = (l == 126 || l == 127) && codec != kFor && codec != kLegacy;
       if (sentinel) ok = e - o >= 1 + (uint64_t)dtype * (l == 127 ? 1 : 2);
       else ok = l <= tb && (e - o) == leco_block_bytes(codec, dtype, l, len);
       if (ok && codec == kFor && l > 0 && l < tb) {

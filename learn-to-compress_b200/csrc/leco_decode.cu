@@ -221,7 +221,7 @@ __global__ void build_dir_kernel(const uint8_t *payload, const uint64_t *offsets
   const BlockHdr h = parse_header<CODEC, S>(payload, __ldg(offsets + b));
   leco_dir_entry e;
   e.word0 = h.body_bit | ((uint64_t)h.l << 56) | ((uint64_t)CODEC << 48);
-  if (CODEC == kLinear || CODEC == kPoly2) {
+  if (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy) {
     e.a0 = h.a0; e.a1 = h.a1; e.a2 = h.a2;
   } else {
     e.a0 = __longlong_as_double((long long)h.base); e.a1 = 0; e.a2 = 0;
@@ -249,6 +249,7 @@ static bool staged_decode_enabled() {
         case kFor: FN<uint32_t, kFor>(__VA_ARGS__); return 0;               \
         case kDelta: FN<uint32_t, kDelta>(__VA_ARGS__); return 0;           \
         case kPoly2: FN<uint32_t, kPoly2>(__VA_ARGS__); return 0;           \
+        case kLegacy: FN<uint32_t, kLegacy>(__VA_ARGS__); return 0;         \
       }                                                                    \
     } else {                                                               \
       switch (codec) {                                                     \
@@ -271,7 +272,7 @@ static void run_decode(const DecodeLaunch &L, cudaStream_t st) {
   const uint64_t b0 = L.first / L.bs, b1 = (L.first + L.count - 1) / L.bs;
   const uint64_t nblk = b1 - b0 + 1;
   const bool staged = L.first == 0 && L.count == L.n && (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 &&
-                      CODEC != kDelta && nblk >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
+                      CODEC != kDelta && CODEC != kLegacy && nblk >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
   if (!staged) {
     if (L.bs <= kWarpBlock) decode_kernel_warp<T, CODEC><<<(unsigned)((nblk + 7) / 8), 256, 0, st>>>(L, nblk);
     else decode_kernel<T, CODEC><<<(unsigned)nblk, 256, 0, st>>>(L);

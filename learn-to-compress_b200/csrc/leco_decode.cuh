@@ -22,6 +22,13 @@ __device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ pay
   h.l = (uint32_t)(w0 & 0xff);
   h.a0 = h.a1 = h.a2 = 0;
   h.base = 0;
+  if (CODEC == kLegacy) {  // [u8 l][f64 theta0][f32 theta1][body]; l >= 31: u32 values (raw)
+    h.a0 = __longlong_as_double((long long)load_u64_at(words, off + 1));
+    h.a1 = (double)__uint_as_float((uint32_t)load_u64_at(words, off + 9));
+    h.body_bit = (off + 13) * 8;
+    if (h.l == 31) h.l = 32;  // raw: the 32-bit values follow the header
+    return h;
+  }
   if (h.l == 8u * S || h.l == 126 || h.l == 127) {
     h.body_bit = (off + 1) * 8;
     return h;
@@ -57,7 +64,7 @@ template <int CODEC, int S>
 __device__ __forceinline__ uint64_t value_from_field(const BlockHdr &h, uint32_t k, uint64_t f) {
   if (CODEC == kFor) return h.base + f;
   int64_t pred;
-  if (CODEC == kLinear) pred = f2i_x86(pred_linear(h.a0, h.a1, k));
+  if (CODEC == kLinear || CODEC == kLegacy) pred = f2i_x86(pred_linear(h.a0, h.a1, k));
   else pred = f2i_x86(pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k)));
   return h.l ? apply_signed((uint64_t)pred, f, h.l) : (uint64_t)pred;
 }
@@ -160,7 +167,7 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
       } else if (CODEC == kFor) {
         v[j] = h.base + f;
       } else {
-        const double pd = CODEC == kLinear ? pred_linear(h.a0, h.a1, kk)
+        const double pd = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, kk)
                                            : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
         const int64_t pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
         const uint32_t mag = f & m1;
@@ -202,7 +209,7 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   const uint64_t obase = base - a.first;  // out index of block value 0
 
   if (h.l == 126 || h.l == 127) {  // sentinel blocks (…_integer_template.h:152-170)
-    if (CODEC == kFor) { if (rank == 0) atomicOr(a.error, kErrBadHeader); return; }
+    if (CODEC == kFor || CODEC == kLegacy) { if (rank == 0) atomicOr(a.error, kErrBadHeader); return; }
     if (rank == 0) {
       const uint32_t cnt = h.l == 127 ? 1 : 2;
       for (uint32_t k = lo; k < cnt && k < hi; ++k)
@@ -279,7 +286,8 @@ __device__ __forceinline__ uint64_t ra_value(const BlockHdr &h, uint32_t k, uint
     return 0;
   }
   if (CODEC == kFor) return h.l ? h.base + f : h.base;
-  const double p = CODEC == kLinear ? pred_linear(h.a0, h.a1, k) : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
+  const double p = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, k)
+                                                        : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(k));
   if (h.l) return apply_signed((uint64_t)f2i_x86(p), f, h.l);
   return f2T_x86<S>(p);  // l == 0: (T)prediction directly (piecewise_fix_integer_template.h:334, poly :288)
 }

@@ -17,6 +17,9 @@ typedef unsigned __int128 u128;
 typedef __int128 i128;
 
 constexpr int kLinear = 0, kFor = 1, kDelta = 2, kPoly2 = 3, kVarlen = 4;
+// Legacy u32 codec piecewise_fix_op_max (piecewise_fix_op_minimize_maxerror.h:45-186):
+// [u8 l][f64 theta0][f32 theta1][body]; raw u32 values after the header when l >= 31.
+constexpr int kLegacy = 5;
 
 // Blocks of at most this many values are encoded/decoded by one warp (eight
 // per CTA) instead of a whole CTA.
@@ -128,13 +131,19 @@ __device__ __forceinline__ uint64_t apply_signed(uint64_t pred, uint64_t f, uint
 template <int CODEC, int S>
 struct Hdr {
   // bytes before the packed body
-  static constexpr uint32_t bytes = CODEC == kLinear ? 17u : CODEC == kFor ? 1u + 2u * S : CODEC == kDelta ? 1u + S : 25u;
+  static constexpr uint32_t bytes =
+      CODEC == kLinear ? 17u : CODEC == kFor ? 1u + 2u * S : CODEC == kDelta ? 1u + S : CODEC == kLegacy ? 13u : 25u;
 };
 
 // Byte size of a block image (headers/bit_write.h:257-323 pad 8-end%8; FOR
 // :326-390 pad (32-l)/8 for l <= 32, none above).
 template <int CODEC, int S>
 __host__ __device__ __forceinline__ uint64_t block_bytes(uint32_t l, uint32_t n) {
+  if (CODEC == kLegacy) {  // write_delta_T (bit_write.h:186-245) / write_delta_default (:395-410)
+    if (l == 0) return 13;
+    if (l >= 31) return 13ull + 4ull * n;
+    return 13ull + ((uint64_t)l * n + 7) / 8 + 1 + (32u - l) / 8u;
+  }
   if (l == 8u * S) return 1ull + (uint64_t)n * S;
   uint64_t h = CODEC == kLinear ? 17u : CODEC == kFor ? 1u + 2u * S : CODEC == kDelta ? 1u + S : 25u;
   if (l == 0) return h;

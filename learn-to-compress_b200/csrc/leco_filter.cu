@@ -593,6 +593,7 @@ int launch_zonemap(int codec, int s, const DecodeLaunch &L, uint64_t *zmin, uint
       case kFor: run_zonemap<uint32_t, kFor>(L, nb, zmin, zmax, st); return 0;
       case kDelta: run_zonemap<uint32_t, kDelta>(L, nb, zmin, zmax, st); return 0;
       case kPoly2: run_zonemap<uint32_t, kPoly2>(L, nb, zmin, zmax, st); return 0;
+      case kLegacy: run_zonemap<uint32_t, kLegacy>(L, nb, zmin, zmax, st); return 0;
     }
   } else {
     switch (codec) {
