@@ -452,23 +452,24 @@ __device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPl
 }
 
 // One warp per group of a.group consecutive blocks (at most 32).  A CTA takes
-// kFB groups by one ticket; its warps are then independent: lane j plans block
-// j of the group (all header, offset and zone-map loads of the group in flight
-// at once), the warp counts the blocks one after another, finds the group's
-// output offset by look-back (the CTA's earlier warps and earlier CTAs are all
-// resident or done, so every wait ends) and writes.
+// kFB groups by one ticket.  Lane j plans block j of its warp's group (all
+// header, offset and zone-map loads of the group in flight at once), the warp
+// counts its blocks one after another, the CTA finds its output offset by one
+// look-back over CTAs (earlier CTAs are resident or done, so every wait ends),
+// and every warp writes its blocks.
 template <int S, int CODEC>
 __global__ void __launch_bounds__(kFT, 3) filter_kernel(FilterLaunch a, int close) {
   extern __shared__ __align__(16) uint32_t fmask[];
   __shared__ uint32_t cta_ticket;
+  __shared__ uint64_t warp_tot[kFB], warp_excl[kFB];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *mask = fmask + (size_t)warp * a.group * a.mask_words;
   if (threadIdx.x == 0) cta_ticket = atomicAdd(a.ticket, 1u);
-  __syncthreads();  // the only CTA barrier: warps are independent from here on
+  __syncthreads();
   const uint64_t grp = (uint64_t)cta_ticket * kFB + warp;
   const uint64_t b0 = grp * a.group;
-  if (b0 >= a.nb) return;
-  const uint32_t nblk = (uint32_t)umin64(a.group, a.nb - b0);
+  // warps past the column still take part in the CTA's barriers, with no blocks
+  const uint32_t nblk = b0 < a.nb ? (uint32_t)umin64(a.group, a.nb - b0) : 0u;
 
   // ---- counting -----------------------------------------------------------------
   BlockPlan mine;
@@ -480,11 +481,28 @@ __global__ void __launch_bounds__(kFT, 3) filter_kernel(FilterLaunch a, int clos
     if (lane == j) mycnt = c;
   }
 
-  // ---- output offset by look-back -------------------------------------------------
+  // ---- output offset: the CTA's total by look-back over CTAs, then the warps' ------
+  // (one look-back per CTA: a per-warp look-back over all warps of a single wave
+  // walks back through ~warps/32 windows of aggregates, one L2 round trip each)
   const uint64_t tot = warp_sum_u64(mycnt);
-  const uint64_t excl = lookback_prefix(a.status, grp, tot, a.error);
+  if (lane == 0) warp_tot[warp] = tot;
+  __syncthreads();
+  if (warp == 0) {
+    const uint64_t wt = lane < kFB ? warp_tot[lane] : 0;
+    uint64_t inc = wt;
+    for (int d = 1; d < kFB; d <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= (uint32_t)d) inc += y;
+    }
+    const uint64_t cta_tot = __shfl_sync(0xffffffffu, inc, kFB - 1);
+    const uint64_t cexcl = lookback_prefix(a.status, cta_ticket, cta_tot, a.error);
+    if (lane < kFB) warp_excl[lane] = cexcl == ~0ull ? ~0ull : cexcl + inc - wt;
+    const uint64_t groups = (a.nb + a.group - 1) / a.group;
+    if (lane == 0 && cexcl != ~0ull && ((uint64_t)cta_ticket + 1) * kFB >= groups) *a.count = cexcl + cta_tot;
+  }
+  __syncthreads();
+  const uint64_t excl = warp_excl[warp];
   if (excl == ~0ull) return;  // a predecessor never published: error word set
-  if (b0 + nblk == a.nb && lane == 0) *a.count = excl + tot;
   if (!tot) return;
   uint64_t inc = mycnt;
   for (int d = 1; d < 32; d <<= 1) {
