@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint
       const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + base);
       const int32_t kstart = -(int32_t)((oaddr & 15) / S);
       const bool fast = (CODEC == kFor) || raw || pred_in_range<CODEC>(h, len);
+      if (!raw) mark_nonneg<CODEC>(h, len);
       if (fast) decode_narrow<T, CODEC, true, true>(h, raw, w32, out, base, 0, len, kstart);
       else decode_narrow<T, CODEC, false, true>(h, raw, w32, out, base, 0, len, kstart);
     }

@@ -12,7 +12,17 @@ struct BlockHdr {
   uint32_t l;         // field width; 8*S = raw; 126/127 = 2/1-value sentinels
   double a0, a1, a2;  // model
   uint64_t base;      // FOR minimum / Delta first value
+  bool nonneg = false;  // linear model: every prediction of the block lies in [0, 2^51)
 };
+
+// Sets h.nonneg for a linear block of len values: the predictions are monotone in
+// k, so the two ends bound them all.
+template <int CODEC>
+__device__ __forceinline__ void mark_nonneg(BlockHdr &h, uint32_t len) {
+  if (CODEC != kLinear && CODEC != kLegacy) return;
+  const double p0 = pred_linear(h.a0, h.a1, 0), p1 = pred_linear(h.a0, h.a1, len ? len - 1 : 0);
+  h.nonneg = p0 >= 0.0 && p1 >= 0.0 && p0 < 2251799813685248.0 && p1 < 2251799813685248.0;
+}
 
 template <int CODEC, int S>
 __device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ payload, uint64_t off) {
@@ -117,12 +127,18 @@ __device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restri
 template <typename T>
 __device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v, int cnt, bool full);
 template <>
-__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
+__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int cnt, bool full) {
+  if (full) {
+    __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
+    if (cnt > 2) __stcs(reinterpret_cast<ulonglong2 *>(out + o0 + 2), make_ulonglong2(v[2], v[3]));
+  }
 }
 template <>
-__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int, bool full) {
-  if (full) __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
+__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int cnt, bool full) {
+  if (full) {
+    __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
+    if (cnt > 4) __stcs(reinterpret_cast<uint4 *>(out + o0 + 4), make_uint4((uint32_t)v[4], (uint32_t)v[5], (uint32_t)v[6], (uint32_t)v[7]));
+  }
 }
 
 
@@ -145,7 +161,7 @@ template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256>
 __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32, T *out,
                                               uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
   constexpr int S = sizeof(T);
-  constexpr int VEC = 16 / S;
+  constexpr int VEC = 32 / S;  // two 16-byte stores per step
   const uint32_t l = raw ? 32u : h.l;
   // words32 + body_bit/32: the body's first word (global payload or a staged copy in shared memory)
   const uint32_t *bp = words32 + (h.body_bit >> 5);
@@ -167,9 +183,19 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
       } else if (CODEC == kFor) {
         v[j] = h.base + f;
       } else {
-        const double pd = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, kk)
-                                           : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
-        const int64_t pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
+        int64_t pred;
+        if (FAST && (CODEC == kLinear || CODEC == kLegacy) && h.nonneg) {
+          // Both conversions on the FP64 pipe instead of the conversion unit, exactly:
+          // (double)k = (2^52 + k) - 2^52, and for 0 <= p < 2^51 the round-toward-zero
+          // sum 2^52 + p is 2^52 + trunc(p), whose low mantissa bits are trunc(p).
+          const double kd = __dsub_rn(__hiloint2double(0x43300000, (int)kk), 4503599627370496.0);
+          const double pd = __dadd_rn(h.a0, __dmul_rn(h.a1, kd));
+          pred = __double_as_longlong(__dadd_rz(pd, 4503599627370496.0)) - 0x4330000000000000ll;
+        } else {
+          const double pd = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, kk)
+                                                                   : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
+          pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
+        }
         const uint32_t mag = f & m1;
         const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
         v[j] = (uint64_t)(pred + d);
@@ -205,7 +231,7 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   const uint32_t lo = (uint32_t)(r0 - base), hi = (uint32_t)(r1 - base);
   T *out = reinterpret_cast<T *>(a.out);
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
-  const BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+  BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
   const uint64_t obase = base - a.first;  // out index of block value 0
 
   if (h.l == 126 || h.l == 127) {  // sentinel blocks (…_integer_template.h:152-170)
@@ -245,6 +271,7 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
     // model keeps every prediction inside int64 (decided once per block).
     const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
     const uint32_t *w32 = reinterpret_cast<const uint32_t *>(a.payload);
+    if (!raw) mark_nonneg<CODEC>(h, len);
     if (fast) decode_narrow<T, CODEC, true, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
     else decode_narrow<T, CODEC, false, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
     return;
