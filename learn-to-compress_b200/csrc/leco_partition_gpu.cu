@@ -36,11 +36,18 @@ constexpr int kPartThreads = 128;
 constexpr int kPartHead = 0;
 constexpr int kPartTail = -2;
 
+// A segment of phase 1.  Its successor and bit class live apart, packed in one
+// 32-bit word per segment ((next + 2) << 8 | class; class 255 = the reference's
+// 10000 sentinel), because the per-class walks read only those: 4 bytes per step
+// instead of the whole record.
 struct PSeg {
-  int32_t start, end, prev, next;
+  int32_t start, end, prev, pad;
   int64_t max_delta, min_delta, next_delta;
-  int32_t ddn, pad;
 };
+constexpr uint32_t kNoClass = 255;
+__device__ __forceinline__ int lk_next(uint32_t w) { return (int)(w >> 8) - 2; }
+__device__ __forceinline__ uint32_t lk_class(uint32_t w) { return w & 0xffu; }
+__device__ __forceinline__ uint32_t lk_make(int next, uint32_t cls) { return ((uint32_t)(next + 2) << 8) | cls; }
 
 __device__ __forceinline__ uint32_t bits64_d(uint64_t v) { return v ? 64u - (uint32_t)__clzll((long long)v) : 0u; }
 
@@ -94,6 +101,7 @@ struct PartitionArgs {
   uint64_t nblocks;  // coarse blocks
   int overhead;      // merge penalty `delta` (bits)
   PSeg *segs;        // per slot: bs + 1 entries
+  uint32_t *links;   // per slot: bs + 1 packed (next, class) words
   uint32_t *pidx;    // per slot: bs entries (segment starts, phase 2)
   uint32_t *psz;     // per slot: bs entries (segment sizes, phase 2)
   uint32_t *stage;   // n entries: block b's starts at [b*bs, ...)
@@ -102,7 +110,7 @@ struct PartitionArgs {
 };
 
 // Segmentation of coarse block [B0, B0 + len) by one thread.
-__device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t len, PSeg *s, uint32_t *idx,
+__device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t len, PSeg *s, uint32_t *lk, uint32_t *idx,
                                   uint32_t *sz, uint32_t *out, uint32_t *count) {
   const uint64_t *array = a.array;
   if (len < 2) {  // the reference needs two points per coarse block (it reads array[B0 + 1])
@@ -112,7 +120,8 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
   }
   // ---- split: linked list of one-point segments (…:286-312) ----
   int ns = 0;
-  s[ns++] = PSeg{0, 0, -1, -1, 0, 0, 0, 10000, 0};  // head
+  s[ns] = PSeg{0, 0, -1, 0, 0, 0, 0};  // head
+  lk[ns++] = lk_make(-1, kNoClass);
   int min_sb = 10000, max_sb = -1;
   int64_t delta_prev = (int64_t)(__ldg(array + B0 + 1) - __ldg(array + B0));
   int cur = kPartHead;
@@ -121,27 +130,32 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
     const int sdb = cal_bits_d(delta_prev, delta);
     min_sb = min(min_sb, sdb);
     max_sb = max(max_sb, sdb);
-    s[ns] = PSeg{(int32_t)i - 1, (int32_t)i - 1, cur, -1, 0, 0, delta_prev, sdb, 0};
-    s[cur].next = ns;
+    s[ns] = PSeg{(int32_t)i - 1, (int32_t)i - 1, cur, 0, 0, 0, delta_prev};
+    lk[ns] = lk_make(-1, (uint32_t)sdb);
+    lk[cur] = lk_make(ns, lk_class(lk[cur]));
     cur = ns++;
     delta_prev = delta;
   }
-  s[ns] = PSeg{(int32_t)(B0 + len - 2), (int32_t)(B0 + len - 2), cur, kPartTail, 0, 0, delta_prev, 10000, 0};
-  s[cur].next = ns;
+  s[ns] = PSeg{(int32_t)(B0 + len - 2), (int32_t)(B0 + len - 2), cur, 0, 0, 0, delta_prev};
+  lk[ns] = lk_make(kPartTail, kNoClass);
+  lk[cur] = lk_make(ns, lk_class(lk[cur]));
   ns++;
   const int overhead = a.overhead;
 
   // ---- merge by bit class (…:326-433) ----
   for (int aim = min_sb; aim <= max_sb; aim++) {
-    int c = s[kPartHead].next;
-    while (c != kPartTail && s[c].next != kPartTail) {
-      if (s[c].ddn != aim) {
-        c = s[c].next;
+    int c = lk_next(lk[kPartHead]);
+    while (c != kPartTail) {
+      const uint32_t wc = lk[c];
+      int n = lk_next(wc);
+      if (n == kPartTail) break;
+      if ((int)lk_class(wc) != aim) {
+        c = n;
         continue;
       }
       PSeg sc = s[c];
-      int n = sc.next;
       const PSeg sn = s[n];
+      const uint32_t wn = lk[n];
       const int former = sc.start, start = sn.start, now = sn.end;
       const int lbo = cal_bits_d(sc.min_delta, sc.max_delta), rbo = cal_bits_d(sn.min_delta, sn.max_delta);
       const int64_t nmax = max(max(sc.max_delta, sn.max_delta), sc.next_delta);
@@ -150,16 +164,16 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
       const int origin_cost = (start - former) * lbo + (now - start + 1) * rbo;
       const int merged_cost = nb * (now - former + 1);
       if (!(merged_cost - origin_cost < overhead)) {
-        c = sc.next;
+        c = n;
         continue;
       }
+      int cnext = lk_next(wn);
+      uint32_t ccls = lk_class(wn);
       sc.end = now;
-      sc.next = sn.next;
-      if (sn.next != kPartTail) s[sn.next].prev = c;
+      if (cnext != kPartTail) s[cnext].prev = c;
       sc.next_delta = sn.next_delta;
       sc.max_delta = nmax;
       sc.min_delta = nmin;
-      sc.ddn = sn.ddn;
       // grow left (never into the first segment of the block)
       int p = sc.prev;
       while (p != kPartHead && s[p].prev != kPartHead) {
@@ -174,14 +188,16 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
         if (!(mc - oc < overhead)) break;
         sc.start = left;
         sc.prev = sp.prev;
-        s[sp.prev].next = c;
+        lk[sp.prev] = lk_make(c, lk_class(lk[sp.prev]));
         sc.min_delta = lmin;
         sc.max_delta = lmax;
         p = sc.prev;
       }
       // grow right (never into the last segment of the block)
-      n = sc.next;
-      while (n != kPartTail && s[n].next != kPartTail) {
+      n = cnext;
+      while (n != kPartTail) {
+        const uint32_t wr = lk[n];
+        if (lk_next(wr) == kPartTail) break;
         const PSeg sr = s[n];
         const int right = sr.end;
         const int64_t rmax = max(max(sr.max_delta, sc.max_delta), sc.next_delta);
@@ -192,22 +208,23 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
         const int mc = bnew * (right - sc.start + 1);
         if (!(mc - oc < overhead)) break;
         sc.end = right;
-        sc.next = sr.next;
-        if (sr.next != kPartTail) s[sr.next].prev = c;
+        cnext = lk_next(wr);
+        ccls = lk_class(wr);
+        s[cnext].prev = c;  // cnext is not the tail: the loop stops before the last segment
         sc.max_delta = rmax;
         sc.min_delta = rmin;
-        sc.ddn = sr.ddn;
         sc.next_delta = sr.next_delta;
-        n = sc.next;
+        n = cnext;
       }
       s[c] = sc;
-      c = sc.next;
+      lk[c] = lk_make(cnext, ccls);
+      c = cnext;
     }
   }
 
   // ---- size-driven pairwise merge passes (…:439-483, merge :516-570), in place ----
   uint32_t m = 0;
-  for (int c = s[kPartHead].next; c != kPartTail; c = s[c].next) idx[m++] = (uint32_t)s[c].start;
+  for (int c = lk_next(lk[kPartHead]); c != kPartTail; c = lk_next(lk[c])) idx[m++] = (uint32_t)s[c].start;
   const uint32_t endv = B0 + len;
   uint64_t total = 0;
   for (uint32_t i = 0; i < m; i++) {
@@ -259,13 +276,14 @@ __device__ void partition_block_d(const PartitionArgs &a, uint32_t B0, uint32_t 
 __global__ void __launch_bounds__(kPartThreads) partition_kernel(PartitionArgs a) {
   const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   PSeg *s = a.segs + slot * (a.bs + 1);
+  uint32_t *lk = a.links + slot * (a.bs + 1);
   uint32_t *idx = a.pidx + slot * a.bs, *sz = a.psz + slot * a.bs;
   for (;;) {
     const uint64_t b = atomicAdd(a.ticket, 1u);
     if (b >= a.nblocks) return;
     const uint64_t B0 = b * a.bs;
     const uint32_t len = (uint32_t)(b == a.nblocks - 1 ? a.n - B0 : a.bs);
-    partition_block_d(a, (uint32_t)B0, len, s, idx, sz, a.stage + B0, a.count + b);
+    partition_block_d(a, (uint32_t)B0, len, s, lk, idx, sz, a.stage + B0, a.count + b);
   }
 }
 
@@ -340,7 +358,8 @@ uint64_t leco_varlen_partition_workspace_bytes(uint64_t n, uint32_t coarse_block
   uint32_t bs;
   uint64_t nb, slots;
   part_layout(n, coarse_blocks, bs, nb, slots);
-  return align256(slots * (bs + 1) * sizeof(PSeg)) + 2 * align256(slots * bs * 4ull) + align256(n * 4) +
+  return align256(slots * (bs + 1) * sizeof(PSeg)) + align256(slots * (bs + 1) * 4ull) + 2 * align256(slots * bs * 4ull) +
+         align256(n * 4) +
          align256(nb * 4) + align256(nb * 8) + 256;
 }
 
@@ -350,6 +369,8 @@ int leco_varlen_partition_device(const uint64_t *d_values, uint64_t n, uint32_t 
   if (!d_values || !d_starts || !d_nseg || !coarse_blocks || n < 2)
     return record_error(LECO_ERR_ARG, "leco_varlen_partition_device: need values (n >= 2), starts and a block count");
   if (n > 0xffffffffull) return record_error(LECO_ERR_ARG, "leco_varlen_partition_device: segments start at 32-bit indices");
+  if (n / coarse_blocks >= (1ull << 24) - 4)
+    return record_error(LECO_ERR_ARG, "leco_varlen_partition_device: coarse blocks of at most 2^24 - 5 values");
   if (!d_ws || ws_bytes < leco_varlen_partition_workspace_bytes(n, coarse_blocks) || (reinterpret_cast<uintptr_t>(d_ws) & 255))
     return record_error(LECO_ERR_ARG, "leco_varlen_partition_device: workspace must be leco_varlen_partition_workspace_bytes(), 256-byte aligned");
   uint32_t *err = nullptr;
@@ -367,6 +388,8 @@ int leco_varlen_partition_device(const uint64_t *d_values, uint64_t n, uint32_t 
   A.overhead = (int)delta;
   A.segs = reinterpret_cast<PSeg *>(w);
   w += align256(slots * (bs + 1) * sizeof(PSeg));
+  A.links = reinterpret_cast<uint32_t *>(w);
+  w += align256(slots * (bs + 1) * 4ull);
   A.pidx = reinterpret_cast<uint32_t *>(w);
   w += align256(slots * bs * 4ull);
   A.psz = reinterpret_cast<uint32_t *>(w);
