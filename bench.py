@@ -463,7 +463,7 @@ def run_varlen(args, world, rank, local):
         r["mlookups_s"] = round(RA_BATCH / (r["gather_ms_2^24"] / 1e3) / 1e6, 1)
         r["sum_gbs"] = round(8 * n / (r["sum_ms"] / 1e3) / 1e9, 1)
     if rank == 0:
-        line = {"metric": "variable-length and degree-2 LeCo on 500M u64: decode GB/s, random access, sum",
+        line = {"metric": f"variable-length and degree-2 LeCo on {n // 1_000_000}M u64: decode GB/s, random access, sum",
                 "value": res["varlen"]["decode_gbs"], "unit": "GB/s", "n_gpus": world, "steps": max(3, args.steps // 4),
                 "warmup": 1, "ms_per_step": res["varlen"]["decode_ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -560,7 +560,7 @@ def run_filter(args, world, rank, local):
         cpu = {"unavailable": str(e)}
     if rank == 0:
         head = res["range_q0.5"]
-        line = {"metric": "LeCo-fix predicate pushdown on 200M sorted u64 keys: filter_range Gvalues/s",
+        line = {"metric": f"LeCo-fix predicate pushdown on {n // 1_000_000}M sorted u64 keys: filter_range Gvalues/s",
                 "value": head["gvalues_s"], "unit": "Gvalues/s", "n_gpus": world, "steps": reps,
                 "warmup": max(3, args.warmup), "ms_per_step": head["ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u64", "data": "synthetic",
