@@ -19,9 +19,7 @@ struct BlockHdr {
 // k, so the two ends bound them all.
 template <int CODEC>
 __device__ __forceinline__ void mark_nonneg(BlockHdr &h, uint32_t len) {
-  if (CODEC != kLinear && CODEC != kLegacy) return;
-  const double p0 = pred_linear(h.a0, h.a1, 0), p1 = pred_linear(h.a0, h.a1, len ? len - 1 : 0);
-  h.nonneg = p0 >= 0.0 && p1 >= 0.0 && p0 < 2251799813685248.0 && p1 < 2251799813685248.0;
+  if (CODEC == kLinear || CODEC == kLegacy) h.nonneg = preds_nonneg(h.a0, h.a1, len);
 }
 
 template <int CODEC, int S>
@@ -185,12 +183,7 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
       } else {
         int64_t pred;
         if (FAST && (CODEC == kLinear || CODEC == kLegacy) && h.nonneg) {
-          // Both conversions on the FP64 pipe instead of the conversion unit, exactly:
-          // (double)k = (2^52 + k) - 2^52, and for 0 <= p < 2^51 the round-toward-zero
-          // sum 2^52 + p is 2^52 + trunc(p), whose low mantissa bits are trunc(p).
-          const double kd = __dsub_rn(__hiloint2double(0x43300000, (int)kk), 4503599627370496.0);
-          const double pd = __dadd_rn(h.a0, __dmul_rn(h.a1, kd));
-          pred = __double_as_longlong(__dadd_rz(pd, 4503599627370496.0)) - 0x4330000000000000ll;
+          pred = trunc_nonneg_fp64(pred_linear_fp64(h.a0, h.a1, kk));  // no conversion-unit work
         } else {
           const double pd = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, kk)
                                                                    : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));

@@ -86,6 +86,26 @@ __device__ __forceinline__ double u128_to_double(u128 x) {
 __device__ __forceinline__ double pred_linear(double t0, double t1, uint32_t k) {
   return __dadd_rn(t0, __dmul_rn(t1, __uint2double_rn(k)));
 }
+
+// The same two conversions on the FP64 pipe instead of the conversion unit, exactly:
+// (double)k = (2^52 + k) - 2^52 for any 32-bit k, and for 0 <= p < 2^51 the
+// round-toward-zero sum 2^52 + p is 2^52 + trunc(p), whose low mantissa bits are
+// trunc(p).  pred_linear_fp64 equals pred_linear bit for bit.
+__device__ __forceinline__ double u32_to_double_fp64(uint32_t k) {
+  return __dsub_rn(__hiloint2double(0x43300000, (int)k), 4503599627370496.0);
+}
+__device__ __forceinline__ double pred_linear_fp64(double t0, double t1, uint32_t k) {
+  return __dadd_rn(t0, __dmul_rn(t1, u32_to_double_fp64(k)));
+}
+__device__ __forceinline__ int64_t trunc_nonneg_fp64(double p) {
+  return __double_as_longlong(__dadd_rz(p, 4503599627370496.0)) - 0x4330000000000000ll;
+}
+// True when every linear prediction of k = 0..len-1 lies in [0, 2^51): they are
+// monotone in k, so the two ends bound them (NaN models fail the comparisons).
+__device__ __forceinline__ bool preds_nonneg(double t0, double t1, uint32_t len) {
+  const double p0 = pred_linear(t0, t1, 0), p1 = pred_linear(t0, t1, len ? len - 1 : 0);
+  return p0 >= 0.0 && p1 >= 0.0 && p0 < 2251799813685248.0 && p1 < 2251799813685248.0;
+}
 // andviane::Polynomial::operator() for degree 2 (Polynomial.tpp:17-28):
 // s = 0; xx = 1; for a in (a0,a1,a2): s = s + xx*a; xx = xx*x.
 __device__ __forceinline__ double pred_poly2(double a0, double a1, double a2, double x) {
