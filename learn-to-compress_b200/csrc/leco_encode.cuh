@@ -216,6 +216,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   uint64_t fbase = 0;             // FOR min / Delta first value
   uint32_t H = Hdr<CODEC, S>::bytes;
 
+  bool narrow_range = false;  // residuals before the midpoint shift span < 2^30
   if (CODEC == kLinear || CODEC == kPoly2) {
     // ---- fit -----------------------------------------------------------------
     if (a.seq_models) {
@@ -268,12 +269,38 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       group_reduce2<3, 4, G>(rmx, rmn, sm.red);
       dmax = (int64_t)(uint64_t)rmx;
       dmin = (int64_t)(uint64_t)rmn;
+      narrow_range = dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
       const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
       m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
     }
     // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
     uint64_t rmax = 0;
     const bool fast = model_in_range(m0, m1, CODEC == kPoly2 ? m2 : 0.0, len);
+    // u64 blocks whose predictions lie in [0, 2^51) (so the reference's unsigned
+    // comparison is the signed one) and whose residuals before the midpoint shift
+    // spanned less than 2^30: every residual after the shift is below 2^31 in
+    // magnitude, so its low 32 bits are the whole of it.  Predictions on the FP64
+    // pipe (exact), residual arithmetic in 32 bits.
+    const bool r32 = CODEC == kLinear && S == 8 && narrow_range && preds_nonneg(m0, m1, len);
+    if (r32) {
+      uint32_t rm32 = 0;
+      for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+        const uint32_t i = i0 + tid;
+        bool pos = false;
+        if (i < len) {
+          const uint64_t y = (uint64_t)sm.vals[i];
+          const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
+          const int32_t d = (int32_t)((uint32_t)y - (uint32_t)pred);
+          pos = d > 0;  // y > pred
+          const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
+          sm.vals[i] = (T)r;
+          rm32 = r > rm32 ? r : rm32;
+        }
+        const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+        if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+      }
+      rmax = rm32;
+    } else
     for (uint32_t i0 = 0; i0 < len; i0 += nt) {
       const uint32_t i = i0 + tid;
       bool pos = false;
