@@ -78,7 +78,7 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
     uint64_t v = kFlagIncl;  // lanes before block 0 read as "inclusive 0"
     uint32_t spins = 0, ns = 32;
     uint32_t incl;
-    int last;  // the farthest lane this round needs
+    int last;  // the farthest lane this window of predecessors needs
     for (;;) {
       if (idx >= 0) v = ld_relaxed(&status[idx]);
       incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
