@@ -45,9 +45,13 @@ enum leco_codec {
   LECO_CODEC_VARLEN = 4, /* Leco_cost_merge_double_wo_round<uint64_t> segments      */
   LECO_CODEC_LINEAR_F32 = 5 /* piecewise_fix_op_max (u32 only, legacy): f32 slope,
                                13-byte header, raw u32 body when l >= 31
-                               (piecewise_fix_op_minimize_maxerror.h:45-186).  Read
-                               side only: decode, random access, sum, directory,
-                               zone map, validation; encode with the reference. */
+                               (piecewise_fix_op_minimize_maxerror.h:45-186).
+                               Encode (leco_encode, leco_encode_host,
+                               leco_block_encode), decode, random access, sum,
+                               directory, zone map, validation.  The encoder's
+                               difference lists for the reference's additive bulk
+                               decoder are not produced: leco_decode returns the
+                               stored values directly. */
 };
 
 /* Value type = bytes per value. */
@@ -102,7 +106,8 @@ uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues);
 /* ---- column encode / decode / random access (device buffers) ---------- */
 
 /* Encodes n values (d_values, dtype) in blocks of block_size with `codec`
- * (LINEAR, FOR, DELTA, POLY2).  Writes the concatenated reference block images
+ * (LINEAR, FOR, DELTA, POLY2; LINEAR_F32 for u32, the loop of
+ * piecewise_fix_op_max::encodeArray8 in experiments/fix_int.cpp:70-80).  Writes the concatenated reference block images
  * to d_payload (capacity payload_cap bytes, see leco_max_payload_bytes),
  * d_offsets[nblocks+1] and, when d_dir != NULL, the directory (nblocks
  * entries).  Replaces the driver loop over <Codec>::encodeArray8_int

@@ -268,16 +268,29 @@ class Delta_int(_BlockCodec):
 
 class piecewise_fix_op_max:
     """Mirror of the reference's legacy u32 codec ``Codecset::piecewise_fix_op_max``
-    (piecewise_fix_op_minimize_maxerror.h:20-186), read side: ``decodeArray8``
-    returns the stored values (the reference's own bulk decoder accumulates the
-    prediction by addition and its drivers correct the difference afterwards,
-    experiments/fix_int.cpp:110-117); ``randomdecodeArray8`` is the reference's.
-    Encoding stays with the reference."""
+    (piecewise_fix_op_minimize_maxerror.h:20-186).  ``encodeArray8`` writes the
+    reference's block image (:45-119) and returns its byte count; the encoder's
+    difference lists (mul_add_diff_set, :79-84) are not kept, because
+    ``decodeArray8`` returns the stored values (the reference's own bulk decoder
+    accumulates the prediction by addition and its drivers correct the difference
+    with those lists afterwards, experiments/fix_int.cpp:110-117);
+    ``randomdecodeArray8`` is the reference's."""
 
     CODEC = LINEAR_F32
 
+    def __init__(self, fit_mode: int = FIT_REFERENCE):
+        self.fit_mode = fit_mode
+
     def init(self, blocks: int, blocksize: int, extra: int = 0) -> None:
         self.block_num, self.block_size = blocks, blocksize
+
+    def encodeArray8(self, in_, length: int, res: np.ndarray, nvalue: int = 0) -> int:
+        data = np.ascontiguousarray(np.asarray(in_, dtype=np.uint32)[:length])
+        tmp = np.zeros(int(lib().leco_block_bytes(LINEAR_F32, 4, 32, length)) + 64, np.uint8)
+        nbytes = _check(lib().leco_block_encode(LINEAR_F32, 4, _np_ptr(data), length, self.fit_mode, _np_ptr(tmp)),
+                        "encodeArray8")
+        res[:nbytes] = tmp[:nbytes]
+        return nbytes
 
     def decodeArray8(self, in_, length: int, out: Optional[np.ndarray] = None, nvalue: int = 0) -> np.ndarray:
         buf = np.frombuffer(bytes(in_), np.uint8).copy()

@@ -50,6 +50,8 @@ static bool codec_ok(int codec) { return codec >= kLinear && codec <= kPoly2; }
 // Codecs the read side (decode, random access, sum, directory, zone map, validation) accepts.
 static bool codec_read_ok(int codec, int dtype) { return codec_ok(codec) || (codec == kLegacy && dtype == LECO_U32); }
 static bool dtype_ok(int dtype) { return dtype == LECO_U32 || dtype == LECO_U64; }
+// Codecs the encoder writes: the four block codecs, and the legacy format for u32.
+static bool codec_write_ok(int codec, int dtype) { return codec_read_ok(codec, dtype); }
 
 void poly2_x_sums(uint32_t N, double X[5]) {
   for (int k = 0; k < 5; ++k) {
@@ -81,7 +83,7 @@ static EncWs enc_ws(uint64_t nb, bool seq) {
 // exact integer, so the exact in-kernel moments reproduce it bit for bit.
 static bool needs_seq_fit(int codec, int dtype, uint32_t bs, int fit_mode) {
   if (fit_mode != LECO_FIT_REFERENCE) return false;
-  if (codec == kLinear) return !(dtype == LECO_U32 && bs <= 2048);
+  if (codec == kLinear || codec == kLegacy) return !(dtype == LECO_U32 && bs <= 2048);
   return codec == kPoly2;
 }
 
@@ -117,7 +119,7 @@ uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues) {
 }
 
 uint64_t leco_max_payload_bytes(int codec, int dtype, uint64_t n, uint32_t block_size) {
-  if (!codec_ok(codec) || !dtype_ok(dtype) || !block_size) return 0;
+  if (!codec_write_ok(codec, dtype) || !dtype_ok(dtype) || !block_size) return 0;
   const uint64_t nb = leco_num_blocks(n, block_size);
   // Worst block: raw (1 + n*s) or the widest packed image; the packed image
   // with l = 8s-1 never exceeds raw + header + 16 bytes.
@@ -132,7 +134,8 @@ uint64_t leco_encode_workspace_bytes(int codec, int dtype, uint64_t n, uint32_t 
 int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
                 uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
                 void *d_workspace, uint64_t workspace_bytes, leco_stream_t stream) {
-  if (!codec_ok(codec)) return fail(LECO_ERR_UNSUPPORTED, "leco_encode: codec must be LINEAR, FOR, DELTA or POLY2");
+  if (!codec_write_ok(codec, dtype))
+    return fail(LECO_ERR_UNSUPPORTED, "leco_encode: codec must be LINEAR, FOR, DELTA, POLY2 or LINEAR_F32 (u32)");
   if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, "leco_encode: dtype must be LECO_U32 or LECO_U64");
   if (!block_size || block_size > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, "leco_encode: block_size must be in 1..16384");
   if (n == 0) return fail(LECO_ERR_ARG, "leco_encode: n must be > 0");
@@ -406,7 +409,7 @@ struct DevBuf {
 int leco_encode_host(int codec, int dtype, const void *h_values, uint64_t n, uint32_t block_size, int fit_mode,
                      uint8_t *h_payload, uint64_t payload_cap, uint64_t *h_offsets, uint64_t *out_bytes) {
   if (!h_values || !h_payload || !h_offsets) return fail(LECO_ERR_ARG, "leco_encode_host: null pointer");
-  if (!codec_ok(codec) || !dtype_ok(dtype) || !block_size || block_size > LECO_MAX_BLOCK || !n)
+  if (!codec_write_ok(codec, dtype) || !dtype_ok(dtype) || !block_size || block_size > LECO_MAX_BLOCK || !n)
     return fail(LECO_ERR_ARG, "leco_encode_host: bad codec/dtype/block_size/n");
   cudaStream_t st;
   LECO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));

@@ -133,9 +133,9 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
   a.seq_models = nullptr; a.status = L.status; a.ticket = L.ticket; a.error = L.error;
   PolyX px;
   for (int i = 0; i < 10; ++i) a.polyX[i] = px.x[i] = L.polyX[i];
-  if (L.seq_models && (CODEC == kLinear || CODEC == kPoly2)) {
-    // four warps per CTA, 32 blocks per warp
-    seq_fit_tiled_kernel<T, CODEC><<<(unsigned)((L.nb + 127) / 128), 128, 0, st>>>(
+  if (L.seq_models && (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy)) {
+    // four warps per CTA, 32 blocks per warp (the legacy codec fits as LINEAR does)
+    seq_fit_tiled_kernel<T, CODEC == kLegacy ? kLinear : CODEC><<<(unsigned)((L.nb + 127) / 128), 128, 0, st>>>(
         reinterpret_cast<const T *>(L.values), L.n, L.bs, L.nb, px, L.seq_models);
     a.seq_models = L.seq_models;
   }
@@ -158,6 +158,7 @@ int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st) {
       case kFor: return launch_encode_t<uint32_t, kFor>(L, st);
       case kDelta: return launch_encode_t<uint32_t, kDelta>(L, st);
       case kPoly2: return launch_encode_t<uint32_t, kPoly2>(L, st);
+      case kLegacy: return launch_encode_t<uint32_t, kLegacy>(L, st);
     }
   } else {
     switch (codec) {

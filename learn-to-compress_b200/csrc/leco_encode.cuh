@@ -183,6 +183,51 @@ __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uin
   }
 }
 
+// Legacy u32 format, piecewise_fix_op_max::encodeArray8
+// (piecewise_fix_op_minimize_maxerror.h:45-95): the slope is rounded to float,
+// residuals are ints against (long long)(theta0 + theta1*i), the midpoint shift
+// is taken in int arithmetic, and the width is bits(max |r|) + 1 where a
+// residual of -2^31 does not count (the reference's abs() leaves it negative).
+// On return vals holds |r| (2^31 for -2^31), signs the bits r > 0, m1 the
+// float slope as a double; returns the width.
+template <int G, typename T>
+__device__ __forceinline__ uint32_t legacy_residuals(const EncSmem<T> &sm, double &m0, double &m1, uint32_t len,
+                                                     uint32_t tid, uint32_t nt) {
+  m1 = (double)__double2float_rn(m1);
+  bool fast = model_in_range(m0, m1, 0.0, len);
+  auto resid = [&](uint32_t i) -> int32_t {
+    const double p = pred_linear(m0, m1, i);
+    return (int32_t)((int64_t)(uint64_t)sm.vals[i] - (fast ? __double2ll_rz(p) : f2i_x86(p)));
+  };
+  int32_t dmax = INT32_MIN, dmin = INT32_MAX;
+  for (uint32_t i = tid; i < len; i += nt) {
+    const int32_t d = resid(i);
+    dmax = d > dmax ? d : dmax;
+    dmin = d < dmin ? d : dmin;
+  }
+  u128 rmx = (u128)(uint64_t)(int64_t)dmax, rmn = (u128)(uint64_t)(int64_t)dmin;
+  group_reduce2<3, 4, G>(rmx, rmn, sm.red);
+  const int32_t mid = (int32_t)((uint32_t)(uint64_t)rmx + (uint32_t)(uint64_t)rmn);
+  m0 = __dadd_rn(m0, __ddiv_rn(__int2double_rn(mid), 2.0));
+  fast = model_in_range(m0, m1, 0.0, len);
+  uint32_t emax = 0;
+  for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+    const uint32_t i = i0 + tid;
+    bool pos = false;
+    if (i < len) {
+      const int32_t d = resid(i);
+      pos = d > 0;
+      const uint32_t mag = d < 0 ? 0u - (uint32_t)d : (uint32_t)d;
+      sm.vals[i] = (T)mag;
+      if (d != INT32_MIN && mag > emax) emax = mag;
+    }
+    const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+    if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+  }
+  emax = (uint32_t)(uint64_t)group_reduce<1, G>((u128)emax, sm.red);
+  return emax ? bits_of(emax) + 1 : 0;
+}
+
 // Encodes block b of the column described by `a` with one thread group: the
 // whole CTA (G = 256) or one warp (G = 32, for small blocks).  The caller
 // guarantees that every block of the column with a smaller index was handed
@@ -217,7 +262,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   uint32_t H = Hdr<CODEC, S>::bytes;
 
   bool narrow_range = false;  // residuals before the midpoint shift span < 2^30
-  if (CODEC == kLinear || CODEC == kPoly2) {
+  if (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy) {
     // ---- fit -----------------------------------------------------------------
     if (a.seq_models) {
       m0 = a.seq_models[b * 3 + 0];
@@ -234,8 +279,8 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       group_reduce2<0, 0, G>(sy, siy, sm.red);
       if (CODEC == kPoly2) sqy = group_reduce<0, G>(sqy, sm.red);
       const double md = __uint2double_rn(len);
-      if (CODEC == kLinear) {
-        // lr_int_T::caltheta (lr.h:79-83) on exact moments
+      if (CODEC == kLinear || CODEC == kLegacy) {
+        // lr_int_T::caltheta (lr.h:79-83; lr_int, lr.h:89-111, is the same) on exact moments
         const uint64_t m = len;
         const double sumx = __ull2double_rn(m * (m - 1) / 2);
         const double sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
@@ -254,80 +299,84 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         m2 = c[2];
       }
     }
-    if (CODEC == kLinear) {
-      // ---- midpoint shift (piecewise_fix_integer_template.h:36-46) -----------
-      int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
-      const bool fast = model_in_range(m0, m1, 0.0, len);
-      for (uint32_t i = tid; i < len; i += nt) {
-        const double p = pred_linear(m0, m1, i);
-        const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
-        int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)pr);
-        dmax = d > dmax ? d : dmax;
-        dmin = d < dmin ? d : dmin;
+    if (CODEC == kLegacy) {
+      l = legacy_residuals<G>(sm, m0, m1, len, tid, nt);
+    } else {
+      if (CODEC == kLinear) {
+        // ---- midpoint shift (piecewise_fix_integer_template.h:36-46) -----------
+        int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
+        const bool fast = model_in_range(m0, m1, 0.0, len);
+        for (uint32_t i = tid; i < len; i += nt) {
+          const double p = pred_linear(m0, m1, i);
+          const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
+          int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)pr);
+          dmax = d > dmax ? d : dmax;
+          dmin = d < dmin ? d : dmin;
+        }
+        u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
+        group_reduce2<3, 4, G>(rmx, rmn, sm.red);
+        dmax = (int64_t)(uint64_t)rmx;
+        dmin = (int64_t)(uint64_t)rmn;
+        narrow_range = dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
+        const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
+        m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
       }
-      u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
-      group_reduce2<3, 4, G>(rmx, rmn, sm.red);
-      dmax = (int64_t)(uint64_t)rmx;
-      dmin = (int64_t)(uint64_t)rmn;
-      narrow_range = dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
-      const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
-      m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
-    }
-    // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
-    uint64_t rmax = 0;
-    const bool fast = model_in_range(m0, m1, CODEC == kPoly2 ? m2 : 0.0, len);
-    // u64 blocks whose predictions lie in [0, 2^51) (so the reference's unsigned
-    // comparison is the signed one) and whose residuals before the midpoint shift
-    // spanned less than 2^30: every residual after the shift is below 2^31 in
-    // magnitude, so its low 32 bits are the whole of it.  Predictions on the FP64
-    // pipe (exact), residual arithmetic in 32 bits.
-    const bool r32 = CODEC == kLinear && S == 8 && narrow_range && preds_nonneg(m0, m1, len);
-    if (r32) {
-      uint32_t rm32 = 0;
+      // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
+      uint64_t rmax = 0;
+      const bool fast = model_in_range(m0, m1, CODEC == kPoly2 ? m2 : 0.0, len);
+      // u64 blocks whose predictions lie in [0, 2^51) (so the reference's unsigned
+      // comparison is the signed one) and whose residuals before the midpoint shift
+      // spanned less than 2^30: every residual after the shift is below 2^31 in
+      // magnitude, so its low 32 bits are the whole of it.  Predictions on the FP64
+      // pipe (exact), residual arithmetic in 32 bits.
+      const bool r32 = CODEC == kLinear && S == 8 && narrow_range && preds_nonneg(m0, m1, len);
+      if (r32) {
+        uint32_t rm32 = 0;
+        for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+          const uint32_t i = i0 + tid;
+          bool pos = false;
+          if (i < len) {
+            const uint64_t y = (uint64_t)sm.vals[i];
+            const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
+            const int32_t d = (int32_t)((uint32_t)y - (uint32_t)pred);
+            pos = d > 0;  // y > pred
+            const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
+            sm.vals[i] = (T)r;
+            rm32 = r > rm32 ? r : rm32;
+          }
+          const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+          if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+        }
+        rmax = rm32;
+      } else
       for (uint32_t i0 = 0; i0 < len; i0 += nt) {
         const uint32_t i = i0 + tid;
         bool pos = false;
         if (i < len) {
           const uint64_t y = (uint64_t)sm.vals[i];
-          const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
-          const int32_t d = (int32_t)((uint32_t)y - (uint32_t)pred);
-          pos = d > 0;  // y > pred
-          const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
+          uint64_t r;
+          if (CODEC == kLinear) {
+            const double p = pred_linear(m0, m1, i);
+            const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+            pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
+            r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+          } else {
+            const double p = pred_poly2(m0, m1, m2, __uint2double_rn(i));
+            const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+            pos = (int64_t)y > pred;
+            r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+          }
+          r &= (S == 8 ? ~0ull : 0xffffffffull);
           sm.vals[i] = (T)r;
-          rm32 = r > rm32 ? r : rm32;
+          rmax = r > rmax ? r : rmax;
         }
         const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
         if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
       }
-      rmax = rm32;
-    } else
-    for (uint32_t i0 = 0; i0 < len; i0 += nt) {
-      const uint32_t i = i0 + tid;
-      bool pos = false;
-      if (i < len) {
-        const uint64_t y = (uint64_t)sm.vals[i];
-        uint64_t r;
-        if (CODEC == kLinear) {
-          const double p = pred_linear(m0, m1, i);
-          const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
-          pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
-          r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
-        } else {
-          const double p = pred_poly2(m0, m1, m2, __uint2double_rn(i));
-          const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
-          pos = (int64_t)y > pred;
-          r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
-        }
-        r &= (S == 8 ? ~0ull : 0xffffffffull);
-        sm.vals[i] = (T)r;
-        rmax = r > rmax ? r : rmax;
-      }
-      const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
-      if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+      rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
+      l = rmax ? bits_of(rmax) + 1 : 0;
+      if (l > TB) l = TB;
     }
-    rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
-    l = rmax ? bits_of(rmax) + 1 : 0;
-    if (l > TB) l = TB;
   } else if (CODEC == kFor) {
     // ---- frame of reference (FOR_integer_template.h:26-52) --------------------
     uint64_t mn = ~0ull, mx = 0;
@@ -359,8 +408,10 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   // treat l >= 8*sizeof(T)-1 as raw (piecewise_fix_integer_template.h:171,
   // FOR_integer_template.h:89, poly_fix_integer_template.h:121), so a packed
   // block of that width would not decode there.  Delta has no such rule.
-  if (CODEC != kDelta && l == TB - 1) l = TB;
-  const bool raw = (l == TB);
+  if (CODEC != kDelta && CODEC != kLegacy && l == TB - 1) l = TB;
+  // the legacy format stores widths of 31 and up as raw u32 values after its
+  // full header (piecewise_fix_op_minimize_maxerror.h:104-108)
+  const bool raw = CODEC == kLegacy ? l >= 31 : l == TB;
   if (raw) {  // residuals overwrote the values: restage them
     group_sync<G>();
     for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
@@ -375,7 +426,12 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   // ---- header bytes ------------------------------------------------------------
   if (tid == 0) {
     sm.hdr[0] = (uint8_t)l;
-    if (raw) {
+    if (CODEC == kLegacy) {  // [u8 l][f64 theta0][f32 theta1], raw blocks included
+      const uint64_t w0 = (uint64_t)__double_as_longlong(m0);
+      const uint32_t w1 = __float_as_uint(__double2float_rn(m1));
+      for (int j = 0; j < 8; ++j) sm.hdr[1 + j] = (uint8_t)(w0 >> (8 * j));
+      for (int j = 0; j < 4; ++j) sm.hdr[9 + j] = (uint8_t)(w1 >> (8 * j));
+    } else if (raw) {
       H = 1;
     } else if (CODEC == kLinear || CODEC == kPoly2) {
       uint64_t w0 = (uint64_t)__double_as_longlong(m0), w1 = (uint64_t)__double_as_longlong(m1),
@@ -397,7 +453,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   }
   group_sync<G>();
   const uint64_t goff = sm.bcast[1];
-  if (raw) H = 1;
+  if (raw && CODEC != kLegacy) H = 1;
   if (goff == ~0ull) return;                       // look-back gave up (error word set)
   if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {  // never write past the buffer
     if (tid == 0) atomicOr(a.error, kErrCapacity);
@@ -408,7 +464,13 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   const T *vals = sm.vals;
   const uint32_t *signs = sm.signs;
   if (raw) {
-    write_image(a.payload, goff, size, 1, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; }, tid, nt);
+    write_image(a.payload, goff, size, H, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; }, tid, nt);
+  } else if (CODEC == kLegacy) {  // write_delta_T (bit_write.h:186-245): |r| below the sign bit
+    const uint32_t sb = l ? l - 1 : 0;
+    const uint32_t mm = (1u << sb) - 1u;
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
+      return (uint64_t)(((uint32_t)vals[k] & mm) | (((signs[k >> 5] >> (k & 31)) & 1u) << sb));
+    }, tid, nt);
   } else if (CODEC == kLinear || CODEC == kPoly2) {
     const uint32_t sb = l ? l - 1 : 0;
     write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
@@ -436,8 +498,9 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
     if (a.dir) {
       leco_dir_entry e;
       uint64_t body_bit = (goff + H) * 8;
-      e.word0 = body_bit | ((uint64_t)l << 56) | ((uint64_t)CODEC << 48);
-      if (CODEC == kLinear || CODEC == kPoly2) {
+      const uint32_t dl = CODEC == kLegacy && raw ? 32u : l;  // as the decoder's directory records it
+      e.word0 = body_bit | ((uint64_t)dl << 56) | ((uint64_t)CODEC << 48);
+      if (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy) {
         e.a0 = m0; e.a1 = m1; e.a2 = m2;
       } else {
         e.a0 = __longlong_as_double((long long)fbase);

@@ -889,7 +889,8 @@ size_t oracle_legacy_encode(const uint32_t *in, size_t n, uint8_t *out, uint8_t 
     pred += (double)t1;
     const int32_t d = (int32_t)((int64_t)in[i] - pm);
     delta[i] = d;
-    const uint32_t a = d < 0 ? (uint32_t)(-(int64_t)d) : (uint32_t)d;
+    /* abs(INT_MIN) stays INT_MIN on x86 and fails the reference's `> max_error` */
+    const uint32_t a = d == INT32_MIN ? 0u : d < 0 ? (uint32_t)(-(int64_t)d) : (uint32_t)d;
     if (a > maxe) maxe = a;
   }
   const unsigned l = maxe ? (unsigned)oracle_bits(maxe) + 1 : 0;

@@ -47,6 +47,22 @@ def main():
             ks = np.unique(np.array([0, n - 1, n // 2, n // 3], dtype=np.int64))
             cases[key + "__ra_k"] = ks
             cases[key + "__ra_v"] = np.array([R.legacy_random(img, int(k)) for k in ks], np.uint32)
+    # palindromes of 0 and 2^32-1: slope 0, a residual of exactly -2^31 (the
+    # reference's abs() leaves it negative, so it does not count toward the width)
+    top = np.uint32(2 ** 32 - 1)
+    for n in (4, 64, 1000):
+        half = np.where(np.arange(n // 2) % 2 == 0, np.uint32(0), top).astype(np.uint32)
+        x = np.concatenate([half, half[::-1]])
+        img, dp, dm = R.legacy_encode_block(x)
+        key = f"legacy_n{n}_wrap"
+        cases[key + "__values"] = x
+        cases[key + "__image"] = np.frombuffer(img, np.uint8)
+        cases[key + "__decoded"] = R.legacy_decode_block(img, n)
+        cases[key + "__plus"] = np.nonzero(dp)[0].astype(np.int64)
+        cases[key + "__minus"] = np.nonzero(dm)[0].astype(np.int64)
+        ks = np.unique(np.array([0, n - 1, n // 2, n // 3], dtype=np.int64))
+        cases[key + "__ra_k"] = ks
+        cases[key + "__ra_v"] = np.array([R.legacy_random(img, int(k)) for k in ks], np.uint32)
     # a column of blocks of 4096 values (sorted keys with a slow drift: difference lists occur)
     n, bs = 200_003, 4096
     i = np.arange(n, dtype=np.float64)
