@@ -53,8 +53,10 @@ __device__ __forceinline__ EncSmem<T> enc_smem(uint8_t *base, uint32_t bs) {
   s.vals = reinterpret_cast<T *>(base + soff);
   return s;
 }
+// The value region holds round32(bs) values plus 16 bytes: the u64 LeCo path keeps
+// round32(bs) staged words and a packed body of up to round32(bs) + 4 words there.
 __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
-  return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + bs * s;
+  return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + (bs + 31) / 32 * 32 * s + 16;
 }
 
 // Decoupled look-back (single-pass prefix sum over per-block totals).  Run by
@@ -183,6 +185,268 @@ __device__ __forceinline__ void write_image(uint8_t *payload, uint64_t goff, uin
   }
 }
 
+// ---- u64 LeCo blocks: residual rows packed in shared memory ------------------------
+// Residual i of a row of 32 is kept at column (i ^ row) of its row, so that a warp
+// over 32 consecutive residuals and a warp over 32 rows (one residual each) both
+// touch 32 distinct banks.
+__device__ __forceinline__ uint32_t swz32(uint32_t i) { return i ^ ((i >> 5) & 31u); }
+
+// Packs rows t0, t0 + step, ... of 32 fields each (magnitude res[k] below the sign
+// bit l-1, sign bit k of signs[row]) into l 32-bit words per row: row t is body
+// words [t*l, t*l + l), the LSB-first field stream of write_delta_int_T
+// (bit_write.h:257-323).  Four zero words follow the last row (the image's pad).
+__device__ __forceinline__ void pack_rows(const uint32_t *res, const uint32_t *signs, uint32_t *pk, uint32_t len,
+                                          uint32_t l, uint32_t t0, uint32_t step) {
+  const uint32_t rows = (len + 31) / 32;
+  const uint32_t sb = l - 1;
+  for (uint32_t t = t0; t < rows; t += step) {
+    const uint32_t sg = signs[t], x = t & 31u;
+    uint32_t *out = pk + t * l;
+    uint64_t acc = 0;
+    uint32_t have = 0, q = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) {
+      const uint32_t f = t * 32 + j < len ? (res[t * 32 + (j ^ x)] | (((sg >> j) & 1u) << sb)) : 0u;
+      acc |= (uint64_t)f << have;
+      have += l;
+      if (have >= 32) {
+        out[q++] = (uint32_t)acc;
+        acc >>= 32;
+        have -= 32;
+      }
+    }
+  }
+  if (t0 == 0)
+    for (uint32_t j = 0; j < 4; ++j) pk[rows * l + j] = 0;
+}
+
+// Writes the image [goff, goff + size) whose body is packed in shared memory
+// (pk, at least size - H + 4 bytes readable): 16-byte chunks inside the body by
+// funnel shifts, the chunks shared with the header or a neighbouring block byte
+// by byte.
+__device__ __forceinline__ void write_image_packed(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
+                                                   const uint8_t *hdr, const uint32_t *pk, uint32_t rank,
+                                                   uint32_t nthreads) {
+  const uint64_t gend = goff + size;
+  const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
+  const uint64_t body0 = goff + H;
+  const uint8_t *pk8 = reinterpret_cast<const uint8_t *>(pk);
+  for (uint64_t c = c0 + rank; c < c1; c += nthreads) {
+    const uint64_t cb = c << 4;
+    if (cb >= body0 && cb + 16 <= gend) {
+      const uint32_t q = (uint32_t)(cb - body0), qw = q >> 2, sh = (q & 3u) * 8u;
+      const uint32_t w0 = pk[qw], w1 = pk[qw + 1], w2 = pk[qw + 2], w3 = pk[qw + 3], w4 = pk[qw + 4];
+      *reinterpret_cast<uint4 *>(payload + cb) = make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                                                            __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
+    } else {
+      for (int j = 0; j < 16; ++j) {
+        const uint64_t g = cb + j;
+        if (g < goff || g >= gend) continue;
+        const uint64_t i = g - goff;
+        payload[g] = i < H ? hdr[i] : pk8[i - H];
+      }
+    }
+  }
+}
+
+// Leco_int<uint64_t>::encodeArray8_int (piecewise_fix_integer_template.h:27-140)
+// for one block with a whole CTA, the same image as the generic encode_block:
+//  * the low 32 bits of each value are staged (row-swizzled) while the values
+//    stream in, and the midpoint pass (:36-46) runs on those same loads;
+//  * blocks whose residuals before the shift span < 2^30 and whose predictions lie
+//    in [0, 2^51) take their residuals in 32 bits from the staged words (every
+//    residual after the shift is below 2^31 in magnitude) and overwrite them;
+//    warps 4..7 pack the rows into the body while warp 0 runs the look-back;
+//  * other blocks (wide residuals, negative predictions, raw) recompute their
+//    residuals from the values in global memory, which are then L2-resident.
+// Shared memory: enc_smem_bytes(bs, 8) -- staged words and packed body take the
+// place of the generic encoder's staged values.
+template <int G>
+__device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
+  constexpr uint32_t TB = 64;
+  EncSmem<uint64_t> sm = enc_smem<uint64_t>(smem_raw, a.bs);
+  uint32_t *lo = reinterpret_cast<uint32_t *>(sm.vals);  // [round32(bs)] low words, then residuals
+  uint32_t *pk = lo + ((a.bs + 31u) & ~31u);              // packed body words
+  const uint32_t tid = group_rank<G>(), nt = group_size<G>();
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  const uint64_t *src = reinterpret_cast<const uint64_t *>(a.values) + base;
+
+  // ---- fit and midpoint shift -------------------------------------------------
+  double m0, m1;
+  auto mid_pass = [&](bool stage) -> bool {  // true: residuals before the shift span < 2^30
+    int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
+    const bool fast = model_in_range(m0, m1, 0.0, len);
+    auto visit = [&](uint64_t y, uint32_t i) {
+      if (stage) lo[swz32(i)] = (uint32_t)y;
+      const double p = pred_linear(m0, m1, i);
+      const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
+      const int64_t d = (int64_t)(y - (uint64_t)pr);
+      dmax = d > dmax ? d : dmax;
+      dmin = d < dmin ? d : dmin;
+    };
+    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, four in flight per thread
+      const uint32_t np = len / 2;
+#pragma unroll 4
+      for (uint32_t q = tid; q < np; q += nt) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+        visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+        visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+      }
+      if ((len & 1) && tid == 0) visit(__ldg(src + len - 1), len - 1);
+    } else {
+      for (uint32_t i = tid; i < len; i += nt) visit(__ldg(src + i), i);
+    }
+    u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
+    group_reduce2<3, 4, G>(rmx, rmn, sm.red);
+    dmax = (int64_t)(uint64_t)rmx;
+    dmin = (int64_t)(uint64_t)rmn;
+    const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
+    m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
+    return dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
+  };
+  bool narrow_range;
+  if (a.seq_models) {
+    m0 = a.seq_models[b * 3 + 0];
+    m1 = a.seq_models[b * 3 + 1];
+    narrow_range = mid_pass(true);
+  } else {
+    u128 sy = 0, siy = 0;
+    auto visit = [&](uint64_t y, uint32_t i) {
+      lo[swz32(i)] = (uint32_t)y;
+      sy += y;
+      siy += (u128)y * i;
+    };
+    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+      const uint32_t np = len / 2;
+#pragma unroll 2
+      for (uint32_t q = tid; q < np; q += nt) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+        visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+        visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+      }
+      if ((len & 1) && tid == 0) visit(__ldg(src + len - 1), len - 1);
+    } else {
+      for (uint32_t i = tid; i < len; i += nt) visit(__ldg(src + i), i);
+    }
+    group_reduce2<0, 0, G>(sy, siy, sm.red);
+    // lr_int_T::caltheta (lr.h:79-83) on exact moments
+    const double md = __uint2double_rn(len);
+    const uint64_t m = len;
+    const double sumx = __ull2double_rn(m * (m - 1) / 2);
+    const double sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
+    const double sumy = u128_to_double(sy), sumxy = u128_to_double(siy);
+    const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+    const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+    m1 = __ddiv_rn(ccc, xxx);
+    m0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(m1, sumx)), md);
+    narrow_range = mid_pass(false);
+  }
+
+  // ---- residuals (:51-72) and width (:108-117) ---------------------------------
+  const bool r32 = narrow_range && preds_nonneg(m0, m1, len);
+  const bool fast = model_in_range(m0, m1, 0.0, len);
+  auto resid = [&](uint32_t k, bool &pos) -> uint64_t {  // from global memory, as the generic encoder
+    const uint64_t y = __ldg(src + k);
+    const double p = pred_linear(m0, m1, k);
+    const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+    pos = y > (uint64_t)pred;
+    return pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+  };
+  uint32_t l;
+  if (r32) {
+    uint32_t rm32 = 0;
+    for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+      const uint32_t i = i0 + tid;
+      bool pos = false;
+      if (i < len) {
+        const uint32_t s = swz32(i);
+        const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
+        const int32_t d = (int32_t)(lo[s] - (uint32_t)pred);
+        pos = d > 0;  // y > pred
+        const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
+        lo[s] = r;
+        rm32 = r > rm32 ? r : rm32;
+      }
+      const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+      if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+    }
+    const uint64_t rmax = (uint64_t)group_reduce<1, G>((u128)rm32, sm.red);
+    l = rmax ? bits_of(rmax) + 1 : 0;
+  } else {
+    uint64_t rmax = 0;
+    for (uint32_t i = tid; i < len; i += nt) {
+      bool pos;
+      const uint64_t r = resid(i, pos);
+      rmax = r > rmax ? r : rmax;
+    }
+    rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
+    l = rmax ? bits_of(rmax) + 1 : 0;
+    if (l > TB) l = TB;
+  }
+  if (l == TB - 1) l = TB;  // written raw, as the generic encoder explains
+  const bool raw = l == TB;
+  const bool rows = r32 && l > 0;
+  const uint64_t size = block_bytes<kLinear, 8>(l, len);
+  const uint32_t H = raw ? 1u : 17u;
+
+  // ---- offset by look-back, packing alongside -----------------------------------
+  const bool split = rows && nt >= 256;
+  if (tid < 32) {
+    const uint64_t excl = lookback_prefix(a.status, b, size, a.error);
+    if (tid == 0) sm.bcast[1] = excl;
+  } else if (split && tid >= 128) {
+    pack_rows(lo, sm.signs, pk, len, l, tid - 128, nt - 128);
+  }
+  if (tid == 0) {
+    sm.hdr[0] = (uint8_t)l;
+    if (!raw) {
+      const uint64_t w0 = (uint64_t)__double_as_longlong(m0), w1 = (uint64_t)__double_as_longlong(m1);
+      for (int j = 0; j < 8; ++j) {
+        sm.hdr[1 + j] = (uint8_t)(w0 >> (8 * j));
+        sm.hdr[9 + j] = (uint8_t)(w1 >> (8 * j));
+      }
+    }
+  }
+  group_sync<G>();
+  if (rows && !split) {
+    pack_rows(lo, sm.signs, pk, len, l, tid, nt);
+    group_sync<G>();
+  }
+  const uint64_t goff = sm.bcast[1];
+  if (goff == ~0ull) return;                                  // look-back gave up (error word set)
+  if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {     // never write past the buffer
+    if (tid == 0) atomicOr(a.error, kErrCapacity);
+    return;
+  }
+
+  // ---- body ----------------------------------------------------------------------
+  if (raw) {
+    write_image(a.payload, goff, size, H, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return __ldg(src + k); }, tid, nt);
+  } else if (rows) {
+    write_image_packed(a.payload, goff, size, H, sm.hdr, pk, tid, nt);
+  } else {
+    const uint32_t sb = l ? l - 1 : 0;
+    write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
+      bool pos;
+      const uint64_t r = resid(k, pos);
+      return r | ((uint64_t)pos << sb);
+    }, tid, nt);
+  }
+
+  // ---- offsets and directory -------------------------------------------------------
+  if (tid == 0) {
+    a.offsets[b] = goff;
+    if (b == a.nb - 1) a.offsets[a.nb] = goff + size;
+    if (a.dir) {
+      leco_dir_entry e;
+      e.word0 = ((goff + H) * 8) | ((uint64_t)l << 56) | ((uint64_t)kLinear << 48);
+      e.a0 = m0; e.a1 = m1; e.a2 = 0.0;
+      a.dir[b] = e;
+    }
+  }
+}
+
 // Legacy u32 format, piecewise_fix_op_max::encodeArray8
 // (piecewise_fix_op_minimize_maxerror.h:45-95): the slope is rounded to float,
 // residuals are ints against (long long)(theta0 + theta1*i), the midpoint shift
@@ -236,6 +500,10 @@ __device__ __forceinline__ uint32_t legacy_residuals(const EncSmem<T> &sm, doubl
 // owned by this group.
 template <typename T, int CODEC, int G = 256>
 __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
+  if constexpr (CODEC == kLinear && sizeof(T) == 8 && G != 32) {
+    encode_block_l64<G>(a, b, smem_raw);
+    return;
+  }
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   EncSmem<T> sm = enc_smem<T>(smem_raw, a.bs);
