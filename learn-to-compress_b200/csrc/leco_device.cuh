@@ -310,6 +310,51 @@ __device__ __forceinline__ void group_reduce2(u128 &a, u128 &b, u128 *red) {
   b = group_reduce<OPB, 32>(b, red);
 }
 
+// Reductions over warps 1.. of a CTA while warp 0 runs something else (the
+// encoder's look-back): named barrier 1 over blockDim.x - 32 threads, which all
+// of warps 1.. must reach.  `red` as block_reduce2 (66 entries).  OP as
+// block_reduce.
+__device__ __forceinline__ void sub_sync() { asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x - 32) : "memory"); }
+template <int OP>
+__device__ __forceinline__ u128 warp_op(u128 x) {
+  switch (OP) {
+    case 0: return warp_sum_u128(x);
+    case 1: return warp_max_u64((uint64_t)x);
+    case 2: return warp_min_u64((uint64_t)x);
+    case 3: return (u128)(uint64_t)warp_max_i64((int64_t)(uint64_t)x);
+    case 4: return (u128)(uint64_t)warp_min_i64((int64_t)(uint64_t)x);
+    default: return warp_sum_u64((uint64_t)x);
+  }
+}
+template <int OP>
+__device__ __forceinline__ u128 op_identity() {
+  return OP == 2 ? (u128)~0ull : OP == 3 ? (u128)0x8000000000000000ull : OP == 4 ? (u128)0x7fffffffffffffffull : (u128)0;
+}
+template <int OPA, int OPB>
+__device__ __forceinline__ void sub_reduce2(u128 &a, u128 &b, u128 *red) {
+  const int lane = threadIdx.x & 31, warp = (int)(threadIdx.x >> 5) - 1, nw = (int)(blockDim.x >> 5) - 1;
+  a = warp_op<OPA>(a);
+  b = warp_op<OPB>(b);
+  sub_sync();  // `red` may still be read by a previous reduction
+  if (lane == 0) {
+    red[warp] = a;
+    red[33 + warp] = b;
+  }
+  sub_sync();
+  if (warp == 0) {
+    u128 x = lane < nw ? red[lane] : op_identity<OPA>(), y = lane < nw ? red[33 + lane] : op_identity<OPB>();
+    x = warp_op<OPA>(x);
+    y = warp_op<OPB>(y);
+    if (lane == 0) {
+      red[32] = x;
+      red[65] = y;
+    }
+  }
+  sub_sync();
+  a = red[32];
+  b = red[65];
+}
+
 // ---- relaxed global word access for the look-back scan ----------------------
 __device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p) {
   uint64_t v;

@@ -59,20 +59,18 @@ __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
   return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + (bs + 31) / 32 * 32 * s + 16;
 }
 
-// Decoupled look-back (single-pass prefix sum over per-block totals).  Run by
-// one full warp.  Publishes this block's total, then walks back over the
-// predecessors 32 at a time (lane i reads block j - i): it needs every block from
-// the nearest one down to the first with an inclusive prefix, and waits only
-// while one of those has published nothing.  Returns the exclusive prefix; on a
-// wait that exceeds the spin limit sets kErrTimeout and returns ~0.
-__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error,
-                                                    uint32_t spin_limit = kSpinLimit) {
+// Decoupled look-back (single-pass prefix sum over per-block totals), run by one
+// full warp.  lookback_excl walks back over the predecessors of block b 32 at a
+// time (lane i reads block j - i): it needs every block from the nearest one down
+// to the first with an inclusive prefix, and waits only while one of those has
+// published nothing.  It needs nothing of block b itself, so it can run while the
+// block is still being encoded.  Returns the exclusive prefix; on a wait that
+// exceeds the spin limit sets kErrTimeout and returns ~0.  lookback_prefix
+// publishes block b's total first and its inclusive prefix last.
+__device__ __forceinline__ uint64_t lookback_excl(const uint64_t *status, uint64_t b, uint32_t *error,
+                                                  uint32_t spin_limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
-  if (b == 0) {
-    if (lane == 0) st_relaxed(&status[0], kFlagIncl | my);
-    return 0;
-  }
-  if (lane == 0) st_relaxed(&status[b], kFlagAgg | my);
+  if (b == 0) return 0;
   uint64_t excl = 0;
   int64_t j = (int64_t)b - 1;
   for (;;) {
@@ -98,7 +96,14 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
     if (incl) break;
     j -= 32;
   }
-  if (lane == 0) st_relaxed(&status[b], kFlagIncl | (excl + my));
+  return excl;
+}
+__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b, uint64_t my, uint32_t *error,
+                                                    uint32_t spin_limit = kSpinLimit) {
+  const int lane = threadIdx.x & 31;
+  if (b > 0 && lane == 0) st_relaxed(&status[b], kFlagAgg | my);
+  const uint64_t excl = lookback_excl(status, b, error, spin_limit);
+  if (excl != ~0ull && lane == 0) st_relaxed(&status[b], kFlagIncl | (excl + my));
   return excl;
 }
 
@@ -251,171 +256,178 @@ __device__ __forceinline__ void write_image_packed(uint8_t *payload, uint64_t go
 
 // Leco_int<uint64_t>::encodeArray8_int (piecewise_fix_integer_template.h:27-140)
 // for one block with a whole CTA, the same image as the generic encode_block:
+//  * warp 0 takes the block's exclusive byte offset by look-back from the start,
+//    while warps 1.. encode (the offset needs nothing of the block itself); the
+//    block's total is published as soon as it is known, its inclusive prefix
+//    once both are;
 //  * the low 32 bits of each value are staged (row-swizzled) while the values
 //    stream in, and the midpoint pass (:36-46) runs on those same loads;
 //  * blocks whose residuals before the shift span < 2^30 and whose predictions lie
 //    in [0, 2^51) take their residuals in 32 bits from the staged words (every
-//    residual after the shift is below 2^31 in magnitude) and overwrite them;
-//    warps 4..7 pack the rows into the body while warp 0 runs the look-back;
+//    residual after the shift is below 2^31 in magnitude), overwrite them, and
+//    pack rows of 32 into the body in shared memory;
 //  * other blocks (wide residuals, negative predictions, raw) recompute their
 //    residuals from the values in global memory, which are then L2-resident.
-// Shared memory: enc_smem_bytes(bs, 8) -- staged words and packed body take the
-// place of the generic encoder's staged values.
+// Needs blockDim.x >= 64 (a multiple of 32).  Shared memory: enc_smem_bytes(bs, 8)
+// -- staged words and packed body take the place of the generic encoder's
+// staged values.
 template <int G>
 __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
   constexpr uint32_t TB = 64;
   EncSmem<uint64_t> sm = enc_smem<uint64_t>(smem_raw, a.bs);
   uint32_t *lo = reinterpret_cast<uint32_t *>(sm.vals);  // [round32(bs)] low words, then residuals
   uint32_t *pk = lo + ((a.bs + 31u) & ~31u);              // packed body words
-  const uint32_t tid = group_rank<G>(), nt = group_size<G>();
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
   const uint64_t base = b * a.bs;
   const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
   const uint64_t *src = reinterpret_cast<const uint64_t *>(a.values) + base;
+  double *model = reinterpret_cast<double *>(&sm.bcast[4]);  // m0, m1 for warp 0
 
-  // ---- fit and midpoint shift -------------------------------------------------
-  double m0, m1;
-  auto mid_pass = [&](bool stage) -> bool {  // true: residuals before the shift span < 2^30
-    int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
-    const bool fast = model_in_range(m0, m1, 0.0, len);
-    auto visit = [&](uint64_t y, uint32_t i) {
-      if (stage) lo[swz32(i)] = (uint32_t)y;
-      const double p = pred_linear(m0, m1, i);
-      const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
-      const int64_t d = (int64_t)(y - (uint64_t)pr);
-      dmax = d > dmax ? d : dmax;
-      dmin = d < dmin ? d : dmin;
-    };
-    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, four in flight per thread
-      const uint32_t np = len / 2;
-#pragma unroll 4
-      for (uint32_t q = tid; q < np; q += nt) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
-        visit(((uint64_t)v.y << 32) | v.x, 2 * q);
-        visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
-      }
-      if ((len & 1) && tid == 0) visit(__ldg(src + len - 1), len - 1);
-    } else {
-      for (uint32_t i = tid; i < len; i += nt) visit(__ldg(src + i), i);
-    }
-    u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
-    group_reduce2<3, 4, G>(rmx, rmn, sm.red);
-    dmax = (int64_t)(uint64_t)rmx;
-    dmin = (int64_t)(uint64_t)rmn;
-    const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
-    m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
-    return dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
-  };
-  bool narrow_range;
-  if (a.seq_models) {
-    m0 = a.seq_models[b * 3 + 0];
-    m1 = a.seq_models[b * 3 + 1];
-    narrow_range = mid_pass(true);
-  } else {
-    u128 sy = 0, siy = 0;
-    auto visit = [&](uint64_t y, uint32_t i) {
-      lo[swz32(i)] = (uint32_t)y;
-      sy += y;
-      siy += (u128)y * i;
-    };
-    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-      const uint32_t np = len / 2;
-#pragma unroll 2
-      for (uint32_t q = tid; q < np; q += nt) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
-        visit(((uint64_t)v.y << 32) | v.x, 2 * q);
-        visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
-      }
-      if ((len & 1) && tid == 0) visit(__ldg(src + len - 1), len - 1);
-    } else {
-      for (uint32_t i = tid; i < len; i += nt) visit(__ldg(src + i), i);
-    }
-    group_reduce2<0, 0, G>(sy, siy, sm.red);
-    // lr_int_T::caltheta (lr.h:79-83) on exact moments
-    const double md = __uint2double_rn(len);
-    const uint64_t m = len;
-    const double sumx = __ull2double_rn(m * (m - 1) / 2);
-    const double sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
-    const double sumy = u128_to_double(sy), sumxy = u128_to_double(siy);
-    const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
-    const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
-    m1 = __ddiv_rn(ccc, xxx);
-    m0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(m1, sumx)), md);
-    narrow_range = mid_pass(false);
-  }
-
-  // ---- residuals (:51-72) and width (:108-117) ---------------------------------
-  const bool r32 = narrow_range && preds_nonneg(m0, m1, len);
-  const bool fast = model_in_range(m0, m1, 0.0, len);
-  auto resid = [&](uint32_t k, bool &pos) -> uint64_t {  // from global memory, as the generic encoder
-    const uint64_t y = __ldg(src + k);
-    const double p = pred_linear(m0, m1, k);
-    const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
-    pos = y > (uint64_t)pred;
-    return pos ? y - (uint64_t)pred : (uint64_t)pred - y;
-  };
-  uint32_t l;
-  if (r32) {
-    uint32_t rm32 = 0;
-    for (uint32_t i0 = 0; i0 < len; i0 += nt) {
-      const uint32_t i = i0 + tid;
-      bool pos = false;
-      if (i < len) {
-        const uint32_t s = swz32(i);
-        const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
-        const int32_t d = (int32_t)(lo[s] - (uint32_t)pred);
-        pos = d > 0;  // y > pred
-        const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
-        lo[s] = r;
-        rm32 = r > rm32 ? r : rm32;
-      }
-      const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
-      if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
-    }
-    const uint64_t rmax = (uint64_t)group_reduce<1, G>((u128)rm32, sm.red);
-    l = rmax ? bits_of(rmax) + 1 : 0;
-  } else {
-    uint64_t rmax = 0;
-    for (uint32_t i = tid; i < len; i += nt) {
-      bool pos;
-      const uint64_t r = resid(i, pos);
-      rmax = r > rmax ? r : rmax;
-    }
-    rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
-    l = rmax ? bits_of(rmax) + 1 : 0;
-    if (l > TB) l = TB;
-  }
-  if (l == TB - 1) l = TB;  // written raw, as the generic encoder explains
-  const bool raw = l == TB;
-  const bool rows = r32 && l > 0;
-  const uint64_t size = block_bytes<kLinear, 8>(l, len);
-  const uint32_t H = raw ? 1u : 17u;
-
-  // ---- offset by look-back, packing alongside -----------------------------------
-  const bool split = rows && nt >= 256;
   if (tid < 32) {
-    const uint64_t excl = lookback_prefix(a.status, b, size, a.error);
+    // ---- offset by look-back, alongside the encoding ------------------------------
+    const uint64_t excl = lookback_excl(a.status, b, a.error);
     if (tid == 0) sm.bcast[1] = excl;
-  } else if (split && tid >= 128) {
-    pack_rows(lo, sm.signs, pk, len, l, tid - 128, nt - 128);
-  }
-  if (tid == 0) {
-    sm.hdr[0] = (uint8_t)l;
-    if (!raw) {
-      const uint64_t w0 = (uint64_t)__double_as_longlong(m0), w1 = (uint64_t)__double_as_longlong(m1);
-      for (int j = 0; j < 8; ++j) {
-        sm.hdr[1 + j] = (uint8_t)(w0 >> (8 * j));
-        sm.hdr[9 + j] = (uint8_t)(w1 >> (8 * j));
+  } else {
+    const uint32_t ct = tid - 32, cn = nt - 32;  // encoding threads
+    // ---- fit and midpoint shift -----------------------------------------------------
+    double m0, m1;
+    auto mid_pass = [&](bool stage) -> bool {  // true: residuals before the shift span < 2^30
+      int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
+      const bool fast = model_in_range(m0, m1, 0.0, len);
+      auto visit = [&](uint64_t y, uint32_t i) {
+        if (stage) lo[swz32(i)] = (uint32_t)y;
+        const double p = pred_linear(m0, m1, i);
+        const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
+        const int64_t d = (int64_t)(y - (uint64_t)pr);
+        dmax = d > dmax ? d : dmax;
+        dmin = d < dmin ? d : dmin;
+      };
+      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, four in flight per thread
+        const uint32_t np = len / 2;
+#pragma unroll 4
+        for (uint32_t q = ct; q < np; q += cn) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+          visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+          visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+        }
+        if ((len & 1) && ct == 0) visit(__ldg(src + len - 1), len - 1);
+      } else {
+        for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
+      }
+      u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
+      sub_reduce2<3, 4>(rmx, rmn, sm.red);
+      dmax = (int64_t)(uint64_t)rmx;
+      dmin = (int64_t)(uint64_t)rmn;
+      const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
+      m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
+      return dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
+    };
+    bool narrow_range;
+    if (a.seq_models) {
+      m0 = a.seq_models[b * 3 + 0];
+      m1 = a.seq_models[b * 3 + 1];
+      narrow_range = mid_pass(true);
+    } else {
+      u128 sy = 0, siy = 0;
+      auto visit = [&](uint64_t y, uint32_t i) {
+        lo[swz32(i)] = (uint32_t)y;
+        sy += y;
+        siy += (u128)y * i;
+      };
+      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+        const uint32_t np = len / 2;
+#pragma unroll 2
+        for (uint32_t q = ct; q < np; q += cn) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+          visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+          visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+        }
+        if ((len & 1) && ct == 0) visit(__ldg(src + len - 1), len - 1);
+      } else {
+        for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
+      }
+      sub_reduce2<0, 0>(sy, siy, sm.red);
+      // lr_int_T::caltheta (lr.h:79-83) on exact moments
+      const double md = __uint2double_rn(len);
+      const uint64_t m = len;
+      const double sumx = __ull2double_rn(m * (m - 1) / 2);
+      const double sumxx = u128_to_double((u128)(m - 1) * m * (2 * m - 1) / 6);
+      const double sumy = u128_to_double(sy), sumxy = u128_to_double(siy);
+      const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+      const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+      m1 = __ddiv_rn(ccc, xxx);
+      m0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(m1, sumx)), md);
+      narrow_range = mid_pass(false);
+    }
+
+    // ---- residuals (:51-72) and width (:108-117) -------------------------------------
+    const bool r32 = narrow_range && preds_nonneg(m0, m1, len);
+    uint32_t l;
+    if (r32) {
+      uint32_t rm32 = 0;
+      for (uint32_t i0 = 0; i0 < len; i0 += cn) {
+        const uint32_t i = i0 + ct;
+        bool pos = false;
+        if (i < len) {
+          const uint32_t s = swz32(i);
+          const int64_t pred = trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
+          const int32_t d = (int32_t)(lo[s] - (uint32_t)pred);
+          pos = d > 0;  // y > pred
+          const uint32_t r = pos ? (uint32_t)d : (uint32_t)(-d);
+          lo[s] = r;
+          rm32 = r > rm32 ? r : rm32;
+        }
+        const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+        if ((ct & 31) == 0) sm.signs[i0 / 32 + ct / 32] = ballot;
+      }
+      u128 rmax = rm32, none = 0;
+      sub_reduce2<1, 5>(rmax, none, sm.red);
+      l = rmax ? bits_of((uint64_t)rmax) + 1 : 0;
+    } else {
+      const bool fast = model_in_range(m0, m1, 0.0, len);
+      uint64_t rm = 0;
+      for (uint32_t i = ct; i < len; i += cn) {
+        const uint64_t y = __ldg(src + i);
+        const double p = pred_linear(m0, m1, i);
+        const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+        const uint64_t r = y > (uint64_t)pred ? y - (uint64_t)pred : (uint64_t)pred - y;
+        rm = r > rm ? r : rm;
+      }
+      u128 rmax = rm, none = 0;
+      sub_reduce2<1, 5>(rmax, none, sm.red);
+      l = rmax ? bits_of((uint64_t)rmax) + 1 : 0;
+      if (l > TB) l = TB;
+    }
+    if (l == TB - 1) l = TB;  // written raw, as the generic encoder explains
+    const bool raw = l == TB;
+    const uint64_t size = block_bytes<kLinear, 8>(l, len);
+    if (ct == 0) {
+      if (b > 0) st_relaxed(&a.status[b], kFlagAgg | size);  // successors need not wait for our prefix
+      sm.bcast[2] = size;
+      sm.bcast[3] = l | ((uint64_t)r32 << 8);
+      model[0] = m0;
+      model[1] = m1;
+      sm.hdr[0] = (uint8_t)l;
+      if (!raw) {
+        const uint64_t w0 = (uint64_t)__double_as_longlong(m0), w1 = (uint64_t)__double_as_longlong(m1);
+        for (int j = 0; j < 8; ++j) {
+          sm.hdr[1 + j] = (uint8_t)(w0 >> (8 * j));
+          sm.hdr[9 + j] = (uint8_t)(w1 >> (8 * j));
+        }
       }
     }
+    if (r32 && l > 0) pack_rows(lo, sm.signs, pk, len, l, ct, cn);  // residuals and signs: after the reduction's barriers
   }
   group_sync<G>();
-  if (rows && !split) {
-    pack_rows(lo, sm.signs, pk, len, l, tid, nt);
-    group_sync<G>();
-  }
-  const uint64_t goff = sm.bcast[1];
-  if (goff == ~0ull) return;                                  // look-back gave up (error word set)
-  if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {     // never write past the buffer
+
+  const uint64_t size = sm.bcast[2], goff = sm.bcast[1];
+  const uint32_t l = (uint32_t)(sm.bcast[3] & 0xff);
+  const bool r32 = (sm.bcast[3] >> 8) & 1, raw = l == TB, rows = r32 && l > 0;
+  const uint32_t H = raw ? 1u : 17u;
+  const double m0 = model[0], m1 = model[1];
+  if (goff == ~0ull) return;  // look-back gave up (error word set)
+  if (tid == 0) st_relaxed(&a.status[b], kFlagIncl | (goff + size));
+  if (goff + size + LECO_PAYLOAD_SLACK > a.payload_cap) {  // never write past the buffer
     if (tid == 0) atomicOr(a.error, kErrCapacity);
     return;
   }
@@ -426,11 +438,14 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
   } else if (rows) {
     write_image_packed(a.payload, goff, size, H, sm.hdr, pk, tid, nt);
   } else {
+    const bool fast = model_in_range(m0, m1, 0.0, len);
     const uint32_t sb = l ? l - 1 : 0;
     write_image(a.payload, goff, size, H, sm.hdr, l, len, [&](uint32_t k) -> uint64_t {
-      bool pos;
-      const uint64_t r = resid(k, pos);
-      return r | ((uint64_t)pos << sb);
+      const uint64_t y = __ldg(src + k);
+      const double p = pred_linear(m0, m1, k);
+      const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+      const bool pos = y > (uint64_t)pred;
+      return (pos ? y - (uint64_t)pred : (uint64_t)pred - y) | ((uint64_t)pos << sb);
     }, tid, nt);
   }
 
