@@ -328,11 +328,16 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       m1 = a.seq_models[b * 3 + 1];
       narrow_range = mid_pass(true);
     } else {
-      u128 sy = 0, siy = 0;
+      // Moments in 32-bit halves of y: a thread sees at most 16384 values, each
+      // i*y_lo, i*y_hi < 2^46, so the 64-bit partial sums stay below 2^60.
+      uint64_t slo = 0, shi = 0, tlo = 0, thi = 0;
       auto visit = [&](uint64_t y, uint32_t i) {
         lo[swz32(i)] = (uint32_t)y;
-        sy += y;
-        siy += (u128)y * i;
+        const uint32_t yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
+        slo += yl;
+        shi += yh;
+        tlo += (uint64_t)yl * i;
+        thi += (uint64_t)yh * i;
       };
       if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
         const uint32_t np = len / 2;
@@ -346,6 +351,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       } else {
         for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
       }
+      u128 sy = ((u128)shi << 32) + slo, siy = ((u128)thi << 32) + tlo;
       sub_reduce2<0, 0>(sy, siy, sm.red);
       // lr_int_T::caltheta (lr.h:79-83) on exact moments
       const double md = __uint2double_rn(len);
