@@ -188,6 +188,40 @@ def test_corrupt_header_sets_error_word(lc, orc, dev):
     lc.check()  # cleared
 
 
+@pytest.mark.parametrize("s,codec,bs,shift", [(8, 0, 4096, 0), (8, 3, 4096, 0), (4, 0, 4096, 0), (4, 5, 4096, 0),
+                                              (8, 0, 4096, 1), (8, 0, 4099, 0), (4, 0, 2050, 0)])
+def test_reference_fit_large_columns(lc, orc, dev, s, codec, bs, shift):
+    """Columns of >= 4096 blocks under the reference fit (the sequential-fit
+    kernel, then the encoder), with values 8 bytes off 16-byte alignment and block
+    sizes whose rows are not a multiple of 16 bytes among them.  Every image equals
+    the oracle's; large values make the reference's sequential FP64 sums round."""
+    import torch
+    rng = np.random.default_rng(7 * s + codec + bs + shift)
+    dt = np.uint64 if s == 8 else np.uint32
+    n = bs * 4100 + 777
+    i = np.arange(n, dtype=np.float64)
+    if s == 8:
+        x = 2.0 ** 41 + np.cumsum(rng.exponential(2.0 ** 14, n)) + rng.normal(0, 2 ** 10, n)
+    else:
+        x = 1e8 + i * 0.9 + rng.normal(0, 40, n)
+    if codec == 3:
+        x = x + 1e-6 * (i % 8192) ** 2
+    x = np.sort(x).astype(np.uint64).astype(dt)
+    buf = torch.from_numpy(np.concatenate([np.zeros(shift, dt), x]).view(np.int64 if s == 8 else np.int32)).to(dev)
+    col = lc.encode(buf[shift:], codec, bs, lc.FIT_REFERENCE)
+    pay, off = col.to_host()
+    if codec == 5:
+        for b in list(range(0, 300)) + list(range(col.nblocks - 300, col.nblocks)):
+            img, _, _ = orc.legacy_encode_block(x[b * bs:(b + 1) * bs])
+            assert pay[off[b]:off[b + 1]].tobytes() == img, b
+    else:
+        epay, eoff, _ = expected_gpu_column(orc, codec, x, bs)
+        assert np.array_equal(off, eoff)
+        assert np.array_equal(pay, epay)
+    assert np.array_equal(to_np(col.decode(), s), x)
+    lc.check()
+
+
 @pytest.mark.parametrize("s", [4, 8])
 def test_staged_decode_large_mixed(lc, orc, dev, s):
     """Columns of >= 1024 blocks take the persistent TMA-staged decoder; mix
