@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint
     if (tid == 0 && has_next) issue(blk + gridDim.x, cur ^ 1);
     const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
     if (cur) ph1 ^= 1; else ph0 ^= 1;
-    if (!ok) {
+    if (!__syncthreads_and(ok)) {  // every thread leaves together
       if (tid == 0) {
         atomicOr(a.error, kErrTimeout);
         if (has_next) mbar_wait_bounded(&bar[cur ^ 1], cur ? ph0 : ph1);  // let our own copy in flight land

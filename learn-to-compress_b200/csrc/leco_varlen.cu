@@ -14,7 +14,9 @@
 
 #include <string>
 
+#include "leco_decode.cuh"
 #include "leco_encode.cuh"
+#include "leco_stage.cuh"
 
 namespace leco {
 
@@ -205,40 +207,129 @@ __device__ __forceinline__ uint64_t seg_value(const uint64_t *words, const SegHd
   return apply_signed(pred, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
 }
 
-// One CTA per segment (Leco_cost_merge_double_wo_round::decodeArray8, :573-626).
-// Fields of at most 32 bits are extracted with one 32-bit funnel shift; when
-// every prediction of the segment lies inside (-2^62, 2^62) the uint64_t
-// conversion needs no out-of-range handling.
+// Bulk decode (Leco_cost_merge_double_wo_round::decodeArray8, :573-626) by
+// persistent CTAs over items of kVarGroup consecutive segments: CTA c walks items
+// c, c + gridDim.x, ...; warp 0 loads the next item's offsets and starts and
+// stages its images (contiguous in the payload) into the other half of a double
+// buffer with one cp.async.bulk while the CTA's warps decode the current item's
+// segments out of shared memory, one segment per warp.  A segment with fields of at most 32 bits whose
+// predictions lie inside (-2^62, 2^62) decodes exactly as a LeCo block with
+// theta0 = t0 and theta1 = slope (same prediction, same sign-magnitude fields;
+// under that bound the uint64_t conversion of bit_read.h:530 is the truncation the
+// block decoder applies), through the block decoder's narrow path; other
+// segments, and items larger than the buffer, decode from global memory.
+constexpr uint32_t kVarGroup = 8;
+constexpr uint32_t kVarStageBytes = 24832;  // one buffer: ~8 segments of ~2000 values of 12-bit fields, + slack
+struct VarStage {
+  uint64_t gbase;                    // staged copy's 16-byte aligned global start
+  uint64_t off[kVarGroup];           // image offsets
+  uint64_t st[kVarGroup + 1];        // value ranges: segment g is [st[g], st[g+1])
+  uint32_t cnt, direct;              // segments in the item; 1: decode from global memory
+};
+
 __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *payload, const uint64_t *offsets,
                                                             const uint64_t *starts, uint64_t nseg, uint64_t n,
-                                                            uint64_t *out, uint32_t *error) {
-  const uint64_t sgi = blockIdx.x;
-  const uint64_t st = starts[sgi], en = sgi + 1 < nseg ? starts[sgi + 1] : n;
-  const uint32_t len = (uint32_t)(en - st);
+                                                            uint64_t *out, uint32_t bufcap, uint32_t *error) {
+  extern __shared__ __align__(128) uint8_t vstage[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ VarStage meta[2];
+  const uint32_t tid = threadIdx.x;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
-  const SegHdr h = parse_seg(payload, offsets[sgi]);
-  if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
-    if (threadIdx.x == 0) atomicOr(error, kErrBadHeader);
-    return;
+  const uint64_t nitems = (nseg + kVarGroup - 1) / kVarGroup;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
   }
-  const bool fast = fabs(h.t0) + fabs(h.slope) * __uint2double_rn(len) < 4611686018427387904.0;
-  if (h.l >= 1 && h.l <= 32 && fast) {
-    const uint32_t *w32 = reinterpret_cast<const uint32_t *>(payload) + (h.body_bit >> 5);
-    const uint32_t bsh = (uint32_t)(h.body_bit & 31), l = h.l, mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
-    const uint32_t sb = l - 1, m1 = mask >> 1;
-    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
-      const uint32_t r = bsh + k * l;
-      const uint32_t *p = w32 + (r >> 5);
-      const uint32_t f = __funnelshift_r(__ldg(p), __ldg(p + 1), r) & mask;
-      const int64_t pred = __double2ll_rz(__dadd_rn(h.t0, __dmul_rn(__uint2double_rn(k), h.slope)));
-      const uint32_t mag = f & m1;
-      const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
-      __stcs(out + st + k, (uint64_t)(pred + d));
+  __syncthreads();
+  auto issue = [&](uint64_t item, int which) {  // warp 0 only
+    const uint32_t lane = tid & 31;
+    const uint64_t s0 = item * kVarGroup;
+    const uint32_t cnt = (uint32_t)umin64(kVarGroup, nseg - s0);
+    VarStage &m = meta[which];
+    uint64_t o = 0;
+    if (lane <= cnt) o = __ldg(offsets + s0 + lane);  // offsets[s0 .. s0 + cnt]
+    if (lane < cnt) m.off[lane] = o;
+    if (lane <= cnt) m.st[lane] = s0 + lane < nseg ? __ldg(starts + s0 + lane) : n;
+    const uint64_t o0 = __shfl_sync(0xffffffffu, o, 0), o1 = __shfl_sync(0xffffffffu, o, cnt);
+    if (lane == 0) {
+      const uint64_t g0 = o0 & ~15ull, g1 = (o1 + 8 + 15) & ~15ull;  // +8: field reads touch one word past a body
+      const uint64_t bytes = g1 - g0;
+      m.gbase = g0;
+      m.cnt = cnt;
+      m.direct = bytes > bufcap;
+      if (!m.direct) {
+        mbar_arrive_tx(&bar[which], (uint32_t)bytes);
+        bulk_g2s(vstage + (size_t)which * bufcap, payload + g0, (uint32_t)bytes, &bar[which]);
+      } else {
+        mbar_arrive(&bar[which]);
+      }
     }
-    return;
+  };
+  uint64_t item = blockIdx.x;
+  if (tid < 32 && item < nitems) issue(item, 0);
+  uint32_t ph0 = 0, ph1 = 0;
+  for (int it = 0; item < nitems; item += gridDim.x, ++it) {
+    const int cur = it & 1;
+    const bool has_next = item + gridDim.x < nitems;
+    if (tid < 32 && has_next) issue(item + gridDim.x, cur ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
+    if (cur) ph1 ^= 1;
+    else ph0 ^= 1;
+    if (!__syncthreads_and(ok)) {  // every thread leaves together
+      if (tid == 0) {
+        atomicOr(error, kErrTimeout);
+        if (has_next) mbar_wait_bounded(&bar[cur ^ 1], cur ? ph0 : ph1);  // let our own copy in flight land
+      }
+      return;
+    }
+    const VarStage &m = meta[cur];
+    const uint8_t *sb = vstage + (size_t)cur * bufcap;
+    const uint32_t lane = tid & 31;
+    for (uint32_t g = tid >> 5; g < m.cnt; g += blockDim.x >> 5) {  // one warp per segment
+      const uint64_t st = m.st[g], off = m.off[g];
+      const uint32_t len = (uint32_t)(m.st[g + 1] - st);
+      bool staged = false;
+      if (!m.direct) {
+        const uint32_t hoff = (uint32_t)(off - m.gbase);
+        const uint8_t *hb = sb + hoff;
+        const uint32_t start = hb[0] | (uint32_t)hb[1] << 8 | (uint32_t)hb[2] << 16 | (uint32_t)hb[3] << 24;
+        const uint32_t l = hb[4];
+        if (l >= 1 && l <= 32 && (uint64_t)start == st) {
+          uint64_t t0w = 0;
+          uint32_t slw = 0;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) t0w |= (uint64_t)hb[5 + j] << (8 * j);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) slw |= (uint32_t)hb[13 + j] << (8 * j);
+          BlockHdr h;
+          h.l = l;
+          h.a0 = __longlong_as_double((long long)t0w);
+          h.a1 = (double)__uint_as_float(slw);
+          h.a2 = 0;
+          h.base = 0;
+          h.body_bit = (uint64_t)(hoff + 17) * 8;
+          if (fabs(h.a0) + fabs(h.a1) * __uint2double_rn(len) < 4611686018427387904.0) {
+            mark_nonneg<kLinear>(h, len);
+            const int32_t kstart = -(int32_t)((reinterpret_cast<uintptr_t>(out + st) & 15) / 8);
+            decode_narrow<uint64_t, kLinear, true, true, 32>(h, false, reinterpret_cast<const uint32_t *>(sb), out, st, 0,
+                                                             len, kstart);
+            staged = true;
+          }
+        }
+      }
+      if (!staged) {
+        const SegHdr h = parse_seg(payload, off);
+        if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
+          if (lane == 0) atomicOr(error, kErrBadHeader);
+        } else {
+          const uint32_t c = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
+          for (uint32_t k = lane; k < c && k < len; k += 32) __stcs(out + st + k, seg_value(words, h, k));
+        }
+      }
+    }
+    __syncthreads();  // everyone is done with this buffer and its meta before they are refilled
   }
-  const uint32_t cnt = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
-  for (uint32_t k = threadIdx.x; k < cnt && k < len; k += blockDim.x) __stcs(out + st + k, seg_value(words, h, k));
 }
 
 // Random access: binary search over the segment starts, then one value
@@ -328,8 +419,17 @@ int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, cons
   uint32_t *err = nullptr;
   int rc = leco::device_error_word(&err);
   if (rc) return rc;
-  varlen_decode_kernel<<<(unsigned)nseg, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts,
-                                                                                          nseg, n, d_out, err);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = (int)(2 * kVarStageBytes);
+  cudaFuncSetAttribute(varlen_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_decode_kernel, 256, smem);
+  const uint64_t nitems = (nseg + kVarGroup - 1) / kVarGroup;
+  const unsigned grid = (unsigned)umin64(nitems, (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1));
+  varlen_decode_kernel<<<grid, 256, smem, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts, nseg, n,
+                                                                                  d_out, kVarStageBytes, err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_decode: ") + cudaGetErrorString(e));
 }
