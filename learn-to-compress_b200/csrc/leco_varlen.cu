@@ -332,28 +332,66 @@ __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *paylo
   }
 }
 
-// Random access: binary search over the segment starts, then one value
-// (randomdecodeArray8, :636-698; the raw case indexes inside the segment).
+// Random access (randomdecodeArray8, :636-698; the raw case indexes inside the
+// segment): the segment is the last one whose start is <= the index.  Every CTA
+// keeps a sample of the start array (every stride-th start, at most kVarSamples)
+// in shared memory; a lookup searches the sample there and then only its
+// stride-wide window of the start array in global memory.  Each thread carries
+// kVarQ lookups through the search level by level, so their loads are in flight
+// together.
+constexpr uint32_t kVarSamples = 4096, kVarQ = 4;
 __global__ void __launch_bounds__(256) varlen_gather_kernel(const uint8_t *payload, const uint64_t *offsets,
                                                             const uint64_t *starts, uint64_t nseg, uint64_t n,
                                                             const uint64_t *idx, uint64_t m, uint64_t *out,
                                                             uint32_t *error) {
+  __shared__ uint64_t samp[kVarSamples];
   const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t g = __ldg(idx + i);
-    if (g >= n) {
-      out[i] = 0;
-      atomicOr(error, kErrBadIndex);
-      continue;
+  const uint64_t stride = (nseg + kVarSamples - 1) / kVarSamples;
+  const uint32_t ns = (uint32_t)((nseg + stride - 1) / stride);
+  for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) samp[i] = __ldg(starts + (uint64_t)i * stride);
+  __syncthreads();
+  const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < m; i0 += T * kVarQ) {
+    uint64_t g[kVarQ], lo[kVarQ], len[kVarQ];
+    bool live[kVarQ];
+#pragma unroll
+    for (uint32_t q = 0; q < kVarQ; ++q) {
+      const uint64_t i = i0 + q * T;
+      live[q] = i < m;
+      g[q] = live[q] ? __ldg(idx + i) : 0;
+      if (live[q] && g[q] >= n) {
+        out[i] = 0;
+        atomicOr(error, kErrBadIndex);
+        live[q] = false;
+      }
+      // sample: largest j with samp[j] <= g (samp[0] = 0)
+      uint32_t base = 0, span = ns;
+      while (span > 1) {
+        const uint32_t half = span / 2;
+        base = samp[base + half] <= g[q] ? base + half : base;
+        span -= half;
+      }
+      lo[q] = (uint64_t)base * stride;
+      len[q] = umin64(stride, nseg - lo[q]);
     }
-    uint64_t lo = 0, hi = nseg;  // largest s with starts[s] <= g
-    while (hi - lo > 1) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (__ldg(starts + mid) <= g) lo = mid;
-      else hi = mid;
+    // window: largest s in [lo, lo + len) with starts[s] <= g, all lookups one level at a time
+    for (uint64_t span = stride; span > 1; span -= span / 2) {
+#pragma unroll
+      for (uint32_t q = 0; q < kVarQ; ++q) {
+        if (len[q] > 1) {
+          const uint64_t half = len[q] / 2;
+          lo[q] = __ldg(starts + lo[q] + half) <= g[q] ? lo[q] + half : lo[q];
+          len[q] -= half;
+        }
+      }
     }
-    const SegHdr h = parse_seg(payload, __ldg(offsets + lo));
-    out[i] = seg_value(words, h, (uint32_t)(g - h.start));
+    SegHdr h[kVarQ];
+#pragma unroll
+    for (uint32_t q = 0; q < kVarQ; ++q)
+      if (live[q]) h[q] = parse_seg(payload, __ldg(offsets + lo[q]));
+#pragma unroll
+    for (uint32_t q = 0; q < kVarQ; ++q)
+      if (live[q]) out[i0 + q * T] = seg_value(words, h[q], (uint32_t)(g[q] - h[q].start));
   }
 }
 
@@ -445,7 +483,7 @@ int leco_varlen_gather(const uint8_t *d_payload, const uint64_t *d_offsets, cons
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned grid = (unsigned)umin64((m + 255) / 256, (uint64_t)sms * 16);
+  const unsigned grid = (unsigned)umin64((m + 256 * kVarQ - 1) / (256 * kVarQ), (uint64_t)sms * 4);
   varlen_gather_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts, nseg, n,
                                                                                 d_idx, m, d_out, err);
   cudaError_t e = cudaGetLastError();
