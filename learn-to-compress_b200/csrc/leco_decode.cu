@@ -33,6 +33,31 @@ __global__ void __launch_bounds__(256) decode_kernel_warp(DecodeLaunch a, uint64
   if (i < nblk) decode_block<T, CODEC, 32>(a, a.first / a.bs + i);
 }
 
+// Sum of the values of block b, this thread's share (all threads of the CTA
+// call it): the values as sum_kernel below computes them, for the staged sum's
+// blocks that do not fit its buffer or are wider than 32 bits.
+template <typename T, int CODEC>
+__device__ __forceinline__ uint64_t sum_block_direct(const DecodeLaunch &a, uint64_t b) {
+  constexpr int S = sizeof(T);
+  constexpr uint32_t TB = 8u * S;
+  const uint64_t base = b * a.bs;
+  const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
+  const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
+  const BlockHdr h = parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b));
+  if (h.l == 126 || h.l == 127 || h.l > TB) {
+    if (threadIdx.x == 0) atomicOr(a.error, kErrBadHeader);
+    return 0;
+  }
+  const bool raw = h.l == TB;
+  const uint32_t l = raw ? TB : h.l;
+  uint64_t acc = 0;
+  for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
+    const uint64_t f = l ? load_field(words, h.body_bit + (uint64_t)k * l, l) : 0;
+    acc += (uint64_t)(T)(raw ? f : value_from_field<CODEC, S>(h, k, f));
+  }
+  return acc;
+}
+
 // ---- TMA-staged persistent decode --------------------------------------------
 struct StageMeta {
   uint64_t gbase;   // 16-byte aligned global byte address of the staged copy
@@ -45,12 +70,16 @@ struct StageMeta {
 // packed body) into the other half of a double buffer with one cp.async.bulk
 // while the CTA decodes the current one out of shared memory.  Blocks that do
 // not fit the buffer, wide (l > 32) and Delta blocks take the direct path.
-template <typename T, int CODEC>
-__global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint32_t bufcap) {
+// SUM: the compressed-domain sum instead -- the values are added up, not stored,
+// and each CTA adds its total to *d_sum once.
+template <typename T, int CODEC, bool SUM = false>
+__global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint32_t bufcap, uint64_t *d_sum = nullptr) {
   constexpr int S = sizeof(T);
   extern __shared__ __align__(128) uint8_t stage[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ StageMeta meta[2];
+  __shared__ u128 red[SUM ? 33 : 1];
+  uint64_t acc = 0;
   const uint32_t tid = threadIdx.x;
   const uint64_t nblk = (a.n + a.bs - 1) / a.bs;
   uint8_t *buf0 = stage, *buf1 = stage + bufcap;
@@ -86,54 +115,62 @@ __global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint
     if (tid == 0 && has_next) issue(blk + gridDim.x, cur ^ 1);
     const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
     if (cur) ph1 ^= 1; else ph0 ^= 1;
-    if (!__syncthreads_and(ok)) {  // every thread leaves together
+    if (ok) {  // a thread whose wait gave up touches neither the buffer nor the output
+      const StageMeta m = meta[cur];
+      const uint8_t *sb = (cur ? buf1 : buf0);
+      const uint32_t l = sb[m.hoff];
+      const uint64_t base = blk * a.bs;
+      const uint32_t len = (uint32_t)umin64(a.bs, a.n - base);
+      const bool raw = l == 8u * S;
+      const bool narrow = (CODEC != kDelta) && (l <= 32) && (!raw || S == 4);
+      if (m.direct || !narrow) {
+        if (SUM) acc += sum_block_direct<T, CODEC>(a, blk);
+        else decode_block<T, CODEC>(a, blk);
+      } else {
+        BlockHdr h;
+        h.l = l;
+        h.a0 = h.a1 = h.a2 = 0;
+        h.base = 0;
+        const uint8_t *hb = sb + m.hoff + 1;
+        if (!raw) {
+          uint64_t w[3] = {0, 0, 0};
+          const int nw = CODEC == kPoly2 ? 3 : (CODEC == kLinear ? 2 : 1);
+  #pragma unroll
+          for (int q = 0; q < 3; ++q)
+            if (q < nw)
+  #pragma unroll
+              for (int j = 0; j < 8; ++j) w[q] |= (uint64_t)hb[8 * q + j] << (8 * j);
+          if (CODEC == kLinear || CODEC == kPoly2) {
+            h.a0 = __longlong_as_double((long long)w[0]);
+            h.a1 = __longlong_as_double((long long)w[1]);
+            h.a2 = __longlong_as_double((long long)w[2]);
+          } else {
+            h.base = S == 8 ? w[0] : (w[0] & 0xffffffffull);
+          }
+        }
+        h.body_bit = (uint64_t)(m.hoff + (raw ? 1u : Hdr<CODEC, S>::bytes)) * 8;
+        const uint32_t *w32 = reinterpret_cast<const uint32_t *>(sb);
+        const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + base);
+        const int32_t kstart = -(int32_t)((oaddr & 15) / S);
+        const bool fast = (CODEC == kFor) || raw || pred_in_range<CODEC>(h, len);
+        if (!raw) mark_nonneg<CODEC>(h, len);
+        if (fast) acc += decode_narrow<T, CODEC, true, true, 256, SUM>(h, raw, w32, out, base, 0, len, kstart);
+        else acc += decode_narrow<T, CODEC, false, true, 256, SUM>(h, raw, w32, out, base, 0, len, kstart);
+      }
+    }
+    // Everyone is done with this buffer before it is refilled; a wait that gave up in
+    // any thread ends the CTA's work in all of them together.
+    if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicOr(a.error, kErrTimeout);
         if (has_next) mbar_wait_bounded(&bar[cur ^ 1], cur ? ph0 : ph1);  // let our own copy in flight land
       }
       return;
     }
-    const StageMeta m = meta[cur];
-    const uint8_t *sb = (cur ? buf1 : buf0);
-    const uint32_t l = sb[m.hoff];
-    const uint64_t base = blk * a.bs;
-    const uint32_t len = (uint32_t)umin64(a.bs, a.n - base);
-    const bool raw = l == 8u * S;
-    const bool narrow = (CODEC != kDelta) && (l <= 32) && (!raw || S == 4);
-    if (m.direct || !narrow) {
-      decode_block<T, CODEC>(a, blk);
-    } else {
-      BlockHdr h;
-      h.l = l;
-      h.a0 = h.a1 = h.a2 = 0;
-      h.base = 0;
-      const uint8_t *hb = sb + m.hoff + 1;
-      if (!raw) {
-        uint64_t w[3] = {0, 0, 0};
-        const int nw = CODEC == kPoly2 ? 3 : (CODEC == kLinear ? 2 : 1);
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-          if (q < nw)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) w[q] |= (uint64_t)hb[8 * q + j] << (8 * j);
-        if (CODEC == kLinear || CODEC == kPoly2) {
-          h.a0 = __longlong_as_double((long long)w[0]);
-          h.a1 = __longlong_as_double((long long)w[1]);
-          h.a2 = __longlong_as_double((long long)w[2]);
-        } else {
-          h.base = S == 8 ? w[0] : (w[0] & 0xffffffffull);
-        }
-      }
-      h.body_bit = (uint64_t)(m.hoff + (raw ? 1u : Hdr<CODEC, S>::bytes)) * 8;
-      const uint32_t *w32 = reinterpret_cast<const uint32_t *>(sb);
-      const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + base);
-      const int32_t kstart = -(int32_t)((oaddr & 15) / S);
-      const bool fast = (CODEC == kFor) || raw || pred_in_range<CODEC>(h, len);
-      if (!raw) mark_nonneg<CODEC>(h, len);
-      if (fast) decode_narrow<T, CODEC, true, true>(h, raw, w32, out, base, 0, len, kstart);
-      else decode_narrow<T, CODEC, false, true>(h, raw, w32, out, base, 0, len, kstart);
-    }
-    __syncthreads();  // everyone is done with this buffer before it is refilled
+  }
+  if (SUM) {
+    acc = (uint64_t)block_reduce<5>((u128)acc, red);
+    if (threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long *>(d_sum), (unsigned long long)acc);
   }
 }
 
@@ -293,7 +330,21 @@ int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st) { LE
 template <typename T, int CODEC>
 static void run_sum(const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st) {
   const uint64_t nb = (L.n + L.bs - 1) / L.bs;
-  if (nb) sum_kernel<T, CODEC><<<(unsigned)nb, 256, 0, st>>>(L, d_sum);
+  if (!nb) return;
+  const bool staged = (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 && CODEC != kDelta && CODEC != kLegacy &&
+                      nb >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
+  if (!staged) {
+    sum_kernel<T, CODEC><<<(unsigned)nb, 256, 0, st>>>(L, d_sum);
+    return;
+  }
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = 2 * kStageBuf + 64;
+  cudaFuncSetAttribute(decode_staged_kernel<T, CODEC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_staged_kernel<T, CODEC, true>, 256, smem);
+  const uint64_t grid = umin64(nb, (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1));
+  decode_staged_kernel<T, CODEC, true><<<(unsigned)grid, 256, smem, st>>>(L, kStageBuf, d_sum);
 }
 int launch_sum(int codec, int s, const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st) {
   LECO_DISPATCH(codec, s, run_sum, L, d_sum, st);

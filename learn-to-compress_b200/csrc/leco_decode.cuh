@@ -155,9 +155,11 @@ __device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
 // Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
 // (raw u32 blocks included).  Each thread produces VEC consecutive values per
 // step and writes them with one 16-byte store.
-template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256>
-__device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32, T *out,
-                                              uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
+// SUM: instead of storing, returns this thread's sum of the values (as T).
+template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256, bool SUM = false>
+__device__ __forceinline__ uint64_t decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32,
+                                                  T *out, uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
+  uint64_t acc = 0;
   constexpr int S = sizeof(T);
   constexpr int VEC = 32 / S;  // two 16-byte stores per step
   const uint32_t l = raw ? 32u : h.l;
@@ -194,6 +196,12 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
         v[j] = (uint64_t)(pred + d);
       }
     }
+    if (SUM) {
+#pragma unroll
+      for (int j = 0; j < VEC; ++j)
+        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) acc += (uint64_t)(T)v[j];
+      continue;
+    }
     const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
     store_vals<T>(out, obase + kv, v, VEC, full);
     if (!full) {
@@ -202,6 +210,7 @@ __device__ __forceinline__ void decode_narrow(const BlockHdr &h, bool raw, const
         if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
     }
   }
+  return acc;
 }
 
 // ---- bulk / range decode ----------------------------------------------------

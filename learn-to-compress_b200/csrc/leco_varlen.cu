@@ -218,6 +218,9 @@ __device__ __forceinline__ uint64_t seg_value(const uint64_t *words, const SegHd
 // under that bound the uint64_t conversion of bit_read.h:530 is the truncation the
 // block decoder applies), through the block decoder's narrow path; other
 // segments, and items larger than the buffer, decode from global memory.
+// SUM: the compressed-domain sum instead -- value k of every segment for k below its
+// length (seg_value: the bulk decoder's values), added up mod 2^64 without being
+// stored, one atomic add per CTA.
 constexpr uint32_t kVarGroup = 8;
 constexpr uint32_t kVarStageBytes = 24832;  // one buffer: ~8 segments of ~2000 values of 12-bit fields, + slack
 struct VarStage {
@@ -227,12 +230,16 @@ struct VarStage {
   uint32_t cnt, direct;              // segments in the item; 1: decode from global memory
 };
 
+template <bool SUM>
 __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *payload, const uint64_t *offsets,
                                                             const uint64_t *starts, uint64_t nseg, uint64_t n,
-                                                            uint64_t *out, uint32_t bufcap, uint32_t *error) {
+                                                            uint64_t *out, uint32_t bufcap, uint32_t *error,
+                                                            uint64_t *d_sum) {
   extern __shared__ __align__(128) uint8_t vstage[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ VarStage meta[2];
+  __shared__ u128 red[SUM ? 33 : 1];
+  uint64_t acc = 0;
   const uint32_t tid = threadIdx.x;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
   const uint64_t nitems = (nseg + kVarGroup - 1) / kVarGroup;
@@ -276,60 +283,87 @@ __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *paylo
     const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
     if (cur) ph1 ^= 1;
     else ph0 ^= 1;
-    if (!__syncthreads_and(ok)) {  // every thread leaves together
+    if (ok) {  // a thread whose wait gave up touches neither the buffer nor the output
+      const VarStage &m = meta[cur];
+      const uint8_t *sb = vstage + (size_t)cur * bufcap;
+      const uint32_t lane = tid & 31;
+      for (uint32_t g = tid >> 5; g < m.cnt; g += blockDim.x >> 5) {  // one warp per segment
+        const uint64_t st = m.st[g], off = m.off[g];
+        const uint32_t len = (uint32_t)(m.st[g + 1] - st);
+        bool staged = false;
+        if (!m.direct) {
+          const uint32_t hoff = (uint32_t)(off - m.gbase);
+          const uint8_t *hb = sb + hoff;
+          const uint32_t start = hb[0] | (uint32_t)hb[1] << 8 | (uint32_t)hb[2] << 16 | (uint32_t)hb[3] << 24;
+          const uint32_t l = hb[4];
+          if (l >= 1 && l <= 32 && (uint64_t)start == st) {
+            uint64_t t0w = 0;
+            uint32_t slw = 0;
+  #pragma unroll
+            for (int j = 0; j < 8; ++j) t0w |= (uint64_t)hb[5 + j] << (8 * j);
+  #pragma unroll
+            for (int j = 0; j < 4; ++j) slw |= (uint32_t)hb[13 + j] << (8 * j);
+            BlockHdr h;
+            h.l = l;
+            h.a0 = __longlong_as_double((long long)t0w);
+            h.a1 = (double)__uint_as_float(slw);
+            h.a2 = 0;
+            h.base = 0;
+            h.body_bit = (uint64_t)(hoff + 17) * 8;
+            if (fabs(h.a0) + fabs(h.a1) * __uint2double_rn(len) < 4611686018427387904.0) {
+              mark_nonneg<kLinear>(h, len);
+              const int32_t kstart = -(int32_t)((reinterpret_cast<uintptr_t>(out + st) & 15) / 8);
+              acc += decode_narrow<uint64_t, kLinear, true, true, 32, SUM>(h, false, reinterpret_cast<const uint32_t *>(sb),
+                                                                           out, st, 0, len, kstart);
+              staged = true;
+            }
+          }
+        }
+        if (!staged && SUM) {
+          const SegHdr h = parse_seg(payload, off);
+          for (uint32_t k = lane; k < len; k += 32) acc += seg_value(words, h, k);
+        } else if (!staged) {
+          const SegHdr h = parse_seg(payload, off);
+          if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
+            if (lane == 0) atomicOr(error, kErrBadHeader);
+          } else {
+            const uint32_t c = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
+            for (uint32_t k = lane; k < c && k < len; k += 32) __stcs(out + st + k, seg_value(words, h, k));
+          }
+        }
+      }
+    }
+    // Everyone is done with this buffer before it is refilled; a wait that gave up in
+    // any thread ends the CTA's work in all of them together.
+    if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicOr(error, kErrTimeout);
         if (has_next) mbar_wait_bounded(&bar[cur ^ 1], cur ? ph0 : ph1);  // let our own copy in flight land
       }
       return;
     }
-    const VarStage &m = meta[cur];
-    const uint8_t *sb = vstage + (size_t)cur * bufcap;
-    const uint32_t lane = tid & 31;
-    for (uint32_t g = tid >> 5; g < m.cnt; g += blockDim.x >> 5) {  // one warp per segment
-      const uint64_t st = m.st[g], off = m.off[g];
-      const uint32_t len = (uint32_t)(m.st[g + 1] - st);
-      bool staged = false;
-      if (!m.direct) {
-        const uint32_t hoff = (uint32_t)(off - m.gbase);
-        const uint8_t *hb = sb + hoff;
-        const uint32_t start = hb[0] | (uint32_t)hb[1] << 8 | (uint32_t)hb[2] << 16 | (uint32_t)hb[3] << 24;
-        const uint32_t l = hb[4];
-        if (l >= 1 && l <= 32 && (uint64_t)start == st) {
-          uint64_t t0w = 0;
-          uint32_t slw = 0;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) t0w |= (uint64_t)hb[5 + j] << (8 * j);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) slw |= (uint32_t)hb[13 + j] << (8 * j);
-          BlockHdr h;
-          h.l = l;
-          h.a0 = __longlong_as_double((long long)t0w);
-          h.a1 = (double)__uint_as_float(slw);
-          h.a2 = 0;
-          h.base = 0;
-          h.body_bit = (uint64_t)(hoff + 17) * 8;
-          if (fabs(h.a0) + fabs(h.a1) * __uint2double_rn(len) < 4611686018427387904.0) {
-            mark_nonneg<kLinear>(h, len);
-            const int32_t kstart = -(int32_t)((reinterpret_cast<uintptr_t>(out + st) & 15) / 8);
-            decode_narrow<uint64_t, kLinear, true, true, 32>(h, false, reinterpret_cast<const uint32_t *>(sb), out, st, 0,
-                                                             len, kstart);
-            staged = true;
-          }
-        }
-      }
-      if (!staged) {
-        const SegHdr h = parse_seg(payload, off);
-        if (h.start != st || (h.l > 64 && h.l != 126 && h.l != 127)) {
-          if (lane == 0) atomicOr(error, kErrBadHeader);
-        } else {
-          const uint32_t c = h.l == 127 ? 1 : h.l == 126 ? 2 : len;
-          for (uint32_t k = lane; k < c && k < len; k += 32) __stcs(out + st + k, seg_value(words, h, k));
-        }
-      }
-    }
-    __syncthreads();  // everyone is done with this buffer and its meta before they are refilled
   }
+  if (SUM) {
+    acc = (uint64_t)block_reduce<5>((u128)acc, red);
+    if (tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(d_sum), (unsigned long long)acc);
+  }
+}
+
+// Launches varlen_decode_kernel<SUM> with its staging buffers.
+template <bool SUM>
+static cudaError_t launch_varlen_staged(const uint8_t *payload, const uint64_t *offsets, const uint64_t *starts,
+                                        uint64_t nseg, uint64_t n, uint64_t *out, uint32_t *err, uint64_t *d_sum,
+                                        cudaStream_t st) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = (int)(2 * kVarStageBytes);
+  cudaFuncSetAttribute(varlen_decode_kernel<SUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_decode_kernel<SUM>, 256, smem);
+  const uint64_t nitems = (nseg + kVarGroup - 1) / kVarGroup;
+  const unsigned grid = (unsigned)umin64(nitems, (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1));
+  varlen_decode_kernel<SUM><<<grid, 256, smem, st>>>(payload, offsets, starts, nseg, n, out, kVarStageBytes, err, d_sum);
+  return cudaGetLastError();
 }
 
 // Random access (randomdecodeArray8, :636-698; the raw case indexes inside the
@@ -395,21 +429,6 @@ __global__ void __launch_bounds__(256) varlen_gather_kernel(const uint8_t *paylo
   }
 }
 
-__global__ void __launch_bounds__(256) varlen_sum_kernel(const uint8_t *payload, const uint64_t *offsets,
-                                                         const uint64_t *starts, uint64_t nseg, uint64_t n,
-                                                         uint64_t *d_sum) {
-  __shared__ u128 red[33];
-  const uint64_t sgi = blockIdx.x;
-  const uint64_t st = starts[sgi], en = sgi + 1 < nseg ? starts[sgi + 1] : n;
-  const uint32_t len = (uint32_t)(en - st);
-  const uint64_t *words = reinterpret_cast<const uint64_t *>(payload);
-  const SegHdr h = parse_seg(payload, offsets[sgi]);
-  uint64_t acc = 0;
-  for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) acc += seg_value(words, h, k);
-  acc = (uint64_t)block_reduce<5>((u128)acc, red);
-  if (threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long *>(d_sum), (unsigned long long)acc);
-}
-
 }  // namespace leco
 
 using namespace leco;
@@ -457,18 +476,8 @@ int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, cons
   uint32_t *err = nullptr;
   int rc = leco::device_error_word(&err);
   if (rc) return rc;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int smem = (int)(2 * kVarStageBytes);
-  cudaFuncSetAttribute(varlen_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_decode_kernel, 256, smem);
-  const uint64_t nitems = (nseg + kVarGroup - 1) / kVarGroup;
-  const unsigned grid = (unsigned)umin64(nitems, (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1));
-  varlen_decode_kernel<<<grid, 256, smem, reinterpret_cast<cudaStream_t>(stream)>>>(d_payload, d_offsets, d_starts, nseg, n,
-                                                                                  d_out, kVarStageBytes, err);
-  cudaError_t e = cudaGetLastError();
+  const cudaError_t e = launch_varlen_staged<false>(d_payload, d_offsets, d_starts, nseg, n, d_out, err, nullptr,
+                                                     reinterpret_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_decode: ") + cudaGetErrorString(e));
 }
 
@@ -495,8 +504,10 @@ int leco_varlen_sum(const uint8_t *d_payload, const uint64_t *d_offsets, const u
   if (!d_payload || !d_offsets || !d_starts || !nseg || !d_sum) return verr(LECO_ERR_ARG, "leco_varlen_sum: null pointer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(d_sum, 0, 8, st);
-  if (e == cudaSuccess) varlen_sum_kernel<<<(unsigned)nseg, 256, 0, st>>>(d_payload, d_offsets, d_starts, nseg, n, d_sum);
-  if (e == cudaSuccess) e = cudaGetLastError();
+  uint32_t *err = nullptr;
+  int rc = leco::device_error_word(&err);
+  if (rc) return rc;
+  if (e == cudaSuccess) e = launch_varlen_staged<true>(d_payload, d_offsets, d_starts, nseg, n, nullptr, err, d_sum, st);
   return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_sum: ") + cudaGetErrorString(e));
 }
 
