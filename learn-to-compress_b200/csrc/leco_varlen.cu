@@ -34,8 +34,76 @@ struct VarArgs {
   uint32_t *ticket;
   uint32_t *error;
   int exact_fit;
-  uint32_t max_seg;  // longest segment of this partition (sizes the shared-memory stage)
+  uint32_t max_seg;           // longest segment of this partition (sizes the shared-memory stage)
+  const double *seq_models;   // [nseg * 2] reference fits (theta0, theta1) of segments of >= 3 values, or null
 };
+
+// The reference's sequential fits of the segments (lr_int_T::caltheta, lr.h:66-85,
+// called by newsegment, :140-148), one lane per segment, one warp per 32
+// consecutive segments: each step the warp loads a tile of 32 values of each of
+// its 32 segments (every row contiguous in memory) into shared memory, and lane
+// j adds row j to its running sums in order.  sumx and sumxx are not summed:
+// every partial sum of i and of i*i is an integer below 2^53, so they equal their
+// closed forms.  Segments that are malformed (empty or longer than 16384 values)
+// are skipped; the encoder reports them.
+__global__ void __launch_bounds__(128) varlen_seq_fit_kernel(const uint64_t *__restrict__ values, uint64_t n,
+                                                             const uint64_t *__restrict__ starts, uint64_t nseg,
+                                                             double *__restrict__ models) {
+  __shared__ uint64_t tile[4][32][33];
+  __shared__ uint64_t rst[4][32];
+  __shared__ uint32_t rlen[4][32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t s0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+  if (s0 >= nseg) return;
+  const uint64_t mine = s0 + lane;
+  uint64_t st = 0;
+  uint32_t len = 0;
+  if (mine < nseg) {
+    st = __ldg(starts + mine);
+    const uint64_t en = mine + 1 < nseg ? __ldg(starts + mine + 1) : n;
+    len = (en > st && en <= n && en - st <= kVarlenMaxSeg) ? (uint32_t)(en - st) : 0;
+  }
+  rst[w][lane] = st;
+  rlen[w][lane] = len;
+  uint32_t maxlen = len;
+  for (int m = 16; m; m >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
+  __syncwarp();
+  double sy = 0, sxy = 0;
+  for (uint32_t t0 = 0; t0 < maxlen; t0 += 32) {
+    const uint32_t i = t0 + lane;
+#pragma unroll 8
+    for (int r = 0; r < 32; ++r) tile[w][r][lane] = i < rlen[w][r] ? __ldg(values + rst[w][r] + i) : 0ull;
+    __syncwarp();
+    const uint32_t cnt = len > t0 ? (len - t0 < 32 ? len - t0 : 32) : 0;
+    const uint64_t *row = &tile[w][lane][0];
+    if (cnt == 32) {
+      double y[32];
+#pragma unroll
+      for (uint32_t c = 0; c < 32; ++c) y[c] = __ull2double_rn(row[c]);
+#pragma unroll
+      for (uint32_t c = 0; c < 32; ++c) {
+        sy = __dadd_rn(sy, y[c]);
+        sxy = __dadd_rn(sxy, __dmul_rn(__uint2double_rn(t0 + c), y[c]));
+      }
+    } else {
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const double yi = __ull2double_rn(row[c]);
+        sy = __dadd_rn(sy, yi);
+        sxy = __dadd_rn(sxy, __dmul_rn(__uint2double_rn(t0 + c), yi));
+      }
+    }
+    __syncwarp();
+  }
+  if (len < 3) return;
+  const uint64_t m = len;
+  const double md = __uint2double_rn(len);
+  const double sumx = __ull2double_rn(m * (m - 1) / 2), sumxx = __ull2double_rn((m - 1) * m * (2 * m - 1) / 6);
+  const double ccc = __dsub_rn(__dmul_rn(sxy, md), __dmul_rn(sumx, sy));
+  const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+  const double th1 = __ddiv_rn(ccc, xxx);
+  models[mine * 2 + 0] = __ddiv_rn(__dsub_rn(sy, __dmul_rn(th1, sumx)), md);
+  models[mine * 2 + 1] = th1;
+}
 
 __device__ __forceinline__ uint64_t seg_bytes(uint32_t l, uint32_t len) {
   if (len == 1) return 13;
@@ -92,21 +160,9 @@ __global__ void __launch_bounds__(256) varlen_encode_kernel(VarArgs a) {
         s_model[1] = th1;
         s_model[0] = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(th1, sumx)), md);
       }
-    } else if (tid == 0) {  // lr_int_T::caltheta, the reference's sequential FP64 loop (lr.h:66-85)
-      double sumx = 0, sumy = 0, sumxx = 0, sumxy = 0;
-      for (uint32_t i = 0; i < len; ++i) {
-        const double di = __uint2double_rn(i), yi = __ull2double_rn(vals[i]);
-        sumx = __dadd_rn(sumx, di);
-        sumy = __dadd_rn(sumy, yi);
-        sumxx = __dadd_rn(sumxx, __dmul_rn(di, di));
-        sumxy = __dadd_rn(sumxy, __dmul_rn(di, yi));
-      }
-      const double md = __uint2double_rn(len);
-      const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
-      const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
-      const double th1 = __ddiv_rn(ccc, xxx);
-      s_model[1] = th1;
-      s_model[0] = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(th1, sumx)), md);
+    } else if (tid == 0) {  // the reference's sequential fit, from varlen_seq_fit_kernel
+      s_model[0] = a.seq_models[sgi * 2 + 0];
+      s_model[1] = a.seq_models[sgi * 2 + 1];
     }
     __syncthreads();
     t0 = s_model[0];
@@ -440,7 +496,7 @@ int verr(int code, const std::string &m) { return leco::record_error(code, m); }
 extern "C" {
 
 uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg) { return 8 * n + 32 * nseg + LECO_PAYLOAD_SLACK; }
-uint64_t leco_varlen_workspace_bytes(uint64_t nseg) { return (nseg * 8 + 255) / 256 * 256 + 256; }
+uint64_t leco_varlen_workspace_bytes(uint64_t nseg) { return (nseg * 8 + 255) / 256 * 256 + 256 + (nseg * 16 + 255) / 256 * 256; }
 uint64_t leco_varlen_max_segment(void) { return kVarlenMaxSeg; }
 
 int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_starts, uint64_t nseg, uint32_t max_segment_len,
@@ -459,9 +515,12 @@ int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_s
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   uint8_t *ws = static_cast<uint8_t *>(d_workspace);
   const uint64_t status_bytes = (nseg * 8 + 255) / 256 * 256;
+  const bool exact = fit_mode == LECO_FIT_EXACT;
+  double *models = reinterpret_cast<double *>(ws + status_bytes + 256);  // workspace: status, ticket, models
   VarArgs a{d_values, n, d_starts, nseg, d_payload, payload_cap, d_offsets, reinterpret_cast<uint64_t *>(ws),
-            reinterpret_cast<uint32_t *>(ws + status_bytes), err, fit_mode == LECO_FIT_EXACT, max_segment_len};
+            reinterpret_cast<uint32_t *>(ws + status_bytes), err, exact, max_segment_len, exact ? nullptr : models};
   cudaError_t e = cudaMemsetAsync(ws, 0, status_bytes + 256, st);
+  if (e == cudaSuccess && !exact) varlen_seq_fit_kernel<<<(unsigned)((nseg + 127) / 128), 128, 0, st>>>(d_values, n, d_starts, nseg, models);
   const int smem = 8 * max_segment_len + (max_segment_len / 32 + 9) * 4;
   if (e == cudaSuccess && smem > 48 * 1024)
     e = cudaFuncSetAttribute(varlen_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
