@@ -40,9 +40,10 @@ struct VarArgs {
 
 // The reference's sequential fits of the segments (lr_int_T::caltheta, lr.h:66-85,
 // called by newsegment, :140-148), one lane per segment, one warp per 32
-// consecutive segments: each step the warp loads a tile of 32 values of each of
-// its 32 segments (every row contiguous in memory) into shared memory, and lane
-// j adds row j to its running sums in order.  sumx and sumxx are not summed:
+// consecutive segments: each step the warp moves a tile of 32 values of each of
+// its 32 segments (every row contiguous in memory) into shared memory, with the
+// next tile already in flight to registers, and lane j adds row j to its running
+// sums in order.  sumx and sumxx are not summed:
 // every partial sum of i and of i*i is an integer below 2^53, so they equal their
 // closed forms.  Segments that are malformed (empty or longer than 16384 values)
 // are skipped; the encoder reports them.
@@ -68,22 +69,33 @@ __global__ void __launch_bounds__(128) varlen_seq_fit_kernel(const uint64_t *__r
   uint32_t maxlen = len;
   for (int m = 16; m; m >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
   __syncwarp();
-  double sy = 0, sxy = 0;
-  for (uint32_t t0 = 0; t0 < maxlen; t0 += 32) {
+  // the next tile's 32 rows are in flight to registers while the current one is summed
+  uint64_t nxt[32];
+  auto fetch = [&](uint32_t t0) {
     const uint32_t i = t0 + lane;
-#pragma unroll 8
-    for (int r = 0; r < 32; ++r) tile[w][r][lane] = i < rlen[w][r] ? __ldg(values + rst[w][r] + i) : 0ull;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) nxt[r] = i < rlen[w][r] ? __ldg(values + rst[w][r] + i) : 0ull;
+  };
+  double sy = 0, sxy = 0;
+  fetch(0);
+  for (uint32_t t0 = 0; t0 < maxlen; t0 += 32) {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) tile[w][r][lane] = nxt[r];
     __syncwarp();
+    if (t0 + 32 < maxlen) fetch(t0 + 32);
     const uint32_t cnt = len > t0 ? (len - t0 < 32 ? len - t0 : 32) : 0;
     const uint64_t *row = &tile[w][lane][0];
     if (cnt == 32) {
-      double y[32];
 #pragma unroll
-      for (uint32_t c = 0; c < 32; ++c) y[c] = __ull2double_rn(row[c]);
+      for (uint32_t h = 0; h < 32; h += 16) {  // 16 conversions issued ahead of their adds
+        double y[16];
 #pragma unroll
-      for (uint32_t c = 0; c < 32; ++c) {
-        sy = __dadd_rn(sy, y[c]);
-        sxy = __dadd_rn(sxy, __dmul_rn(__uint2double_rn(t0 + c), y[c]));
+        for (uint32_t c = 0; c < 16; ++c) y[c] = __ull2double_rn(row[h + c]);
+#pragma unroll
+        for (uint32_t c = 0; c < 16; ++c) {
+          sy = __dadd_rn(sy, y[c]);
+          sxy = __dadd_rn(sxy, __dmul_rn(__uint2double_rn(t0 + h + c), y[c]));
+        }
       }
     } else {
       for (uint32_t c = 0; c < cnt; ++c) {
@@ -169,14 +181,26 @@ __global__ void __launch_bounds__(256) varlen_encode_kernel(VarArgs a) {
     slope = __double2float_rn(s_model[1]);  // float final_slope = mylr.theta1 (:148)
     t1d = (double)slope;
     uint64_t rmax = 0;
+    // Predictions are monotone in i, so the two ends bound them; when all lie in
+    // [0, 2^63) the 128-bit residual of :158-166 is the 64-bit one.
+    const double pe0 = __dadd_rn(t0, __dmul_rn(t1d, 0.0)), pe1 = __dadd_rn(t0, __dmul_rn(t1d, __uint2double_rn(len - 1)));
+    const bool u64pred = pe0 >= 0.0 && pe1 >= 0.0 && pe0 < 9223372036854775808.0 && pe1 < 9223372036854775808.0;
     for (uint32_t i0 = 0; i0 < len; i0 += nt) {
       const uint32_t i = i0 + tid;
       bool pos = false;
       if (i < len) {
-        const i128 pred = f2i128(__dadd_rn(t0, __dmul_rn(t1d, __uint2double_rn(i))));
-        const i128 y = (i128)vals[i];
-        pos = y > pred;
-        const uint64_t r = (uint64_t)(pos ? y - pred : pred - y);
+        const double p = __dadd_rn(t0, __dmul_rn(t1d, __uint2double_rn(i)));
+        uint64_t r;
+        if (u64pred) {
+          const uint64_t pred = __double2ull_rz(p), y = vals[i];
+          pos = y > pred;
+          r = pos ? y - pred : pred - y;
+        } else {
+          const i128 pred = f2i128(p);
+          const i128 y = (i128)vals[i];
+          pos = y > pred;
+          r = (uint64_t)(pos ? y - pred : pred - y);
+        }
         vals[i] = r;
         rmax = r > rmax ? r : rmax;
       }
@@ -524,7 +548,7 @@ int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_s
   const int smem = 8 * max_segment_len + (max_segment_len / 32 + 9) * 4;
   if (e == cudaSuccess && smem > 48 * 1024)
     e = cudaFuncSetAttribute(varlen_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) varlen_encode_kernel<<<(unsigned)nseg, 256, smem, st>>>(a);
+  if (e == cudaSuccess) varlen_encode_kernel<<<(unsigned)nseg, 128, smem, st>>>(a);  // 128 threads: more segments in flight per SM
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? LECO_OK : verr(LECO_ERR_CUDA, std::string("leco_varlen_encode: ") + cudaGetErrorString(e));
 }
