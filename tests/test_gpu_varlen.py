@@ -74,6 +74,52 @@ def test_varlen_short_and_raw_segments(lc, orc, dev):
     lc.check()
 
 
+def test_varlen_decode_paths_large(lc, orc, dev):
+    """A column whose segment items take every decoder path: narrow segments
+    decoded from the staged copy, runs of wide-residual segments whose eight-image
+    items exceed the staging buffer (decoded from global memory), raw and
+    one/two-value segments, and a segment count not a multiple of eight; decoded
+    into an aligned and an 8-byte-offset output, summed and sampled at random."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    parts, starts, pos = [], [], 0
+    for k in range(400):
+        kind = k % 10
+        if kind < 5:    # narrow: slope + small noise
+            ln = int(rng.integers(500, 2000))
+            seg = 10 ** 9 + 37 * pos + np.arange(ln) * 11 + rng.integers(0, 64, ln)
+        elif kind < 8:  # wide residuals (about 40 bits): items of these exceed the buffer
+            ln = int(rng.integers(1500, 2000))
+            seg = 2 ** 50 + rng.integers(0, 2 ** 40, ln)
+        elif kind == 8:  # raw
+            ln = int(rng.integers(30, 300))
+            seg = rng.integers(0, 2 ** 64 - 1, ln, dtype=np.uint64)
+        else:            # one or two values
+            ln = 1 + (k // 10) % 2
+            seg = rng.integers(0, 2 ** 60, ln)
+        starts.append(pos)
+        parts.append(np.asarray(seg, dtype=np.uint64))
+        pos += ln
+    x = np.concatenate(parts)
+    n = len(x)
+    starts = np.array(starts, np.uint64)
+    xd = _dev(x, dev)
+    col = lc.varlen_encode(xd, starts, lc.FIT_REFERENCE)
+    pay, off, _ = col.to_host()
+    ends = list(starts[1:]) + [n]
+    for s in range(0, len(starts), 13):
+        assert pay[off[s]:off[s + 1]].tobytes() == orc.varseg_encode(x, int(starts[s]), int(ends[s]) - 1), s
+    assert torch.equal(col.decode(), xd)
+    buf = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    col.decode(out=buf[1:])
+    assert torch.equal(buf[1:], xd) and int(buf[0]) == 0
+    assert col.sum() == int(x.sum(dtype=np.uint64))
+    idx = torch.from_numpy(rng.integers(0, n, 1 << 16).astype(np.int64)).to(dev)
+    assert torch.equal(col.gather(idx), xd[idx])
+    lc.check()
+
+
 def _starts(t):
     return t.cpu().numpy().view(np.uint64)
 
