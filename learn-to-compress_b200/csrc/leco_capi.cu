@@ -447,6 +447,16 @@ int leco_encode_host(int codec, int dtype, const void *h_values, uint64_t n, uin
 // Decodes a host column in chunks of whole blocks on two streams, so the
 // host->device copy of one chunk, the decode of another and the device->host
 // copy of a third overlap.
+}  // extern "C"
+
+// Chunk-relative offsets on the device: off[0..cnt] -= base.
+__global__ void rebase_offsets_kernel(uint64_t *off, uint64_t cnt, uint64_t base) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= cnt; k += (uint64_t)gridDim.x * blockDim.x)
+    off[k] -= base;
+}
+
+extern "C" {
+
 int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
                      uint32_t block_size, void *h_out) {
   int rc = check_column("leco_decode_host", codec, dtype, h_payload, h_offsets, block_size);
@@ -455,10 +465,12 @@ int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint6
   const uint64_t nb = leco_num_blocks(n, block_size);
   if (!nb) return LECO_OK;
   const uint64_t total = h_offsets[nb];
-  // chunk = ~64 MiB of decoded values, whole blocks
-  uint64_t bpc = std::max<uint64_t>(1, (64ull << 20) / ((uint64_t)block_size * dtype));
+  // chunk = ~32 MiB of decoded values, whole blocks; four streams keep the
+  // device->host copies queued back to back even when this thread is slow to
+  // enqueue the next chunk
+  uint64_t bpc = std::max<uint64_t>(1, (32ull << 20) / ((uint64_t)block_size * dtype));
   bpc = std::min(bpc, nb);
-  const int NS = 2;
+  const int NS = 4;
   cudaStream_t st[NS];
   for (int i = 0; i < NS; ++i) LECO_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
   DevBuf pay[NS], off[NS], out[NS];
@@ -472,18 +484,17 @@ int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint6
         out[i].alloc(bpc * block_size * (uint64_t)dtype, st[i]))
       rc = fail(LECO_ERR_NOMEM, "leco_decode_host: device allocation failed");
   }
-  std::vector<std::vector<uint64_t>> rel(NS, std::vector<uint64_t>(bpc + 1));
   uint64_t chunk = 0;
   for (uint64_t b0 = 0; b0 < nb && !rc; b0 += bpc, ++chunk) {
     const int i = (int)(chunk % NS);
     cudaStream_t s = st[i];
     const uint64_t b1 = std::min(nb, b0 + bpc), cb = b1 - b0;
     const uint64_t pbase = h_offsets[b0] & ~7ull;  // keep the 8-byte word alignment of bit addresses
-    cudaStreamSynchronize(s);                       // rel[i] and the buffers are reused
-    for (uint64_t b = 0; b <= cb; ++b) rel[i][b] = h_offsets[b0 + b] - pbase;
+    cudaStreamSynchronize(s);                       // the buffers are reused
     const uint64_t nbytes = h_offsets[b1] - pbase;
     cudaMemcpyAsync(pay[i].p, h_payload + pbase, std::min<uint64_t>(nbytes + 8, total - pbase), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(off[i].p, rel[i].data(), (cb + 1) * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(off[i].p, h_offsets + b0, (cb + 1) * 8, cudaMemcpyHostToDevice, s);
+    rebase_offsets_kernel<<<(unsigned)std::min<uint64_t>((cb + 256) / 256, 64), 256, 0, s>>>((uint64_t *)off[i].p, cb, pbase);
     const uint64_t v0 = b0 * block_size, nv = std::min<uint64_t>(n, b1 * block_size) - v0;
     rc = leco_decode(codec, dtype, (const uint8_t *)pay[i].p, (const uint64_t *)off[i].p, nv, block_size, out[i].p,
                      reinterpret_cast<leco_stream_t>(s));
