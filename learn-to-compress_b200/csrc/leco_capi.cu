@@ -87,6 +87,12 @@ static bool needs_seq_fit(int codec, int dtype, uint32_t bs, int fit_mode) {
   return codec == kPoly2;
 }
 
+// Chunk-relative offsets on the device (leco_decode_host): off[0..cnt] -= base.
+__global__ void rebase_offsets_kernel(uint64_t *off, uint64_t cnt, uint64_t base) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= cnt; k += (uint64_t)gridDim.x * blockDim.x)
+    off[k] -= base;
+}
+
 }  // namespace leco
 
 using namespace leco;
@@ -444,19 +450,9 @@ int leco_encode_host(int codec, int dtype, const void *h_values, uint64_t n, uin
   return rc;
 }
 
-// Decodes a host column in chunks of whole blocks on two streams, so the
+// Decodes a host column in chunks of whole blocks on four streams, so the
 // host->device copy of one chunk, the decode of another and the device->host
 // copy of a third overlap.
-}  // extern "C"
-
-// Chunk-relative offsets on the device: off[0..cnt] -= base.
-__global__ void rebase_offsets_kernel(uint64_t *off, uint64_t cnt, uint64_t base) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= cnt; k += (uint64_t)gridDim.x * blockDim.x)
-    off[k] -= base;
-}
-
-extern "C" {
-
 int leco_decode_host(int codec, int dtype, const uint8_t *h_payload, const uint64_t *h_offsets, uint64_t n,
                      uint32_t block_size, void *h_out) {
   int rc = check_column("leco_decode_host", codec, dtype, h_payload, h_offsets, block_size);
