@@ -243,6 +243,8 @@ int leco_varlen_partition_device(const uint64_t *d_values, uint64_t n, uint32_t 
                                  uint64_t *d_starts, uint64_t starts_cap, uint64_t *d_nseg, void *d_ws, uint64_t ws_bytes,
                                  leco_stream_t stream);
 uint64_t leco_varlen_max_payload_bytes(uint64_t n, uint64_t nseg);
+/* Device workspace of leco_varlen_encode: the look-back status words and ticket,
+ * and for LECO_FIT_REFERENCE the segments' sequential fits (16 bytes a segment). */
 uint64_t leco_varlen_workspace_bytes(uint64_t nseg);
 /* Longest segment leco_varlen_encode accepts (values). */
 uint64_t leco_varlen_max_segment(void);
