@@ -34,6 +34,7 @@ N_DEFAULT = 200_000_000
 BS = 4096
 RA_BATCH = 1 << 24
 DECODE_KERNEL = "decode_staged_kernel"
+RA_DRAM_BYTES = 8 + 8 + 32  # per lookup: index, value, one payload sector (directory L2-resident)
 
 
 def parse():
@@ -45,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter"],
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter", "gather"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
@@ -65,9 +66,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the decode kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "decode_staged_kernel_leco_u64_200M.txt")
+def profile_traffic(name: str = "decode_staged_kernel_leco_u64_200M.txt"):
+    """Per-launch DRAM bytes of a kernel at the bench's full size, from its
+    committed ncu summary (line `traffic_bytes_per_launch_full_size:`)."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -81,7 +83,7 @@ def profile_traffic():
 
 class ClockSampler:
     """Samples SM clocks and clock-event (throttle) reasons through NVML every
-    few milliseconds while the timed region runs (falls back to nvidia-smi)."""
+    few milliseconds while the timed region runs."""
 
     REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
@@ -130,93 +132,130 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_reference_decode(x: np.ndarray, bs: int, threads: int, budget_s: float = 10.0):
-    """Times the compiled reference headers (oracle/_ref): Leco_int<uint64_t>
-    encodeArray8_int per block once, then decodeArray8 over all blocks with
-    `threads` host threads, repeated until `budget_s` elapses.  Returns
-    (GB/s of decoded bytes, kind, sample description, ratio)."""
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def decode_config(n: int, world: int) -> dict:
+    """The decode workload's config; both arms (this library and --impl
+    reference) print exactly this dict."""
+    return {"workload": f"leco_fix u64 {n / 1e6:g}M piecewise-linear sorted keys, {BS}-value blocks, "
+                        f"bulk decode + 2^{RA_BATCH.bit_length() - 1} uniform random lookups per step",
+            "keys_per_gpu": n, "block_size": BS, "blocks": (n + BS - 1) // BS, "ra_batch": RA_BATCH,
+            "l2": "inputs and outputs larger than L2 (no flush needed)", "parallelism": f"shard{world}",
+            "generator_seed": 2}
+
+
+def reference_lib():
+    """The compiled reference headers (oracle/_ref), or None if not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    if os.path.exists(oracle.REF_SO):
-        R, kind = oracle.Reference(), "reference"
-    else:
-        R, kind = None, "port"
-    s = x.dtype.itemsize
-    if R is not None:
-        pay, off = R.encode_column(0, x, bs)
-    else:
-        O = oracle.Oracle()
-        pay, off = O.encode_column(0, x, bs)
+    return oracle.Reference() if os.path.exists(oracle.REF_SO) else None
+
+
+def cpu_reference_baseline(R, x: np.ndarray, pay: np.ndarray, off: np.ndarray, threads: int, budget_s: float = 6.0):
+    """Times the compiled reference (Leco_int<uint64_t>::decodeArray8 per block,
+    randomdecodeArray8 per index) on the workload's whole column, as the
+    reference's drivers run it (experiments/leco_int_fix_template.cpp:142-153
+    bulk decode, :180-213 random access): (ii) `threads` host threads over
+    disjoint block / index ranges, repeated for about `budget_s`; (i) one
+    thread.  Every run is checked against the input."""
+    n = len(x)
+    padded = R.pad(pay)
+    out = np.empty(n + 64, np.uint64)
+    rng = np.random.default_rng(7)
+    idx = rng.integers(0, n, 1 << 22).astype(np.uint64)
+    rout = np.empty(len(idx), np.uint64)
+    R.decode_column(0, padded, off, n, 8, BS, threads=threads, out=out, padded=True)  # warm the pages
     reps, t0 = 0, time.perf_counter()
     while True:
-        if R is not None:
-            y = R.decode_column(0, pay, off, len(x), s, bs, threads=threads)
-        else:
-            y = oracle.Oracle().decode_column(0, pay, off, len(x), s, bs)
+        R.decode_column(0, padded, off, n, 8, BS, threads=threads, out=out, padded=True)
         reps += 1
         el = time.perf_counter() - t0
-        if el > budget_s or reps >= 5000:
+        if el > budget_s or reps >= 1000:
             break
-    assert np.array_equal(y, x), "reference decode mismatch"
-    gbs = reps * len(x) * s / el / 1e9
-    sample = f"{len(x)/1e6:.0f}M keys of the same generator, {reps} full decodes in {el:.1f}s"
-    return gbs, kind, sample, len(pay) / (len(x) * s), pay, off
-
-
-def cpu_reference_random(pay, off, x, bs, threads, m=4_000_000):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    R = oracle.Reference()
-    rng = np.random.default_rng(7)
-    idx = rng.integers(0, len(x), m).astype(np.uint64)
+    assert np.array_equal(out[:n], x), "reference decode mismatch"
+    gbs = reps * n * 8 / el / 1e9
     t0 = time.perf_counter()
-    y = R.random_column(0, pay, off, 8, bs, idx, threads=threads)
-    el = time.perf_counter() - t0
-    assert np.array_equal(y, x[idx])
-    return m / el / 1e6
+    R.random_column(0, padded, off, 8, BS, idx, threads=threads, out=rout, padded=True)
+    ra = len(idx) / (time.perf_counter() - t0) / 1e6
+    assert np.array_equal(rout, x[idx.astype(np.int64)]), "reference random access mismatch"
+    # (i) one thread, the reference drivers' own loop structure
+    t1 = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        R.decode_column(0, padded, off, n, 8, BS, threads=1, out=out, padded=True)
+        t1.append(time.perf_counter() - t0)
+    assert np.array_equal(out[:n], x), "reference decode mismatch"
+    m1 = 1 << 20
+    t0 = time.perf_counter()
+    R.random_column(0, padded, off, 8, BS, idx[:m1], threads=1, out=rout, padded=True)
+    ra1 = m1 / (time.perf_counter() - t0) / 1e6
+    assert np.array_equal(rout[:m1], x[idx[:m1].astype(np.int64)])
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+            "sample": f"the whole {n / 1e6:g}M-key column, {reps} full decodes in {el:.1f}s on {threads} threads; "
+                      f"{len(idx)} random lookups",
+            "ra_mlookups_s": round(ra, 2),
+            "single_thread": {"value": round(n * 8 / min(t1) / 1e9, 3), "unit": "GB/s", "cores": 1,
+                              "ra_mlookups_s": round(ra1, 2),
+                              "sample": f"the whole column decoded twice (best of 2) and {m1} random lookups on one "
+                                        "thread, the reference drivers' per-block and per-index loops"}}
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference's CPU codec on the host cores."""
+    """--impl reference: the reference's CPU codec (the unmodified headers,
+    compiled into oracle/_ref) on the host cores, on the same column as this
+    library's rank-0 arm: each step is one bulk decode of the whole column
+    and one batch of 2^24 uniform random lookups, on all host threads."""
     if rank != 0:
         return
     from leco_b200 import workloads
 
-    threads = os.cpu_count() or 1
-    n = min(args.n, 50_000_000)  # bounded sample of the same workload
-    x = workloads.piecewise_linear_u64(n, seed=2).numpy().view(np.uint64)
-    times = []
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    if not os.path.exists(oracle.REF_SO):
+    R = reference_lib()
+    if R is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libleco_ref.so was not built"}))
         return
-    R = oracle.Reference()
-    pay, off = R.encode_column(0, x, BS)
+    threads = host_threads()
+    n = args.n
+    x = workloads.piecewise_linear_u64(n, seed=2).numpy().view(np.uint64)
+    pay, off = R.encode_column(0, x, BS, threads=threads)
+    padded = R.pad(pay)
+    out = np.empty(n + 64, np.uint64)
+    rng = np.random.default_rng(11)
+    idx_sets = [rng.integers(0, n, RA_BATCH).astype(np.uint64) for _ in range(2)]
+    rout = np.empty(RA_BATCH, np.uint64)
+    dec, ra = [], []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        y = R.decode_column(0, pay, off, n, 8, BS, threads=threads)
-        el = time.perf_counter() - t0
+        R.decode_column(0, padded, off, n, 8, BS, threads=threads, out=out, padded=True)
+        t1 = time.perf_counter()
+        R.random_column(0, padded, off, 8, BS, idx_sets[i % 2], threads=threads, out=rout, padded=True)
+        t2 = time.perf_counter()
         if i >= args.warmup:
-            times.append(el)
-    assert np.array_equal(y, x)
-    ms = float(np.mean(times)) * 1e3
-    gbs = n * 8 / (ms / 1e3) / 1e9
-    ra = cpu_reference_random(pay, off, x, BS, threads)
-    sample = f"{n/1e6:.0f}M keys of the 200M-key generator (bounded sample), {threads} threads"
-    out = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-           "config": {"workload": "leco_fix u64 piecewise-linear sorted keys, 4096-value blocks", "keys": n,
-                      "block_size": BS, "threads": threads},
-           "ra_mlookups_s": round(ra, 2),
-           "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
-                            "sample": sample},
-           "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out), flush=True)
+            dec.append(t1 - t0)
+            ra.append(t2 - t1)
+    assert np.array_equal(out[:n], x), "reference decode mismatch"
+    last = idx_sets[(args.warmup + args.steps - 1) % 2]
+    assert np.array_equal(rout, x[last.astype(np.int64)]), "reference random access mismatch"
+    dec_s, ra_s = float(np.mean(dec)), float(np.mean(ra))
+    gbs = n * 8 / dec_s / 1e9
+    base = cpu_reference_baseline(R, x, pay, off, threads, budget_s=3.0)
+    cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+           "sample": f"the whole {n / 1e6:g}M-key column per step ({args.steps} timed steps, {threads} threads)",
+           "single_thread": base["single_thread"]}
+    out_line = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round((dec_s + ra_s) * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": decode_config(n, world),
+                "decode_ms": round(dec_s * 1e3, 3), "ra_mlookups_s": round(RA_BATCH / ra_s / 1e6, 2),
+                "compressed_ratio": round(len(pay) / (n * 8), 5),
+                "cpu_baseline": cpu,
+                "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out_line), flush=True)
 
 
 def run_batch(args, world, rank, local):
@@ -234,15 +273,9 @@ def run_batch(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    rng = np.random.default_rng(3 + rank)
-    fams = autotune.FAMILIES
     cols, raw, shapes = [], 0, {}
-    for i in range(args.ncols):
-        n = int(math.exp(rng.uniform(math.log(1000), math.log(4_000_000))))
-        s = 4 if rng.random() < 0.5 else 8
-        fam = fams[int(rng.integers(4))]
-        codec = (lc.LINEAR, lc.DELTA, lc.FOR)[int(rng.integers(3))]
-        x = workloads.families(n, fam, s, rng)
+    for x, codec, _ in workloads.batch_columns(args.ncols, seed=3 + rank):
+        s, n = x.dtype.itemsize, len(x)
         bs = autotune.pick_block_size(codec, s, n, autotune.classify(x))
         shapes[bs] = shapes.get(bs, 0) + 1
         cols.append((torch.from_numpy(x.view(np.int64 if s == 8 else np.int32)).to(dev), codec, bs))
@@ -323,7 +356,7 @@ def run_serve(args, world, rank, local):
     dev = torch.device("cuda", local)
     raws, cols = [], []
     for c in range(args.serve_cols):
-        x = workloads.piecewise_linear_u64(args.serve_n, seed=100 + c + 1000 * rank, device=dev)
+        x = workloads.piecewise_linear_u64(args.serve_n, seed=100 + c + 1000 * rank, device=dev, noise_on="device")
         cols.append(lc.encode(x, lc.LINEAR, BS, lc.FIT_EXACT).compact())
         raws.append(x)
     torch.cuda.synchronize()
@@ -433,6 +466,7 @@ def run_varlen(args, world, rank, local):
     idx = torch.randint(0, n, (RA_BATCH,), device=dev)
     ra = torch.empty(RA_BATCH, dtype=torch.int64, device=dev)
     res = {}
+    clk = ClockSampler(local).__enter__()
     res["varlen"] = {
         "segments": int(len(starts)), "partition_host_s": round(t_part, 3), "host_threads": os.cpu_count(),
         "partition_gpu_ms": round(t_part_dev, 2),
@@ -455,6 +489,7 @@ def run_varlen(args, world, rank, local):
     res["poly2_8192"]["sum_ms"] = round(ev_time(lambda: pc.sum()), 3)
     res["poly2_8192"]["compressed_ratio"] = round(pc.nbytes / (8 * n), 5)
     assert torch.equal(pc.decode(out=out), x) and torch.equal(pc.gather(idx, out=ra), x[idx])
+    clk.__exit__(None, None, None)
     assert pc.sum() == int(x.sum().item()) & 0xFFFFFFFFFFFFFFFF
     lc.check()
     for k in res:
@@ -469,7 +504,7 @@ def run_varlen(args, world, rank, local):
                 "vs_baseline": None, "dtype": "u64", "data": "synthetic",
                 "config": {"workload": f"{n} u64 regime-switching (linear/quadratic/flat, sigma 2^8); varlen: coarse "
                                        "blocks of 2000, delta 12; poly2: 8192-value blocks", "keys": n},
-                **res}
+                "clocks": clk.summary(), **res}
         print(json.dumps(line), flush=True)
 
 
@@ -570,6 +605,59 @@ def run_filter(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_gather(args, world, rank, local):
+    """Random access alone on the decode workload's column (200M u64 keys,
+    LeCo-fix, 4096-value blocks): the column is encoded, the keys and every
+    temporary are released, and each step is one batch of 2^24 uniform
+    lookups.  The device then holds only the compressed column, its directory,
+    the index sets and the output (under 1 GB), which keeps an ncu capture of
+    the gather kernel at the full column size small."""
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    x = workloads.piecewise_linear_u64(n, seed=2 + rank, device=dev)
+    col = lc.encode(x, lc.LINEAR, BS, lc.FIT_REFERENCE).compact()
+    idx_sets = [torch.randint(0, n, (RA_BATCH,), device=dev, dtype=torch.int64) for _ in range(2)]
+    want = [x[i] for i in idx_sets]
+    del x
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    out = torch.empty(RA_BATCH, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream()
+    for i in range(max(3, args.warmup)):
+        col.gather(idx_sets[i % 2], out=out)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            col.gather(idx_sets[i % 2], out=out)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    lc.check()
+    assert torch.equal(out, want[(args.steps - 1) % 2]), "random access mismatch"
+    ms = [a.elapsed_time(b) for a, b in ev]
+    mean = float(np.mean(ms))
+    peak, _ = peaks()
+    if rank == 0:
+        ach = RA_BATCH * RA_DRAM_BYTES / (mean / 1e3) / 1e9
+        line = {"metric": "LeCo-fix batched random access on 200M u64 keys: Glookups/s",
+                "value": round(RA_BATCH / mean / 1e6, 2), "unit": "Glookups/s", "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": round(mean, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"{n} u64 piecewise-linear keys, LeCo-fix blocks of {BS}, 2^24 uniform lookups",
+                           "keys": n, "compressed_bytes": col.nbytes, "device_bytes_held": int(torch.cuda.memory_allocated())},
+                "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(ach / peak, 4), "algorithmic_bytes_per_lookup": RA_DRAM_BYTES},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+
+
 def to_np_u64(t):
     return t.cpu().numpy().view(np.uint64)
 
@@ -591,6 +679,9 @@ def main():
         return
     if args.workload == "filter":
         run_filter(args, world, rank, local)
+        return
+    if args.workload == "gather":
+        run_gather(args, world, rank, local)
         return
 
     import torch
@@ -682,6 +773,7 @@ def main():
     ra_rate = world * RA_BATCH / (ra_mean / 1e3) / 1e6
     peak, peak_kind = peaks()
     alg_bytes = comp + (col.nblocks + 1) * 8 + dec_bytes  # payload + offsets read, values written
+    ra_alg = RA_BATCH * RA_DRAM_BYTES
     achieved = alg_bytes / (dec_mean / 1e3) / 1e9
 
     # end-to-end through the public host-buffer API: pinned compressed bytes in,
@@ -726,15 +818,20 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        xs = x[: min(n, 20_000_000)].cpu().numpy().view(np.uint64)
-        threads = os.cpu_count() or 1
-        gbs, kind, sample, ref_ratio, rpay, roff = cpu_reference_decode(xs, BS, threads, budget_s=10.0)
-        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample,
-               "ratio_on_sample": round(ref_ratio, 5)}
-        # the GPU stream of the same sample is byte-identical to the reference's
-        gcol = lc.encode(x[: len(xs)].contiguous(), lc.LINEAR, BS, lc.FIT_REFERENCE)
-        gp, go = gcol.to_host()
-        cpu["gpu_stream_identical_on_sample"] = bool(np.array_equal(gp, rpay) and np.array_equal(go, roff))
+        R = reference_lib()
+        if R is None:
+            cpu = {"unavailable": "oracle/_ref/libleco_ref.so was not built"}
+        else:
+            # the same column through the reference on the host cores; its stream must be
+            # this library's, byte for byte, over the whole column
+            threads = host_threads()
+            xh = x.cpu().numpy().view(np.uint64)
+            rpay, roff = R.encode_column(0, xh, BS, threads=threads)
+            gp, go = col.to_host()
+            cpu = cpu_reference_baseline(R, xh, rpay, roff, threads)
+            cpu["gpu_stream_identical_full_column"] = bool(np.array_equal(go, roff) and np.array_equal(gp[: len(rpay)], rpay))
+            cpu["reference_compressed_ratio"] = round(len(rpay) / (n * 8), 5)
+            del xh, rpay, gp
 
     if rank == 0:
         clocks = clk.summary()
@@ -742,10 +839,7 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "leco_fix u64 200M piecewise-linear sorted keys, 4096-value blocks, "
-                                   "bulk decode + 2^24 uniform random lookups per step",
-                       "keys_per_gpu": n, "block_size": BS, "blocks": col.nblocks, "ra_batch": RA_BATCH,
-                       "l2": "inputs and outputs larger than L2 (no flush needed)", "parallelism": f"shard{world}"},
+            "config": decode_config(n, world),
             "decode_ms": round(dec_mean, 4),
             "ra_mlookups_s": round(ra_rate, 1),
             "ra_batch_p50_us": round(float(np.percentile(ra_ms, 50)) * 1e3, 1),
@@ -759,6 +853,15 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "kernel": DECODE_KERNEL, "algorithmic_bytes_per_launch": int(alg_bytes)},
+            "roofline_gather": {"bound": "hbm", "achieved": round(ra_alg / (ra_mean / 1e3) / 1e9, 1), "peak": peak,
+                                "unit": "GB/s", "frac": round(ra_alg / (ra_mean / 1e3) / 1e9 / peak, 4),
+                                "traffic": profile_traffic("gather_kernel_leco_u64_200M.txt"),
+                                "kernel": "gather_kernel",
+                                "algorithmic_bytes_per_lookup": RA_DRAM_BYTES,
+                                "algorithmic_bytes_per_launch": int(ra_alg),
+                                "note": "per lookup: 8 B index read + 8 B value written + one 32 B payload sector; "
+                                        "the 32 B directory sector is L2-resident (48,829 blocks x 32 B = 1.6 MB) "
+                                        "and not counted"},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * 2,

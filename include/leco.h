@@ -24,6 +24,9 @@
  * every call is asynchronous on `stream` unless documented otherwise; status 0 =
  * success, negative = error (leco_last_error() describes the last one on the
  * calling thread).  No call allocates device memory unless its comment says so.
+ * The library keeps per-device addresses of its own device variables (the error
+ * word, the built-in encoder scratch) from the first call on each device, so the
+ * device must not be reset (cudaDeviceReset) while the library is in use.
  */
 #ifndef LECO_B200_H_
 #define LECO_B200_H_
@@ -128,7 +131,8 @@ int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t
  * the array's device address (cudaGetSymbolAddress), so make that first call before any stream
  * capture.  Every call uses the same array and the scratch is re-zeroed by each call: calls whose
  * work overlaps on the GPU (different streams, no ordering between them) race and must not be
- * issued.  Allocates nothing. */
+ * issued.  Allocates nothing.  The resolved address belongs to the CUDA context of that
+ * first call: do not reset the device (cudaDeviceReset) while this library is in use. */
 int leco_encode_noalloc(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
                         uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
                         leco_stream_t stream);
@@ -438,7 +442,9 @@ int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t 
 /* Reads and clears the device error word (bad index, bad header, bounded-wait
  * timeout). Synchronous. Returns LECO_OK, LECO_ERR_CORRUPT or LECO_ERR_TIMEOUT. */
 int leco_check(leco_stream_t stream);
-/* Runs the encoder's look-back wait on a predecessor that never publishes, with
+/* TEST HOOK, not part of the codec interface (no counterpart in the reference):
+ * the failure-detection test calls it; applications have no use for it.
+ * Runs the encoder's look-back wait on a predecessor that never publishes, with
  * at most spin_limit polls (the encoder itself uses about 4 million, ~1-2 s), and
  * returns what leco_check reports afterwards: LECO_ERR_TIMEOUT when the bounded
  * wait gave up as designed (*h_result = ~0).  Synchronous; the context stays usable. */

@@ -143,10 +143,11 @@ class FOR_int : public LecoBlockCodec<T, LECO_CODEC_FOR> {};
 template <typename T>
 class Delta_int : public LecoBlockCodec<T, LECO_CODEC_DELTA> {};
 
-// The reference's legacy u32 codec (piecewise_fix_op_minimize_maxerror.h:20-186), read side.
-// decodeArray8 returns the stored values: the reference's own bulk decoder accumulates the
-// prediction by addition and its drivers then correct it with the encoder's difference lists
-// (experiments/fix_int.cpp:110-117), which this decoder does not need.  Encode with the reference.
+// The reference's legacy u32 codec (piecewise_fix_op_minimize_maxerror.h:20-186).
+// encodeArray8 writes the reference's block image (:45-119) byte for byte.  The encoder's
+// difference lists (mul_add_diff_set, :79-84) stay empty: decodeArray8 returns the stored
+// values, whereas the reference's own bulk decoder accumulates the prediction by addition and
+// its drivers then correct it with those lists (experiments/fix_int.cpp:110-117).
 class piecewise_fix_op_max {
  public:
   std::vector<int> mul_add_diff_set, mul_add_diff_set_minus;  // always empty: nothing to correct
@@ -156,8 +157,12 @@ class piecewise_fix_op_max {
     block_num = blocks;
     block_size = blocksize;
   }
-  uint8_t *encodeArray8(uint32_t *, const size_t, uint8_t *, size_t) {
-    throw std::runtime_error("piecewise_fix_op_max::encodeArray8: this library reads the legacy format only");
+  int fit_mode = LECO_FIT_REFERENCE;
+  // Writes the block image of in[0..length) to res; returns the end pointer.
+  uint8_t *encodeArray8(uint32_t *in, const size_t length, uint8_t *res, size_t /*nvalue*/) {
+    int64_t nb = leco_block_encode(LECO_CODEC_LINEAR_F32, LECO_U32, in, (uint32_t)length, fit_mode, res);
+    leco_detail::check(nb, "encodeArray8");
+    return res + nb;
   }
   uint32_t *decodeArray8(uint8_t *in, const size_t length, uint32_t *out, size_t /*nvalue*/) {
     const uint64_t bytes = leco_block_bytes(LECO_CODEC_LINEAR_F32, LECO_U32, in[0], (uint32_t)length);

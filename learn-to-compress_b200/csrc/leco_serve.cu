@@ -116,15 +116,18 @@ __global__ void __launch_bounds__(256) serve_kernel(const ServeCol *__restrict__
 // First-fit allocator over one device buffer (the output/index budget).
 class Arena {
  public:
+  // Every allocation is a multiple of 256 bytes, so only that much of `size` is usable.
   void init(uint64_t size) {
+    size &= ~255ull;
     size_ = size;
     free_.clear();
     free_[0] = size;
     used_ = 0;
   }
+  static uint64_t round(uint64_t bytes) { return (bytes + 255) & ~255ull; }
   // Offset of `bytes` (rounded to 256) or ~0 when nothing fits.
   uint64_t alloc(uint64_t bytes) {
-    bytes = (bytes + 255) & ~255ull;
+    bytes = round(bytes);
     for (auto it = free_.begin(); it != free_.end(); ++it) {
       if (it->second >= bytes) {
         const uint64_t off = it->first, rest = it->second - bytes;
@@ -137,7 +140,7 @@ class Arena {
     return ~0ull;
   }
   void release(uint64_t off, uint64_t bytes) {
-    bytes = (bytes + 255) & ~255ull;
+    bytes = round(bytes);
     used_ -= bytes;
     auto it = free_.emplace(off, bytes).first;
     auto nx = std::next(it);
@@ -232,6 +235,9 @@ void CUDART_CB batch_done(void *p) {
     r->done.store(1, std::memory_order_release);
   }
   s->finished.store(1, std::memory_order_release);
+  // taking the lock orders this store before the loop's check-then-wait, so the wake-up
+  // below cannot fall between them and be lost
+  { std::lock_guard<std::mutex> lk(s->server->mu); }
   s->server->cv.notify_one();  // wake the server loop to retire the batch
 }
 
@@ -283,6 +289,7 @@ void issue(leco_server *sv, Slot *s) {
 
 void server_loop(leco_server *sv) {
   const uint32_t max_req = std::max<uint32_t>(1, sv->opt.max_requests_per_batch);
+  uint64_t tried_id = 0;  // next_id when admission into a free slot was last tried
   for (;;) {
     bool worked = false;
     // retire finished batches
@@ -308,6 +315,7 @@ void server_loop(leco_server *sv) {
       if (s->busy.load()) continue;
       {
         std::lock_guard<std::mutex> lk(sv->mu);
+        tried_id = sv->next_id;
         uint32_t items = 0;
         while (!sv->pending.empty() && s->reqs.size() < max_req) {
           Req *q = sv->pending.front();
@@ -334,10 +342,18 @@ void server_loop(leco_server *sv) {
       bool inflight = false;
       for (Slot *s : sv->slots) inflight |= s->busy.load() != 0;
       if (sv->stop && sv->pending.empty() && !inflight) return;
-      // batch callbacks and submissions notify `cv`; the timeout only bounds a missed wake-up
-      bool ready = !sv->pending.empty();
-      for (Slot *s : sv->slots) ready |= s->busy.load() && s->finished.load();
-      if (!ready) sv->cv.wait_for(lk, std::chrono::microseconds(200));
+      // Nothing was retired or admitted in this pass: the requests that were pending then
+      // wait for a slot or for arena space, which come back only when a batch finishes.  Go
+      // round again at once only for a finished batch, or for requests that arrived after the
+      // last admission try while a slot is free.  Batch callbacks and submissions notify `cv`
+      // under `mu`, so the wait misses neither; its timeout is only a backstop.
+      bool ready = false, free_slot = false;
+      for (Slot *s : sv->slots) {
+        ready |= s->busy.load() && s->finished.load();
+        free_slot |= !s->busy.load();
+      }
+      ready |= free_slot && !sv->pending.empty() && sv->next_id != tried_id;
+      if (!ready) sv->cv.wait_for(lk, std::chrono::milliseconds(2));
     }
   }
 }
@@ -402,7 +418,9 @@ int leco_server_submit(leco_server *sv, const leco_request *req, uint64_t *req_i
   if (req->kind == LECO_REQ_RANGE && (req->first > c.n || req->count > c.n - req->first))
     return serr(LECO_ERR_ARG, "leco_server_submit: range outside the column");
   const uint64_t bytes = req_bytes(*req, c.dtype);
-  if (bytes > sv->arena.size() || req_items(*req, c.block_size) > sv->max_items)
+  // compared as the arena will allocate it (rounded up to 256 bytes): a request that could
+  // never be admitted is refused here instead of blocking every request behind it
+  if (Arena::round(bytes) > sv->arena.size() || req_items(*req, c.block_size) > sv->max_items)
     return serr(LECO_ERR_NOMEM, "leco_server_submit: request larger than the server's device budget");
   auto *q = new Req();
   q->r = *req;

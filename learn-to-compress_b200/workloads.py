@@ -25,11 +25,19 @@ def sorted_keys_u32(n: int = 1_000_000, seed: int = 1) -> np.ndarray:
 
 
 def piecewise_linear_u64(n: int, seed: int = 2, device="cpu", mean_seg: float = 50_000.0,
-                         max_slope_log2: float = 20.0, sigma: float = 4096.0):
+                         max_slope_log2: float = 20.0, sigma: float = 4096.0, noise_on: str = "cpu"):
     """Sorted uint64 keys: a piecewise-linear trend (segment lengths geometric
     with mean `mean_seg`, slopes log-uniform in [1, 2^max_slope_log2]) plus
     round(N(0, sigma)) noise, clipped at 0 and sorted.  Returns an int64 torch
-    tensor holding the uint64 bit patterns (all values < 2^63)."""
+    tensor holding the uint64 bit patterns (all values < 2^63).
+
+    With noise_on="cpu" (default) the values do not depend on `device`: the
+    noise comes from the CPU generator, and the trend of segment r at position
+    i is C_r + slope_r * (i - start_r + 1), C_r summed in order on the host,
+    so every device-side step is one IEEE-rounded elementwise operation.  A CPU
+    run (the reference's timed arm) and a GPU run then see the same column.
+    noise_on="device" draws the noise on `device` instead (faster for many
+    columns; the values then depend on the device)."""
     torch = _torch()
     g = torch.Generator(device="cpu").manual_seed(seed)
     # segment lengths / slopes on the host (a few thousand segments)
@@ -39,11 +47,26 @@ def piecewise_linear_u64(n: int, seed: int = 2, device="cpu", mean_seg: float = 
     while int(lens.sum()) < n:
         lens = torch.cat([lens, lens])
     slopes = torch.exp(torch.rand(len(lens), generator=g, dtype=torch.float64) * (max_slope_log2 * math.log(2.0)))
-    dev_g = torch.Generator(device=device).manual_seed(seed + 1)
-    per = torch.repeat_interleave(slopes.to(device), lens.to(device))[:n]
-    trend = torch.cumsum(per, 0)
-    noise = torch.round(torch.randn(n, generator=dev_g, device=device, dtype=torch.float64) * sigma)
+    # segment bases: the trend's value just before each segment, accumulated in order
+    lens_np, slopes_np = lens.numpy(), slopes.numpy()
+    bases = np.zeros(len(lens_np), np.float64)
+    acc = 0.0
+    for r in range(len(lens_np)):
+        bases[r] = acc
+        acc = acc + float(slopes_np[r]) * float(lens_np[r])
+    starts = np.concatenate([[0], np.cumsum(lens_np)[:-1]]).astype(np.int64)
+    seg = torch.repeat_interleave(torch.arange(len(lens), device=device), lens.to(device))[:n]
+    pos = (torch.arange(n, device=device, dtype=torch.int64) - torch.from_numpy(starts).to(device)[seg] + 1).to(torch.float64)
+    trend = torch.from_numpy(bases).to(device)[seg] + torch.from_numpy(slopes_np).to(device)[seg] * pos
+    del seg, pos
+    if noise_on == "cpu":
+        noise = torch.randn(n, generator=torch.Generator(device="cpu").manual_seed(seed + 1), dtype=torch.float64)
+        noise = torch.round(noise * sigma).to(device)
+    else:
+        dev_g = torch.Generator(device=device).manual_seed(seed + 1)
+        noise = torch.round(torch.randn(n, generator=dev_g, device=device, dtype=torch.float64) * sigma)
     x = torch.clamp(torch.round(trend) + noise, min=0).to(torch.int64)
+    del trend, noise
     x, _ = torch.sort(x)
     return x
 
@@ -112,3 +135,22 @@ def families(n: int, family: str, dtype_bytes: int, rng: np.random.Generator) ->
         raise ValueError(family)
     x = np.clip(np.round(x), 0, top - 1)
     return x.astype(np.uint64).astype(np.uint32 if dtype_bytes == 4 else np.uint64)
+
+
+BATCH_FAMILIES = ("linear", "step", "walk", "uniform")
+
+
+def batch_columns(ncols: int, seed: int, max_len: int | None = None):
+    """The mixed batching workload: `ncols` columns with lengths log-uniform in
+    [1K, 4M] (optionally capped at `max_len`), 50 % uint32 / 50 % uint64, each
+    from one of the four `families`, each coded LeCo-fix (0), Delta-fix (2) or
+    FOR (1).  Yields (values as a numpy array, codec, family) per column."""
+    rng = np.random.default_rng(seed)
+    for _ in range(ncols):
+        n = int(math.exp(rng.uniform(math.log(1000), math.log(4_000_000))))
+        if max_len is not None:
+            n = min(n, max_len)
+        s = 4 if rng.random() < 0.5 else 8
+        fam = BATCH_FAMILIES[int(rng.integers(4))]
+        codec = (0, 2, 1)[int(rng.integers(3))]
+        yield families(n, fam, s, rng), codec, fam

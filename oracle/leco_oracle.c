@@ -7,7 +7,7 @@
  * product against the reference's algorithm.  The product never links,
  * imports or calls this file.
  *
- * Pinning: tests/test_oracle_pin.py compares every function here against the
+ * Pinning: tests/test_oracle.py compares every function here against the
  * unmodified reference headers compiled into oracle/_ref/libleco_ref.so
  * (oracle/Makefile), and tests/golden/ holds fixtures generated by that
  * library (tests/golden/gen_golden.py).

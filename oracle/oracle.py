@@ -24,6 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libleco_ref.so")
+# The reference checkout sits beside this repository unless LECO_REFERENCE_ROOT names it.
+REF_ROOT = os.environ.get("LECO_REFERENCE_ROOT", os.path.abspath(os.path.join(HERE, "..", "..", "reference")))
 
 LECO, FOR, DELTA, POLY2 = 0, 1, 2, 3
 _P = ctypes.c_void_p
@@ -34,8 +36,8 @@ def build(force: bool = False) -> None:
     """Compiles the oracle libraries with oracle/Makefile (gcc only)."""
     if force or not os.path.exists(ORACLE_SO):
         subprocess.check_call(["make", "-s", "-C", HERE, "_build/liboracle.so"])
-    if os.path.isdir("/root/reference/headers"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    if os.path.isdir(os.path.join(REF_ROOT, "headers")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"LECO_REFERENCE_ROOT={REF_ROOT}"])
 
 
 def _ptr(a: np.ndarray):
@@ -273,6 +275,7 @@ class Reference:
             f = getattr(L, f"ref_decode_block_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _SZ, _P]
             f = getattr(L, f"ref_random_{t}"); f.restype = ct; f.argtypes = [ctypes.c_int, _P, ctypes.c_int]
             f = getattr(L, f"ref_column_encode_{t}"); f.restype = _SZ; f.argtypes = [ctypes.c_int, _P, _SZ, ctypes.c_uint32, _P, _P]
+            f = getattr(L, f"ref_column_encode_mt_{t}"); f.restype = _SZ; f.argtypes = [ctypes.c_int, _P, _SZ, ctypes.c_uint32, _P, _P, ctypes.c_int]
             f = getattr(L, f"ref_column_decode_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _P, _SZ, ctypes.c_uint32, _P, ctypes.c_int]
             f = getattr(L, f"ref_column_random_{t}"); f.restype = None; f.argtypes = [ctypes.c_int, _P, _P, ctypes.c_uint32, _P, _SZ, _P, ctypes.c_int]
         L.ref_varlen_encode_u64.restype = _P
@@ -326,27 +329,43 @@ class Reference:
         buf = np.frombuffer(block + b"\0" * 32, np.uint8).copy()
         return int(getattr(self.L, f"ref_random_{self._t(s)}")(codec, _ptr(buf), k))
 
-    def encode_column(self, codec: int, data: np.ndarray, bs: int):
+    def encode_column(self, codec: int, data: np.ndarray, bs: int, threads: int = 1):
         data = np.ascontiguousarray(data)
         s, n = data.dtype.itemsize, len(data)
         nb = (n + bs - 1) // bs
-        out = np.zeros(worst_case_bytes(n, s, bs) + n * s, np.uint8)
+        out = np.empty(worst_case_bytes(n, s, bs) + n * s, np.uint8)
         off = np.zeros(nb + 1, np.uint64)
-        total = getattr(self.L, f"ref_column_encode_{self._t(s)}")(codec, _ptr(data), n, bs, _ptr(out), _ptr(off))
+        if threads > 1:
+            total = getattr(self.L, f"ref_column_encode_mt_{self._t(s)}")(codec, _ptr(data), n, bs, _ptr(out), _ptr(off),
+                                                                          threads)
+        else:
+            total = getattr(self.L, f"ref_column_encode_{self._t(s)}")(codec, _ptr(data), n, bs, _ptr(out), _ptr(off))
         return out[:total].copy(), off
 
-    def decode_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int, threads: int = 1):
-        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
-        out = np.zeros(n + 64, _dtype(s))
+    @staticmethod
+    def pad(payload: np.ndarray) -> np.ndarray:
+        """The payload followed by the 64 zero bytes the block readers may touch."""
+        return np.concatenate([payload, np.zeros(64, np.uint8)])
+
+    def decode_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, n: int, s: int, bs: int, threads: int = 1,
+                      out: np.ndarray | None = None, padded: bool = False):
+        """Bulk decode of a column (per block decodeArray8).  `padded`: the payload
+        already carries pad()'s 64 bytes; `out` (>= n + 64 values) is reused."""
+        pay = payload if padded else self.pad(payload)
+        if out is None:
+            out = np.zeros(n + 64, _dtype(s))
         getattr(self.L, f"ref_column_decode_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), n, bs, _ptr(out), threads)
         return out[:n]
 
-    def random_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, s: int, bs: int, idx: np.ndarray, threads: int = 1):
-        pay = np.concatenate([payload, np.zeros(64, np.uint8)])
+    def random_column(self, codec: int, payload: np.ndarray, offsets: np.ndarray, s: int, bs: int, idx: np.ndarray, threads: int = 1,
+                      out: np.ndarray | None = None, padded: bool = False):
+        """randomdecodeArray8 per index (global indices)."""
+        pay = payload if padded else self.pad(payload)
         idx = np.ascontiguousarray(idx, np.uint64)
-        out = np.zeros(len(idx), _dtype(s))
+        if out is None:
+            out = np.zeros(len(idx), _dtype(s))
         getattr(self.L, f"ref_column_random_{self._t(s)}")(codec, _ptr(pay), _ptr(offsets), bs, _ptr(idx), len(idx), _ptr(out), threads)
-        return out
+        return out[:len(idx)]
 
     # -- legacy u32 format (piecewise_fix_op_max) ---------------------------
     def legacy_encode_block(self, data: np.ndarray):

@@ -85,6 +85,43 @@ size_t col_encode(int codec, const T *data, size_t n, uint32_t bs, uint8_t *out,
   return pos;
 }
 
+// col_encode over `threads` contiguous block ranges: each range is encoded into its own
+// buffer, then the images are placed back to back in `out` (same bytes as col_encode).
+template <typename T>
+size_t col_encode_mt(int codec, const T *data, size_t n, uint32_t bs, uint8_t *out, uint64_t *offsets, int threads) {
+  const size_t nb = (n + bs - 1) / bs;
+  if (threads <= 1 || nb < 2) return col_encode<T>(codec, data, n, bs, out, offsets);
+  const size_t per = (nb + threads - 1) / threads;
+  const size_t parts = (nb + per - 1) / per;
+  std::vector<std::vector<uint8_t>> buf(parts);
+  std::vector<size_t> used(parts, 0);
+  parallel_ranges(parts, (int)parts, [&](size_t lo, size_t hi) {
+    for (size_t p = lo; p < hi; ++p) {
+      const size_t b0 = p * per, b1 = std::min(nb, b0 + per);
+      const size_t v0 = b0 * bs, v1 = std::min(n, b1 * (size_t)bs);
+      buf[p].resize((v1 - v0) * sizeof(T) * 2 + (b1 - b0) * 64 + 64);
+      size_t pos = 0;
+      for (size_t b = b0; b < b1; ++b) {
+        const size_t len = std::min<size_t>(bs, n - b * bs);
+        offsets[b] = pos;  // relative to the range; rebased below
+        pos += enc_block<T>(codec, data + b * bs, len, buf[p].data() + pos, b);
+      }
+      used[p] = pos;
+    }
+  });
+  std::vector<size_t> base(parts + 1, 0);
+  for (size_t p = 0; p < parts; ++p) base[p + 1] = base[p] + used[p];
+  parallel_ranges(parts, (int)parts, [&](size_t lo, size_t hi) {
+    for (size_t p = lo; p < hi; ++p) {
+      memcpy(out + base[p], buf[p].data(), used[p]);
+      const size_t b0 = p * per, b1 = std::min(nb, b0 + per);
+      for (size_t b = b0; b < b1; ++b) offsets[b] += base[p];
+    }
+  });
+  offsets[nb] = base[parts];
+  return base[parts];
+}
+
 template <typename T>
 void col_decode(int codec, const uint8_t *payload, const uint64_t *offsets, size_t n, uint32_t bs, T *out, int threads) {
   size_t nb = (n + bs - 1) / bs;
@@ -123,6 +160,9 @@ uint64_t ref_random_u64(int codec, const uint8_t *in, int k) { return ra_block<u
 // Whole column, blocks of `bs` values, concatenated block images + byte offsets[nb+1].
 size_t ref_column_encode_u32(int codec, const uint32_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off) { return col_encode<uint32_t>(codec, d, n, bs, out, off); }
 size_t ref_column_encode_u64(int codec, const uint64_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off) { return col_encode<uint64_t>(codec, d, n, bs, out, off); }
+// The same column encoded with `threads` host threads over contiguous block ranges.
+size_t ref_column_encode_mt_u32(int codec, const uint32_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off, int threads) { return col_encode_mt<uint32_t>(codec, d, n, bs, out, off, threads); }
+size_t ref_column_encode_mt_u64(int codec, const uint64_t *d, size_t n, uint32_t bs, uint8_t *out, uint64_t *off, int threads) { return col_encode_mt<uint64_t>(codec, d, n, bs, out, off, threads); }
 void ref_column_decode_u32(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint32_t *out, int threads) { col_decode<uint32_t>(codec, p, off, n, bs, out, threads); }
 void ref_column_decode_u64(int codec, const uint8_t *p, const uint64_t *off, size_t n, uint32_t bs, uint64_t *out, int threads) { col_decode<uint64_t>(codec, p, off, n, bs, out, threads); }
 void ref_column_random_u32(int codec, const uint8_t *p, const uint64_t *off, uint32_t bs, const uint64_t *idx, size_t m, uint32_t *out, int threads) { col_random<uint32_t>(codec, p, off, bs, idx, m, out, threads); }

@@ -52,6 +52,46 @@ static int run(const char *name, std::vector<T> &data, int blocks, FILE *out) {
   return bad;
 }
 
+// The legacy u32 codec's driver loop (experiments/fix_int.cpp:57,75,108,153: init with three
+// arguments and encodeArray8 / decodeArray8 / randomdecodeArray8 on uint32_t blocks).
+static int run_legacy(const char *name, std::vector<uint32_t> &data, int blocks, FILE *out) {
+  Codecset::piecewise_fix_op_max codec;
+  const int N = (int)data.size();
+  int block_size = N / blocks;
+  blocks = N / block_size;
+  if (blocks * block_size < N) blocks++;
+  codec.init(blocks, block_size, 0);
+  std::vector<uint8_t *> block_start_vec;
+  std::vector<uint32_t> sizes;
+  for (int i = 0; i < blocks; i++) {
+    int len = (i == blocks - 1) ? N - (blocks - 1) * block_size : block_size;
+    uint8_t *descriptor = (uint8_t *)malloc((size_t)len * 4 * 4 + 64);
+    uint8_t *end = codec.encodeArray8(data.data() + (size_t)i * block_size, len, descriptor, i);
+    sizes.push_back((uint32_t)(end - descriptor));
+    block_start_vec.push_back(descriptor);
+  }
+  int bad = 0;
+  std::vector<uint32_t> recover(N);
+  for (int i = 0; i < blocks; i++) {
+    int len = (i == blocks - 1) ? N - (blocks - 1) * block_size : block_size;
+    codec.decodeArray8(block_start_vec[i], len, recover.data() + (size_t)i * block_size, i);
+  }
+  for (int j = 0; j < N; j++) bad += recover[j] != data[j];
+  uint64_t state = 99;
+  for (int r = 0; r < 2000; r++) {
+    state = state * 6364136223846793005ull + 1442695040888963407ull;
+    int idx = (int)((state >> 33) % (uint64_t)N);
+    bad += codec.randomdecodeArray8(block_start_vec[idx / block_size], idx % block_size, nullptr, N) != data[idx];
+  }
+  uint32_t nb = (uint32_t)blocks;
+  fwrite(&nb, 4, 1, out);
+  fwrite(sizes.data(), 4, nb, out);
+  for (int i = 0; i < blocks; i++) fwrite(block_start_vec[i], 1, sizes[i], out);
+  for (auto *p : block_start_vec) free(p);
+  printf("%s: %d blocks, %d mismatches\n", name, blocks, bad);
+  return bad;
+}
+
 // The reference's filter experiments (experiments/leco_int_fix_template.cpp:216-326,
 // FOR_int_fix_template.cpp:226-322) on the drop-in classes: zone map from the data, the
 // filter_range loop with its zone-map skip, the close-range loop with LeCo's per-block window
@@ -127,6 +167,7 @@ int main(int argc, char **argv) {
   bad += run<Codecset::FOR_int<uint64_t>>("for_u64", k64, 49, out);
   bad += run<Codecset::Delta_int<uint32_t>>("delta_u32", k32, 200, out);
   bad += run<Codecset::Leco_int_poly<uint64_t, 2>>("poly2_u64", k64, 25, out);
+  bad += run_legacy("legacy_u32", k32, 200, out);
   // column extension: one launch for the whole column
   Codecset::Leco_int<uint64_t> col;
   col.init(0, 4096);

@@ -56,6 +56,17 @@ def test_cpp_dropin_driver(tmp_path, orc, lc):
                 img = mask_delta_last_fields(np.frombuffer(img, np.uint8), off, s, m, m).tobytes()
                 ref = mask_delta_last_fields(np.frombuffer(ref, np.uint8), np.array([0, len(ref)], np.uint64), s, m, m).tobytes()
             assert img == ref, (codec, b)
+    # legacy u32 blocks (piecewise_fix_op_max::encodeArray8) == the oracle's legacy images
+    nb = struct.unpack_from("<I", data, pos)[0]
+    pos += 4
+    sizes = np.frombuffer(data, np.uint32, nb, pos)
+    pos += 4 * nb
+    bs = len(k32) // 200
+    for b in range(nb):
+        img = data[pos:pos + int(sizes[b])]
+        pos += int(sizes[b])
+        assert img == orc.legacy_encode_block(k32[b * bs:(b + 1) * bs])[0], ("legacy", b)
+    assert pos == len(data)
 
     # the filter experiments through the drop-in classes == the oracle's column loops
     fdata = fout.read_bytes()

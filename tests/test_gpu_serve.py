@@ -111,3 +111,29 @@ def test_admission_by_device_memory(lc, dev):
     assert st["completed"] == 60 and st["arena_bytes"] == budget
     srv.close()
     lc.check()
+
+
+def test_unaligned_budget(lc, dev):
+    """The arena hands out 256-byte multiples, so a budget that is not one is
+    rounded down: a request sized between the rounded and the given budget is
+    refused at submit (it could never be admitted), and a request of exactly
+    the rounded budget is admitted and completes."""
+    import torch
+
+    raw, cols = _setup(lc, dev)
+    budget = (1 << 20) + 100
+    srv = lc.Server(cols, slots=2, max_requests_per_batch=8, hbm_budget_bytes=budget)
+    assert srv.stats()["arena_bytes"] == 1 << 20
+    over = torch.empty((1 << 17) + 12, dtype=torch.int64).pin_memory()  # (1 << 20) + 96 bytes of results
+    with pytest.raises(lc.LecoError):
+        srv.submit(0, over, first=0, count=over.numel())
+    whole = torch.empty(1 << 17, dtype=torch.int64).pin_memory()  # exactly the usable arena
+    small = torch.empty(1000, dtype=torch.int64).pin_memory()
+    r1 = srv.submit(0, whole, first=5, count=whole.numel())
+    r2 = srv.submit(0, small, first=7, count=small.numel())  # queued behind it, admitted after it retires
+    srv.wait(r1)
+    srv.wait(r2)
+    assert torch.equal(whole, raw[0][5:5 + (1 << 17)])
+    assert torch.equal(small, raw[0][7:1007])
+    srv.close()
+    lc.check()

@@ -58,6 +58,36 @@ def test_noalloc_encode_matches_workspace_encode_twice(lc):
     _encode_both(lc, a[:500_000], 3, 8192, 0)
 
 
+def test_noalloc_encode_allocates_nothing(lc):
+    """A call after the first on the device (which loads the library's kernels)
+    changes neither the device's free memory nor torch's allocator counters."""
+    import torch
+
+    L = lc.lib()
+    dev = torch.device("cuda:0")
+    x = torch.cumsum(torch.randint(0, 999, (2_000_000,), device=dev), 0)
+    n, bs = x.numel(), 4096
+    cap = L.leco_max_payload_bytes(0, 8, n, bs)
+    pay = torch.empty(cap, dtype=torch.uint8, device=dev)
+    off = torch.empty(L.leco_num_blocks(n, bs) + 1, dtype=torch.int64, device=dev)
+    stream = P(torch.cuda.current_stream().cuda_stream)
+    args = (0, 8, P(x.data_ptr()), n, bs, 0, P(pay.data_ptr()), cap, P(off.data_ptr()), None, stream)
+    assert L.leco_encode_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    stats0 = torch.cuda.memory_stats()
+    for _ in range(3):
+        assert L.leco_encode_noalloc(*args) == 0, L.leco_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    stats1 = torch.cuda.memory_stats()
+    # any device allocation takes at least one 2 MiB page off the free count
+    assert abs(free1 - free0) < (1 << 21), (free0, free1)
+    for key in ("allocation.all.allocated", "segment.all.allocated", "reserved_bytes.all.current"):
+        assert stats1.get(key) == stats0.get(key), key
+    lc.check()
+
+
 def test_noalloc_rejects_columns_beyond_its_scratch(lc):
     import torch
 
