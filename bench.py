@@ -273,12 +273,13 @@ def run_batch(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    cols, raw, shapes = [], 0, {}
+    cols, raw, shapes, launch = [], 0, {}, {}
     for x, codec, _ in workloads.batch_columns(args.ncols, seed=3 + rank):
         s, n = x.dtype.itemsize, len(x)
-        bs = autotune.pick_block_size(codec, s, n, autotune.classify(x))
+        bs, g, u = autotune.pick(codec, s, n, autotune.classify(x))
         shapes[bs] = shapes.get(bs, 0) + 1
-        cols.append((torch.from_numpy(x.view(np.int64 if s == 8 else np.int32)).to(dev), codec, bs))
+        launch[f"{g}x{u}"] = launch.get(f"{g}x{u}", 0) + 1
+        cols.append((torch.from_numpy(x.view(np.int64 if s == 8 else np.int32)).to(dev), codec, bs, g, u))
         raw += n * s
     fit = lc.FIT_EXACT if args.fit == "exact" else lc.FIT_REFERENCE
     b = lc.Batch(cols, fit_mode=fit)
@@ -296,8 +297,8 @@ def run_batch(args, world, rank, local):
 
     def verify():
         lc.check()
-        for (x, _, _), c in zip(cols, b.cols):
-            assert torch.equal(c.out, x), "batch decode mismatch"
+        for spec, c in zip(cols, b.cols):
+            assert torch.equal(c.out, spec[0]), "batch decode mismatch"
 
     per_col = lambda: (b.encode_per_column(), b.decode_per_column())
     batch = lambda: (b.encode(), b.decode())
@@ -324,9 +325,11 @@ def run_batch(args, world, rank, local):
                 "ms_per_step": round(t_graph, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "u32+u64", "data": "synthetic",
                 "config": {"workload": f"{args.ncols} columns, lengths log-uniform 1K-4M, 50% u32/50% u64, "
-                                       "families linear/step/walk/uniform, codecs LeCo/Delta/FOR, autotuned block size",
+                                       "families linear/step/walk/uniform, codecs LeCo/Delta/FOR, autotuned block "
+                                       "size, threads per block and unroll depth",
                            "raw_bytes": raw, "blocks": b.total_blocks, "fit": args.fit,
-                           "block_sizes": {str(k_): v for k_, v in sorted(shapes.items())}},
+                           "block_sizes": {str(k_): v for k_, v in sorted(shapes.items())},
+                           "threads_x_unroll": dict(sorted(launch.items()))},
                 "ms_per_pass": {"per_column_launches": round(t_col, 3), "persistent": round(t_batch, 3),
                                 "persistent_graph": round(t_graph, 3)},
                 "decode_ms": {"per_column_launches": round(t_dec_col, 3), "persistent": round(t_dec_batch, 3)},
@@ -778,7 +781,7 @@ def main():
 
     # end-to-end through the public host-buffer API: pinned compressed bytes in,
     # pinned decoded values out, copies inside the timed region
-    e2e = None
+    e2e = e2e_ra = None
     if not args.no_e2e:
         pay_h, off_h = col.to_host()
         pay_pin = torch.empty(len(pay_h) + 64, dtype=torch.uint8).pin_memory()
@@ -810,6 +813,24 @@ def main():
             link_s.append(time.perf_counter() - t0)
         lc._check(L.leco_decode_host(*args_e2e))
         assert torch.equal(out_pin, x.cpu())
+        # random access end to end: leco_gather_host uploads the compressed column and the
+        # indices, builds the directory, gathers and copies the values back, every call
+        idx_pin = idx_sets[0].cpu().pin_memory()
+        ra_pin = torch.empty(RA_BATCH, dtype=torch.int64).pin_memory()
+        args_ra = (0, 8, P(pay_pin.data_ptr()), P(off_pin.data_ptr()), n, BS, P(idx_pin.data_ptr()), RA_BATCH,
+                   P(ra_pin.data_ptr()))
+        lc._check(L.leco_gather_host(*args_ra))
+        ra_s = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            lc._check(L.leco_gather_host(*args_ra))
+            ra_s.append(time.perf_counter() - t0)
+        assert torch.equal(ra_pin, x[idx_sets[0]].cpu())
+        e2e_ra = {"value": round(world * RA_BATCH / float(np.median(ra_s)) / 1e6, 2), "unit": "Mlookups/s",
+                  "api": "leco_gather_host (pinned host buffers; column, indices and results cross PCIe every call)",
+                  "statistic": "median of 5 calls", "call_ms": [round(t * 1e3, 2) for t in ra_s],
+                  "h2d_bytes_per_call": int(comp + off_h.nbytes + RA_BATCH * 8), "d2h_bytes_per_call": RA_BATCH * 8}
+        del idx_pin, ra_pin
         e2e = {"value": round(world * dec_bytes / e2e_s / 1e9, 3), "unit": "GB/s",
                "h2d_bytes_per_step": int(comp + off_h.nbytes), "d2h_bytes_per_step": int(dec_bytes),
                "api": "leco_decode_host (pinned host buffers)", "statistic": "median of 5 calls",
@@ -863,6 +884,7 @@ def main():
                                         "the 32 B directory sector is L2-resident (48,829 blocks x 32 B = 1.6 MB) "
                                         "and not counted"},
             "e2e": e2e,
+            "e2e_random_access": e2e_ra,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * 2,
             "clocks": clocks,

@@ -277,7 +277,11 @@ typedef struct leco_column_desc {
   int32_t codec;       /* LINEAR, FOR, DELTA or POLY2                          */
   int32_t dtype;       /* LECO_U32 or LECO_U64                                 */
   uint32_t block_size; /* values per block, 1..16384                           */
-  uint32_t reserved;
+  uint16_t group_threads; /* batch engine: threads per block, 32/64/128/256;
+                             0 = 32 for blocks of <= 512 values, else 256       */
+  uint16_t unroll;     /* batch engine: unroll depth 1/2/4 (0 = 2): the decoder
+                          writes `unroll` 16-byte chunks per thread step, the u64
+                          LeCo encoder keeps 2*unroll 16-byte loads in flight   */
   uint64_t n;          /* values in the column                                 */
   const void *d_values;/* encode input (n values)                              */
   void *d_out;         /* decode output (n values); may be NULL if never decoded */
@@ -291,7 +295,11 @@ typedef struct leco_batch leco_batch; /* opaque */
 
 /* Builds a batch over ncols column descriptors (copied).  Allocates the device
  * descriptor table and the batch workspace (the only allocations of the batch
- * engine); sizes the persistent grids so every CTA is resident. */
+ * engine); sizes the persistent grids so every CTA is resident.  A column's
+ * work items hold 256/group_threads blocks, one per group of a 256-thread CTA;
+ * an item's shared memory (enc_smem per block x blocks per item) must stay
+ * within 200 KB, else LECO_ERR_ARG.  The committed autotune table gives
+ * block_size, group_threads and unroll per column shape. */
 int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mode, leco_batch **out);
 int leco_batch_destroy(leco_batch *b);
 uint64_t leco_batch_total_blocks(const leco_batch *b);

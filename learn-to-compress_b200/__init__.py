@@ -632,14 +632,17 @@ def version() -> str:
 class ColumnDesc(ctypes.Structure):
     """``leco_column_desc`` of include/leco.h."""
     _fields_ = [("codec", ctypes.c_int32), ("dtype", ctypes.c_int32), ("block_size", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("n", ctypes.c_uint64), ("d_values", _P), ("d_out", _P),
+                ("group_threads", ctypes.c_uint16), ("unroll", ctypes.c_uint16), ("n", ctypes.c_uint64),
+                ("d_values", _P), ("d_out", _P),
                 ("d_payload", _P), ("payload_cap", ctypes.c_uint64), ("d_offsets", _P), ("d_dir", _P)]
 
 
 class Batch:
     """Columns encoded/decoded together by the persistent batch kernels.
 
-    ``columns``: list of (values CUDA tensor, codec, block_size).  Payload,
+    ``columns``: list of (values CUDA tensor, codec, block_size) or
+    (values, codec, block_size, group_threads, unroll) -- the autotune table's
+    three parameters; 0 (or absent) takes the engine's defaults.  Payload,
     offsets, directory and decode-output tensors are allocated here; the C
     side keeps only raw pointers, so this object owns them.
     """
@@ -650,7 +653,9 @@ class Batch:
         self.fit_mode = fit_mode
         self.values, self.cols = [], []
         descs = (ColumnDesc * len(columns))()
-        for i, (v, codec, bs) in enumerate(columns):
+        for i, spec in enumerate(columns):
+            v, codec, bs = spec[:3]
+            group, unroll = (int(spec[3]), int(spec[4])) if len(spec) > 3 else (0, 0)
             s, n = v.element_size(), v.numel()
             nb = L.leco_num_blocks(n, bs)
             cap = L.leco_max_payload_bytes(codec, s, n, bs)
@@ -662,7 +667,7 @@ class Batch:
             col.out = out
             self.values.append(v)
             self.cols.append(col)
-            descs[i] = ColumnDesc(codec, s, bs, 0, n, v.data_ptr(), out.data_ptr() if out is not None else None,
+            descs[i] = ColumnDesc(codec, s, bs, group, unroll, n, v.data_ptr(), out.data_ptr() if out is not None else None,
                                   pay.data_ptr(), cap, off.data_ptr(), d.data_ptr())
         self._descs = descs
         h = _P()
@@ -743,7 +748,7 @@ class Server:
         for i, c in enumerate(self.columns):
             if c.dir is None:
                 c.build_directory()
-            descs[i] = ColumnDesc(c.codec, c.dtype, c.block_size, 0, c.n, None, None, c.payload.data_ptr(),
+            descs[i] = ColumnDesc(c.codec, c.dtype, c.block_size, 0, 0, c.n, None, None, c.payload.data_ptr(),
                                   c.payload.numel(), c.offsets.data_ptr(), c.dir.data_ptr())
         self.options = dict(slots=slots, max_requests_per_batch=max_requests_per_batch,
                             hbm_budget_bytes=hbm_budget_bytes, max_items_per_batch=max_items_per_batch)

@@ -37,17 +37,31 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
 
 
+FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object file in parallel (one nvcc per file),
+    then links the shared library."""
     if not force and up_to_date():
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
+    obj_dir = os.path.join(LIB_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
-           "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-o", LIB + ".tmp", *sources(), "-lpthread"]
+    extra = ["-Xptxas=-v"] if verbose else []
+    jobs = []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        jobs.append((obj, [nvcc, *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]))
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.check_call(cmd)
+        for _, cmd in jobs:
+            print(" ".join(cmd), file=sys.stderr)
+    procs = [subprocess.Popen(cmd) for _, cmd in jobs]
+    failed = [" ".join(cmd) for p, (_, cmd) in zip(procs, jobs) if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    subprocess.check_call([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *[o for o, _ in jobs], "-lpthread"])
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

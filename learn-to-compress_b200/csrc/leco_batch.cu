@@ -2,11 +2,12 @@
 // uint32/uint64 and mixed LeCo/FOR/Delta/poly codecs, encoded and decoded by
 // one persistent launch per pass.
 //
-// Work queue: the batch's blocks are listed column by column as work items --
-// one block of a column with large blocks, or up to eight consecutive blocks of
-// a column with small blocks (<= 512 values; one warp each).  Every CTA of a
-// persistent grid takes the next item from an atomic ticket and runs the
-// per-block encoder or decoder for that column's codec and value type.  Items
+// Work queue: the batch's blocks are listed column by column as work items of
+// 256/G consecutive blocks, G being the column's threads per block (32, 64, 128
+// or 256): one block per item for G = 256, eight for G = 32 (one warp each).
+// Every CTA (256 threads) of a persistent grid takes the next item from an atomic
+// ticket and runs the per-block encoder or decoder instance for that column's
+// codec, value type, G and unroll depth in each of its 256/G groups.  Items
 // are handed out in order and every CTA of the grid is resident, so the
 // encoder's per-column look-back (byte offsets) only ever waits on blocks that
 // are already being processed.
@@ -29,6 +30,8 @@ namespace leco {
 struct DevCol {
   int32_t codec, dtype;
   uint32_t bs, seq;
+  uint32_t group, unroll;  // threads per block (32, 64, 128, 256), unroll depth (1, 2, 4)
+  uint32_t slice, pad;     // encoder shared memory per group (bytes)
   uint64_t n;
   const void *values;
   void *out;
@@ -74,7 +77,6 @@ struct BatchArgs {
   const uint64_t *items;   // [nitems] (column << 32) | first block
   uint32_t ncols;
   uint64_t nitems;
-  uint32_t warp_slice;     // shared-memory bytes per warp for small-block columns
   uint64_t total;          // blocks in the batch
   uint64_t *status;        // [total] look-back words (zeroed per encode pass)
   unsigned long long *ticket;  // zeroed per pass
@@ -82,7 +84,7 @@ struct BatchArgs {
   uint32_t *error;
 };
 
-template <typename T, int CODEC, int G>
+template <typename T, int CODEC, int G, int U>
 __device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b,
                                                  uint8_t *smem) {
   EncodeArgs a;
@@ -100,26 +102,57 @@ __device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCo
   a.status = B.status + p0;
   a.ticket = nullptr;
   a.error = B.error;
-  encode_block<T, CODEC, G>(a, b, smem);
+  encode_block<T, CODEC, G, U>(a, b, smem);
+}
+// The unroll depth changes only the u64 LeCo encoder; other codecs take one instance.
+template <typename T, int CODEC, int G>
+__device__ __forceinline__ void batch_encode_u(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
+  if constexpr (CODEC == kLinear && sizeof(T) == 8 && G != 32) {
+    switch (c.unroll) {
+      case 1: batch_encode_one<T, CODEC, G, 1>(B, c, ci, b, smem); return;
+      case 4: batch_encode_one<T, CODEC, G, 4>(B, c, ci, b, smem); return;
+      default: batch_encode_one<T, CODEC, G, 2>(B, c, ci, b, smem); return;
+    }
+  } else {
+    batch_encode_one<T, CODEC, G, 2>(B, c, ci, b, smem);
+  }
 }
 template <typename T, int CODEC>
-__device__ __forceinline__ void batch_encode_cta(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
-  batch_encode_one<T, CODEC, 256>(B, c, ci, b, smem);
-}
-template <typename T, int CODEC>
-__device__ __forceinline__ void batch_encode_warp(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
-  batch_encode_one<T, CODEC, 32>(B, c, ci, b, smem);
+__device__ __forceinline__ void batch_encode_any(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
+  switch (c.group) {
+    case 32: batch_encode_u<T, CODEC, 32>(B, c, ci, b, smem); return;
+    case 64: batch_encode_u<T, CODEC, 64>(B, c, ci, b, smem); return;
+    case 128: batch_encode_u<T, CODEC, 128>(B, c, ci, b, smem); return;
+    default: batch_encode_u<T, CODEC, 256>(B, c, ci, b, smem); return;
+  }
 }
 
-template <typename T, int CODEC>
-__device__ __forceinline__ void batch_decode_cta(const BatchArgs &B, const DevCol &c, uint64_t b) {
+template <typename T, int CODEC, int G, int U>
+__device__ __forceinline__ void batch_decode_one(const BatchArgs &B, const DevCol &c, uint64_t b) {
   DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
-  decode_block<T, CODEC, 256>(a, b);
+  decode_block<T, CODEC, G, U>(a, b);
+}
+// The unroll depth changes the narrow-field decoder; Delta blocks take one instance.
+template <typename T, int CODEC, int G>
+__device__ __forceinline__ void batch_decode_u(const BatchArgs &B, const DevCol &c, uint64_t b) {
+  if constexpr (CODEC != kDelta) {
+    switch (c.unroll) {
+      case 1: batch_decode_one<T, CODEC, G, 1>(B, c, b); return;
+      case 4: batch_decode_one<T, CODEC, G, 4>(B, c, b); return;
+      default: batch_decode_one<T, CODEC, G, 2>(B, c, b); return;
+    }
+  } else {
+    batch_decode_one<T, CODEC, G, 2>(B, c, b);
+  }
 }
 template <typename T, int CODEC>
-__device__ __forceinline__ void batch_decode_warp(const BatchArgs &B, const DevCol &c, uint64_t b) {
-  DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
-  decode_block<T, CODEC, 32>(a, b);
+__device__ __forceinline__ void batch_decode_any(const BatchArgs &B, const DevCol &c, uint64_t b) {
+  switch (c.group) {
+    case 32: batch_decode_u<T, CODEC, 32>(B, c, b); return;
+    case 64: batch_decode_u<T, CODEC, 64>(B, c, b); return;
+    case 128: batch_decode_u<T, CODEC, 128>(B, c, b); return;
+    default: batch_decode_u<T, CODEC, 256>(B, c, b); return;
+  }
 }
 
 template <typename T, int CODEC>
@@ -127,7 +160,8 @@ __device__ __forceinline__ void batch_seq_one(const DevCol &c, uint64_t b, doubl
   seq_fit_block<T, CODEC>(reinterpret_cast<const T *>(c.values), c.n, c.bs, b, c.polyX, models);
 }
 
-// Persistent encode: one ticket = one work item.
+// Persistent encode: one ticket = one work item; group g of the CTA takes block
+// first + g of the item with its own slice of shared memory.
 __global__ void __launch_bounds__(256) batch_encode_kernel(BatchArgs B) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ unsigned long long item;
@@ -139,21 +173,16 @@ __global__ void __launch_bounds__(256) batch_encode_kernel(BatchArgs B) {
     if (it >= B.nitems) break;
     const uint64_t e = __ldg(B.items + it);
     const uint32_t ci = (uint32_t)(e >> 32);
-    const uint64_t b0 = e & 0xffffffffull;
     const DevCol &c = B.cols[ci];
-    if (c.bs <= kWarpBlock) {
-      const uint32_t w = threadIdx.x >> 5;
-      const uint64_t b = b0 + w;
-      if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci))
-        LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_warp, B, c, ci, b, smem + (size_t)w * B.warp_slice);
-    } else {
-      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_cta, B, c, ci, b0, smem);
-    }
+    const uint32_t gi = threadIdx.x / c.group;
+    const uint64_t b = (e & 0xffffffffull) + gi;
+    if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci))
+      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_any, B, c, ci, b, smem + (size_t)gi * c.slice);
     __syncthreads();  // shared memory is reused by the next item
   }
 }
 
-// Persistent decode: one ticket = one work item.
+// Persistent decode: one ticket = one work item, as the encoder.
 __global__ void __launch_bounds__(256) batch_decode_kernel(BatchArgs B) {
   __shared__ unsigned long long item;
   for (;;) {
@@ -164,14 +193,10 @@ __global__ void __launch_bounds__(256) batch_decode_kernel(BatchArgs B) {
     if (it >= B.nitems) break;
     const uint64_t e = __ldg(B.items + it);
     const uint32_t ci = (uint32_t)(e >> 32);
-    const uint64_t b0 = e & 0xffffffffull;
     const DevCol &c = B.cols[ci];
-    if (c.bs <= kWarpBlock) {
-      const uint64_t b = b0 + (threadIdx.x >> 5);
-      if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci)) LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_warp, B, c, b);
-    } else {
-      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_cta, B, c, b0);
-    }
+    const uint64_t b = (e & 0xffffffffull) + threadIdx.x / c.group;
+    if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci)) LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_any, B, c, b);
+    __syncthreads();  // the Delta row scan's shared scratch is reused by the next item
   }
 }
 
@@ -200,7 +225,6 @@ struct leco_batch {
   uint64_t *d_prefix = nullptr;
   uint64_t *d_items = nullptr;
   uint64_t nitems = 0;
-  uint32_t warp_slice = 0;
   uint8_t *d_ws = nullptr;  // status [total] | ticket | models [total*3]
   uint64_t ws_bytes = 0, status_bytes = 0, models_off = 0;
   uint32_t enc_smem = 0;
@@ -211,6 +235,9 @@ struct leco_batch {
 };
 
 namespace {
+
+// Shared memory one work item may take (the CTA limit is 227 KB).
+constexpr uint32_t kBatchMaxSmem = 200 * 1024;
 
 int berr(int code, const std::string &m) { return leco::record_error(code, m); }
 
@@ -226,7 +253,6 @@ BatchArgs args_of(const leco_batch *b, uint32_t *err) {
   B.prefix = b->d_prefix;
   B.items = b->d_items;
   B.nitems = b->nitems;
-  B.warp_slice = b->warp_slice;
   B.ncols = (uint32_t)b->cols.size();
   B.total = b->prefix.back();
   B.status = reinterpret_cast<uint64_t *>(b->d_ws);
@@ -279,16 +305,30 @@ int leco_batch_create(const leco_column_desc *h_cols, uint32_t ncols, int fit_mo
       poly2_x_sums((uint32_t)std::min<uint64_t>(c.n, c.block_size), d.polyX);
       poly2_x_sums((uint32_t)(c.n - (nb - 1) * c.block_size), d.polyX + 5);
     }
-    const uint32_t sm = enc_smem_bytes(c.block_size, (uint32_t)c.dtype);
-    if (c.block_size <= kWarpBlock) b->warp_slice = std::max(b->warp_slice, (sm + 15) / 16 * 16);
-    else max_smem = std::max(max_smem, sm);
+    d.group = c.group_threads ? c.group_threads : (c.block_size <= kWarpBlock ? 32u : 256u);
+    d.unroll = c.unroll ? c.unroll : 2u;
+    d.pad = 0;
+    if ((d.group != 32 && d.group != 64 && d.group != 128 && d.group != 256) ||
+        (d.unroll != 1 && d.unroll != 2 && d.unroll != 4)) {
+      delete b;
+      return berr(LECO_ERR_ARG, "leco_batch_create: column " + std::to_string(i) +
+                                    ": group_threads must be 0, 32, 64, 128 or 256 and unroll 0, 1, 2 or 4");
+    }
+    d.slice = (enc_smem_bytes(c.block_size, (uint32_t)c.dtype) + 15) / 16 * 16;
+    const uint32_t item_smem = d.slice * (256 / d.group);
+    if (item_smem > kBatchMaxSmem) {
+      delete b;
+      return berr(LECO_ERR_ARG, "leco_batch_create: column " + std::to_string(i) + ": " + std::to_string(256 / d.group) +
+                                    " groups of " + std::to_string(d.slice) + " bytes of shared memory exceed the " +
+                                    std::to_string(kBatchMaxSmem) + " a CTA may use");
+    }
+    max_smem = std::max(max_smem, item_smem);
   }
-  max_smem = std::max(max_smem, 8 * b->warp_slice);
-  // work items: (column << 32) | first block; eight blocks per item for small-block columns
+  // work items: (column << 32) | first block, 256/G blocks per item
   std::vector<uint64_t> items;
   for (uint32_t i = 0; i < ncols; ++i) {
     const uint64_t nb = leco_num_blocks(h_cols[i].n, h_cols[i].block_size);
-    const uint64_t step = h_cols[i].block_size <= kWarpBlock ? 8 : 1;
+    const uint64_t step = 256 / dc[i].group;
     for (uint64_t blk = 0; blk < nb; blk += step) items.push_back(((uint64_t)i << 32) | blk);
   }
   b->nitems = items.size();

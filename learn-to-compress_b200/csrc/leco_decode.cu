@@ -194,12 +194,11 @@ __global__ void __launch_bounds__(256) sum_kernel(DecodeLaunch a, uint64_t *d_su
   }
   const bool raw = h.l == TB;
   if (CODEC == kDelta && !raw) {
-    const DeltaChunk c = delta_chunk_start<256>(words, h, len);
-    uint64_t run = c.run;
-    for (uint32_t k = c.k0; k < c.k1; ++k) {
-      acc += run & tmask;
-      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-    }
+    delta_tiles<T, 256>(words, h, len, 0, len, [&](uint32_t k0, const auto *v) {
+#pragma unroll
+      for (int j = 0; j < kDeltaSpan; ++j)
+        if (k0 + j < len) acc += (uint64_t)v[j] & tmask;
+    });
   } else {
     const uint32_t l = raw ? TB : h.l;
     for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
@@ -218,18 +217,26 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherLaunch a) {
   gather_lookups<T, CODEC>(a, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
 }
 
-// Delta random access: prefix walk over fields 0..k-1 (bit_read.h:1292-1317).
+// Delta random access: value k = x0 + the signed fields 0..k-1
+// (Delta_int::randomdecodeArray8, delta_integer_template.h:132-154, read_Delta_int
+// bit_read.h:1292-1317).  The walk is shared by a warp: lane j adds fields
+// j, j+32, ... < k, so each step reads 32 consecutive fields, and a warp sum
+// combines the lanes.  Each warp takes lookups in turn (warp-uniform loop).
 template <typename T>
 __global__ void __launch_bounds__(256) gather_delta_kernel(GatherLaunch a) {
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
   T *out = reinterpret_cast<T *>(a.out);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.m; i += (uint64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < a.m; i += warps) {
     const uint64_t g = __ldg(a.idx + i);
     if (g >= a.n) {
-      out[i] = 0;
-      atomicOr(a.error, kErrBadIndex);
+      if (lane == 0) {
+        out[i] = 0;
+        atomicOr(a.error, kErrBadIndex);
+      }
       continue;
     }
     const uint64_t b = g / a.bs;
@@ -240,13 +247,14 @@ __global__ void __launch_bounds__(256) gather_delta_kernel(GatherLaunch a) {
       v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);
     } else if (h.l > TB) {
       v = 0;
-      atomicOr(a.error, kErrBadHeader);
+      if (lane == 0) atomicOr(a.error, kErrBadHeader);
     } else {
-      v = h.base;
-      if (h.l)
-        for (uint32_t j = 0; j < k; ++j) v += apply_signed(0, load_field(words, h.body_bit + (uint64_t)j * h.l, h.l), h.l);
+      uint64_t part = 0;
+#pragma unroll 4
+      for (uint32_t j = lane; j < k; j += 32) part += delta_field<uint64_t>(words, h, h.l ? k + 1 : 0, j);
+      v = h.base + warp_sum_u64(part);
     }
-    out[i] = (T)v;
+    if (lane == 0) out[i] = (T)v;
   }
 }
 
@@ -356,8 +364,8 @@ static void run_gather(const GatherLaunch &L, cudaStream_t st) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (CODEC == kDelta) {
-    const unsigned grid = (unsigned)umin64((L.m + 255) / 256, (uint64_t)sms * 16);
+  if (CODEC == kDelta) {  // one warp per lookup at a time
+    const unsigned grid = (unsigned)umin64((L.m + 7) / 8, (uint64_t)sms * 8);
     gather_delta_kernel<T><<<grid, 256, 0, st>>>(L);
     return;
   }

@@ -1,6 +1,8 @@
 // leco_decode.cuh -- per-block decode / random-access helpers shared by the
 // single-column kernels (leco_decode.cu) and the batch kernels (leco_batch.cu).
 #pragma once
+#include <type_traits>
+
 #include "leco_device.cuh"
 #include "leco_internal.h"
 
@@ -77,68 +79,114 @@ __device__ __forceinline__ uint64_t value_from_field(const BlockHdr &h, uint32_t
   return h.l ? apply_signed((uint64_t)pred, f, h.l) : (uint64_t)pred;
 }
 
-// Delta running sum split over the CTA: each thread owns a contiguous chunk
-// [k0, k1) of values; a block-wide exclusive scan of the chunks' delta sums
-// gives each thread the value at k0.  Must be called by all threads.
-struct DeltaChunk {
-  uint32_t k0, k1;
-  uint64_t run;  // decoded value k0 (mod 2^64)
-};
-template <int G>
-__device__ __forceinline__ DeltaChunk delta_chunk_start(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len) {
-  __shared__ uint64_t wsum[32];
-  const uint32_t nt = group_size<G>(), tid = group_rank<G>();
-  const uint32_t chunk = (len + nt - 1) / nt;
-  DeltaChunk c;
-  c.k0 = min(len, tid * chunk);
-  c.k1 = min(len, c.k0 + chunk);
-  uint64_t local = 0;  // fields k0 .. k1-1 feed values k0+1 .. k1; field len-1 is not a delta
-  if (h.l)
-    for (uint32_t k = c.k0; k < c.k1 && k + 1 < len; ++k)
-      local += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
+// Scratch of the Delta scan: 10 words for each of up to four groups of a CTA.  One
+// non-template function, so every kernel holds a single copy however many decoder
+// instances it contains.
+__device__ __forceinline__ uint64_t *delta_scan_scratch() {
+  __shared__ uint64_t s[4 * 10];
+  return s;
+}
+
+// Signed Delta field i of a block (0 for fields that are not deltas, i.e. i < 0 or
+// i >= len - 1), in the value type's modular arithmetic.  Fields of up to 32 bits
+// are read through 32-bit words.
+template <typename A>
+__device__ __forceinline__ A delta_field(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, int64_t i) {
+  const uint32_t l = h.l;
+  if (i < 0 || (uint64_t)i + 1 >= len || !l) return (A)0;
+  const uint64_t bit = h.body_bit + (uint64_t)i * l;
+  uint64_t f;
+  if (l <= 32) {
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(words) + (bit >> 5);
+    f = __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(bit & 31)) & (uint32_t)lowmask(l);
+  } else {
+    f = load_field(words, bit, l);
+  }
+  const uint64_t mag = f & lowmask(l - 1);
+  return ((f >> (l - 1)) & 1ull) ? (A)mag : (A)(0 - mag);
+}
+
+// Delta_int<T>::decodeArray8 (delta_integer_template.h:89-127): value k =
+// x0 + sum_{i<k} signed(field_i), mod 2^(8*sizeof(T)); field len-1 is not a delta
+// (the reference packs n fields from n-1 deltas, :83).  The block is walked in tiles
+// of DS*GS values (GS threads in the group): thread t owns the DS consecutive values
+// from k0 = tile start + t*DS, i.e. fields k0-1 .. k0+DS-2, which it keeps in
+// registers; one group-wide exclusive scan of the threads' sums (warp shuffles,
+// then the warps' totals through shared memory) plus the carry of the tiles before
+// gives its first value.  EMIT(k0, v) receives the DS values k0 .. k0+DS-1 (some
+// may lie outside [lo, hi) or past the block); the group must call this together.
+constexpr int kDeltaSpan = 16;
+template <typename T, int G, typename Emit>
+__device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, uint32_t lo,
+                                            uint32_t hi, Emit emit) {
+  using A = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;  // arithmetic mod 2^(8S)
+  constexpr int DS = kDeltaSpan;
+  uint64_t *wtot = delta_scan_scratch() + (GroupOf<G>::sub ? 10 * group_index<G>() : 0);
+  const uint32_t tid = group_rank<G>();
   const int lane = tid & 31, warp = tid >> 5;
-  uint64_t incl = local;
-  for (int d = 1; d < 32; d <<= 1) {
-    uint64_t y = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl += y;
-  }
-  if (G == 32) {  // one warp owns the block: the warp scan is the whole scan
-    c.run = h.base + (incl - local);
-    return c;
-  }
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = (nt + 31) >> 5;
-    uint64_t x = lane < nw ? wsum[lane] : 0, xi = x;
-    for (int d = 1; d < 32; d <<= 1) {
-      uint64_t y = __shfl_up_sync(0xffffffffu, xi, d);
-      if (lane >= d) xi += y;
+  const uint32_t GS = group_size<G>(), NW = GS / 32;  // NW <= 8: whole-CTA groups here have <= 256 threads
+  const uint32_t TW = DS * GS;                         // values per tile
+  const uint32_t t1 = (hi + TW - 1) / TW;               // tiles up to the last value wanted
+  A carry = (A)h.base;
+  for (uint32_t tl = 0; tl < t1; ++tl) {
+    const uint32_t k0 = tl * TW + tid * DS;
+    A v[DS];
+#pragma unroll
+    for (int j = 0; j < DS; ++j) v[j] = delta_field<A>(words, h, len, (int64_t)k0 - 1 + j);
+#pragma unroll
+    for (int j = 1; j < DS; ++j) v[j] += v[j - 1];  // inclusive prefix inside the span
+    const A tot = v[DS - 1];
+    A incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const A y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    if (lane < nw) wsum[lane] = xi - x;
+    A before = carry, tile_sum;
+    if (NW == 1) {
+      before += incl - tot;
+      tile_sum = __shfl_sync(0xffffffffu, incl, 31);
+    } else {
+      if (lane == 31) wtot[warp] = incl;
+      group_sync<G>();
+      if (warp == 0) {
+        A x = lane < (int)NW ? (A)wtot[lane] : (A)0, xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const A y = __shfl_up_sync(0xffffffffu, xi, o);
+          if (lane >= o) xi += y;
+        }
+        if (lane < (int)NW) wtot[lane] = xi - x;
+        if (lane == (int)NW - 1) wtot[NW] = xi;
+      }
+      group_sync<G>();
+      before += (A)wtot[warp] + (incl - tot);
+      tile_sum = (A)wtot[NW];
+      group_sync<G>();  // wtot is rewritten by the next tile
+    }
+    if (k0 + DS > lo && k0 < hi) {
+#pragma unroll
+      for (int j = 0; j < DS; ++j) v[j] += before;
+      emit(k0, v);
+    }
+    carry += tile_sum;
   }
-  __syncthreads();
-  c.run = h.base + wsum[warp] + (incl - local);
-  return c;
 }
 
-template <typename T>
-__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v, int cnt, bool full);
-template <>
-__device__ __forceinline__ void store_vals<uint64_t>(uint64_t *out, uint64_t o0, const uint64_t *v, int cnt, bool full) {
-  if (full) {
-    __stcs(reinterpret_cast<ulonglong2 *>(out + o0), make_ulonglong2(v[0], v[1]));
-    if (cnt > 2) __stcs(reinterpret_cast<ulonglong2 *>(out + o0 + 2), make_ulonglong2(v[2], v[3]));
+// Streams CNT values (a whole number of 16-byte chunks, 16-byte aligned) to out[o0...].
+template <typename T, int CNT>
+__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v) {
+  if (sizeof(T) == 8) {
+#pragma unroll
+    for (int c = 0; c < CNT / 2; ++c)
+      __stcs(reinterpret_cast<ulonglong2 *>(out + o0 + 2 * c), make_ulonglong2(v[2 * c], v[2 * c + 1]));
+  } else {
+#pragma unroll
+    for (int c = 0; c < CNT / 4; ++c)
+      __stcs(reinterpret_cast<uint4 *>(out + o0 + 4 * c),
+             make_uint4((uint32_t)v[4 * c], (uint32_t)v[4 * c + 1], (uint32_t)v[4 * c + 2], (uint32_t)v[4 * c + 3]));
   }
 }
-template <>
-__device__ __forceinline__ void store_vals<uint32_t>(uint32_t *out, uint64_t o0, const uint64_t *v, int cnt, bool full) {
-  if (full) {
-    __stcs(reinterpret_cast<uint4 *>(out + o0), make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], (uint32_t)v[3]));
-    if (cnt > 4) __stcs(reinterpret_cast<uint4 *>(out + o0 + 4), make_uint4((uint32_t)v[4], (uint32_t)v[5], (uint32_t)v[6], (uint32_t)v[7]));
-  }
-}
-
 
 // True when every prediction of the block is a finite double inside
 // (-2^63, 2^63), so the x86 out-of-range rule of f2i_x86 can never apply:
@@ -154,14 +202,14 @@ __device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
 
 // Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
 // (raw u32 blocks included).  Each thread produces VEC consecutive values per
-// step and writes them with one 16-byte store.
+// step and writes them with U 16-byte stores (U: the unroll depth).
 // SUM: instead of storing, returns this thread's sum of the values (as T).
-template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256, bool SUM = false>
+template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256, bool SUM = false, int U = 2>
 __device__ __forceinline__ uint64_t decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32,
                                                   T *out, uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
   uint64_t acc = 0;
   constexpr int S = sizeof(T);
-  constexpr int VEC = 32 / S;  // two 16-byte stores per step
+  constexpr int VEC = U * 16 / S;  // U 16-byte stores per step
   const uint32_t l = raw ? 32u : h.l;
   // words32 + body_bit/32: the body's first word (global payload or a staged copy in shared memory)
   const uint32_t *bp = words32 + (h.body_bit >> 5);
@@ -203,8 +251,9 @@ __device__ __forceinline__ uint64_t decode_narrow(const BlockHdr &h, bool raw, c
       continue;
     }
     const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
-    store_vals<T>(out, obase + kv, v, VEC, full);
-    if (!full) {
+    if (full) {
+      store_vals<T, VEC>(out, obase + kv, v);
+    } else {
 #pragma unroll
       for (int j = 0; j < VEC; ++j)
         if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
@@ -219,7 +268,7 @@ __device__ __forceinline__ uint64_t decode_narrow(const BlockHdr &h, bool raw, c
 // 16-byte store.
 // Decodes the values of block b inside [a.first, a.first + a.count) with one
 // thread group: the whole CTA (G = 256) or one warp (G = 32, small blocks).
-template <typename T, int CODEC, int G = 256>
+template <typename T, int CODEC, int G = 256, int U = 2>
 __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) {
   const uint32_t rank = group_rank<G>();
   constexpr int S = sizeof(T);
@@ -252,13 +301,19 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   const bool raw = h.l == TB;
 
   if (CODEC == kDelta && !raw) {
-    // Running sum: value k = x0 + sum_{i<k} signed(field_i) (mod 2^(8S)).
-    const DeltaChunk c = delta_chunk_start<G>(words, h, len);
-    uint64_t run = c.run;
-    for (uint32_t k = c.k0; k < c.k1; ++k) {
-      if (k >= lo && k < hi) out[obase + k] = (T)run;
-      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-    }
+    delta_tiles<T, G>(words, h, len, lo, hi, [&](uint32_t k0, const auto *v) {
+      T *o = out + obase + k0;
+      if (k0 >= lo && k0 + kDeltaSpan <= hi && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+        uint64_t w[kDeltaSpan];
+#pragma unroll
+        for (int j = 0; j < kDeltaSpan; ++j) w[j] = (uint64_t)v[j];
+        store_vals<T, kDeltaSpan>(out, obase + k0, w);
+      } else {
+#pragma unroll
+        for (int j = 0; j < kDeltaSpan; ++j)
+          if (k0 + j >= lo && k0 + j < hi) o[j] = (T)v[j];
+      }
+    });
     return;
   }
 
@@ -274,8 +329,8 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
     const bool fast = (CODEC == kFor) || pred_in_range<CODEC>(h, len);
     const uint32_t *w32 = reinterpret_cast<const uint32_t *>(a.payload);
     if (!raw) mark_nonneg<CODEC>(h, len);
-    if (fast) decode_narrow<T, CODEC, true, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
-    else decode_narrow<T, CODEC, false, false, G>(h, raw, w32, out, obase, lo, hi, kstart);
+    if (fast) decode_narrow<T, CODEC, true, false, G, false, U>(h, raw, w32, out, obase, lo, hi, kstart);
+    else decode_narrow<T, CODEC, false, false, G, false, U>(h, raw, w32, out, obase, lo, hi, kstart);
     return;
   }
   for (int32_t kv = kstart + (int32_t)rank * VEC; kv < (int32_t)hi; kv += (int32_t)group_size<G>() * VEC) {
@@ -296,8 +351,8 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
       v[j] = raw ? f : value_from_field<CODEC, S>(h, (uint32_t)k, f);
     }
     const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
-    store_vals<T>(out, obase + kv, v, VEC, full);
-    if (!full) {
+    if (full) store_vals<T, VEC>(out, obase + kv, v);
+    else {
 #pragma unroll
       for (int j = 0; j < VEC; ++j)
         if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];

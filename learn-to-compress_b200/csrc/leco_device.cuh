@@ -275,48 +275,36 @@ __device__ __forceinline__ void block_reduce2(u128 &a, u128 &b, u128 *red) {
 }
 
 // ---- thread groups ----------------------------------------------------------
-// A block of values is processed either by a whole CTA (G = CTA size) or by one
-// warp (G = 32, several small blocks per CTA).  These helpers give the rank in
-// the group, synchronise it and reduce over it.
+// A block of values is processed by a group of G threads:
+//   G = 32        one warp (several blocks per CTA);
+//   G = 64, 128   a sub-group of a 256-thread CTA: the CTA holds 256/G groups, group
+//                 g synchronises on its own named barrier 8 + g;
+//   G = 256       the whole CTA (any blockDim.x).
+// These helpers give the rank in the group, synchronise it and reduce over it.
 template <int G>
-__device__ __forceinline__ uint32_t group_rank() { return G == 32 ? (threadIdx.x & 31) : threadIdx.x; }
+struct GroupOf {
+  static constexpr bool warp = G == 32;
+  static constexpr bool sub = G == 64 || G == 128;
+};
 template <int G>
-__device__ __forceinline__ uint32_t group_size() { return G == 32 ? 32u : blockDim.x; }
+__device__ __forceinline__ uint32_t group_rank() {
+  return GroupOf<G>::warp ? (threadIdx.x & 31) : GroupOf<G>::sub ? (threadIdx.x & (G - 1)) : threadIdx.x;
+}
+template <int G>
+__device__ __forceinline__ uint32_t group_size() { return (GroupOf<G>::warp || GroupOf<G>::sub) ? (uint32_t)G : blockDim.x; }
+// Index of this thread's group inside the CTA (0 for a whole-CTA group).
+template <int G>
+__device__ __forceinline__ uint32_t group_index() {
+  return GroupOf<G>::warp ? (threadIdx.x >> 5) : GroupOf<G>::sub ? (threadIdx.x / G) : 0u;
+}
 template <int G>
 __device__ __forceinline__ void group_sync() {
-  if (G == 32) __syncwarp();
+  if (GroupOf<G>::warp) __syncwarp();
+  else if (GroupOf<G>::sub) asm volatile("bar.sync %0, %1;" ::"r"(8u + threadIdx.x / G), "n"(G) : "memory");
   else __syncthreads();
 }
-template <int OP, int G>
-__device__ __forceinline__ u128 group_reduce(u128 v, u128 *red) {
-  if (G != 32) return block_reduce<OP>(v, red);
-  switch (OP) {
-    case 0: return warp_sum_u128(v);
-    case 1: return warp_max_u64((uint64_t)v);
-    case 2: return warp_min_u64((uint64_t)v);
-    case 3: return (u128)(uint64_t)warp_max_i64((int64_t)(uint64_t)v);
-    case 4: return (u128)(uint64_t)warp_min_i64((int64_t)(uint64_t)v);
-    default: return warp_sum_u64((uint64_t)v);
-  }
-}
-
-template <int OPA, int OPB, int G>
-__device__ __forceinline__ void group_reduce2(u128 &a, u128 &b, u128 *red) {
-  if (G != 32) {
-    block_reduce2<OPA, OPB>(a, b, red);
-    return;
-  }
-  a = group_reduce<OPA, 32>(a, red);
-  b = group_reduce<OPB, 32>(b, red);
-}
-
-// Reductions over warps 1.. of a CTA while warp 0 runs something else (the
-// encoder's look-back): named barrier 1 over blockDim.x - 32 threads, which all
-// of warps 1.. must reach.  `red` as block_reduce2 (66 entries).  OP as
-// block_reduce.
-__device__ __forceinline__ void sub_sync() { asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x - 32) : "memory"); }
 template <int OP>
-__device__ __forceinline__ u128 warp_op(u128 x) {
+__device__ __forceinline__ u128 warp_reduce_op(u128 x) {
   switch (OP) {
     case 0: return warp_sum_u128(x);
     case 1: return warp_max_u64((uint64_t)x);
@@ -327,32 +315,80 @@ __device__ __forceinline__ u128 warp_op(u128 x) {
   }
 }
 template <int OP>
-__device__ __forceinline__ u128 op_identity() {
+__device__ __forceinline__ u128 reduce_identity() {
   return OP == 2 ? (u128)~0ull : OP == 3 ? (u128)0x8000000000000000ull : OP == 4 ? (u128)0x7fffffffffffffffull : (u128)0;
 }
-template <int OPA, int OPB>
-__device__ __forceinline__ void sub_reduce2(u128 &a, u128 &b, u128 *red) {
-  const int lane = threadIdx.x & 31, warp = (int)(threadIdx.x >> 5) - 1, nw = (int)(blockDim.x >> 5) - 1;
-  a = warp_op<OPA>(a);
-  b = warp_op<OPB>(b);
-  sub_sync();  // `red` may still be read by a previous reduction
+// Two reductions over `nw` (<= 32) warps: `warp` is this warp's index among them,
+// SYNC synchronises exactly those warps.  `red` as block_reduce2 (66 entries).
+template <int OPA, int OPB, typename Sync>
+__device__ __forceinline__ void warps_reduce2(u128 &a, u128 &b, u128 *red, int warp, int nw, Sync sync) {
+  const int lane = threadIdx.x & 31;
+  a = warp_reduce_op<OPA>(a);
+  b = warp_reduce_op<OPB>(b);
+  sync();  // `red` may still be read by a previous reduction
   if (lane == 0) {
     red[warp] = a;
     red[33 + warp] = b;
   }
-  sub_sync();
+  sync();
   if (warp == 0) {
-    u128 x = lane < nw ? red[lane] : op_identity<OPA>(), y = lane < nw ? red[33 + lane] : op_identity<OPB>();
-    x = warp_op<OPA>(x);
-    y = warp_op<OPB>(y);
+    u128 x = lane < nw ? red[lane] : reduce_identity<OPA>(), y = lane < nw ? red[33 + lane] : reduce_identity<OPB>();
+    x = warp_reduce_op<OPA>(x);
+    y = warp_reduce_op<OPB>(y);
     if (lane == 0) {
       red[32] = x;
       red[65] = y;
     }
   }
-  sub_sync();
+  sync();
   a = red[32];
   b = red[65];
+}
+template <int OP, int G>
+__device__ __forceinline__ u128 group_reduce(u128 v, u128 *red) {
+  if (GroupOf<G>::warp) return warp_reduce_op<OP>(v);
+  if (GroupOf<G>::sub) {
+    u128 none = 0;
+    warps_reduce2<OP, 5>(v, none, red, (int)(group_rank<G>() >> 5), G / 32, [] { group_sync<G>(); });
+    return v;
+  }
+  return block_reduce<OP>(v, red);
+}
+
+template <int OPA, int OPB, int G>
+__device__ __forceinline__ void group_reduce2(u128 &a, u128 &b, u128 *red) {
+  if (GroupOf<G>::warp) {
+    a = warp_reduce_op<OPA>(a);
+    b = warp_reduce_op<OPB>(b);
+  } else if (GroupOf<G>::sub) {
+    warps_reduce2<OPA, OPB>(a, b, red, (int)(group_rank<G>() >> 5), G / 32, [] { group_sync<G>(); });
+  } else {
+    block_reduce2<OPA, OPB>(a, b, red);
+  }
+}
+
+// Reductions over warps 1.. of a CTA while warp 0 runs something else (the
+// encoder's look-back): named barrier 1 over blockDim.x - 32 threads, which all
+// of warps 1.. must reach.  `red` as block_reduce2 (66 entries).  OP as
+// block_reduce.
+__device__ __forceinline__ void sub_sync() { asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x - 32) : "memory"); }
+template <int OPA, int OPB>
+__device__ __forceinline__ void sub_reduce2(u128 &a, u128 &b, u128 *red) {
+  warps_reduce2<OPA, OPB>(a, b, red, (int)(threadIdx.x >> 5) - 1, (int)(blockDim.x >> 5) - 1, [] { sub_sync(); });
+}
+// The same over warps 1.. of a group of G threads (warp 0 of the group runs the
+// look-back): a whole CTA uses named barrier 1, a sub-group g barrier 12 + g.
+template <int G>
+__device__ __forceinline__ void group_sub_sync() {
+  if (GroupOf<G>::sub) asm volatile("bar.sync %0, %1;" ::"r"(12u + threadIdx.x / G), "n"(G - 32) : "memory");
+  else sub_sync();
+}
+template <int OPA, int OPB, int G>
+__device__ __forceinline__ void group_sub_reduce2(u128 &a, u128 &b, u128 *red) {
+  if (GroupOf<G>::sub)
+    warps_reduce2<OPA, OPB>(a, b, red, (int)(group_rank<G>() >> 5) - 1, G / 32 - 1, [] { group_sub_sync<G>(); });
+  else
+    sub_reduce2<OPA, OPB>(a, b, red);
 }
 
 // ---- relaxed global word access for the look-back scan ----------------------

@@ -268,16 +268,18 @@ __device__ __forceinline__ void write_image_packed(uint8_t *payload, uint64_t go
 //    pack rows of 32 into the body in shared memory;
 //  * other blocks (wide residuals, negative predictions, raw) recompute their
 //    residuals from the values in global memory, which are then L2-resident.
-// Needs blockDim.x >= 64 (a multiple of 32).  Shared memory: enc_smem_bytes(bs, 8)
-// -- staged words and packed body take the place of the generic encoder's
-// staged values.
-template <int G>
+// Needs a group of >= 64 threads (G = 64, 128 or the whole CTA).  Unroll depth U:
+// 2U 16-byte loads in flight per thread in the midpoint pass (U in the exact-fit
+// moment pass).  Shared memory: enc_smem_bytes(bs, 8) -- staged words and packed
+// body take the place of the generic encoder's staged values.
+template <int G, int U = 2>
 __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
   constexpr uint32_t TB = 64;
+  constexpr int UR = 2 * U, UE = U;
   EncSmem<uint64_t> sm = enc_smem<uint64_t>(smem_raw, a.bs);
   uint32_t *lo = reinterpret_cast<uint32_t *>(sm.vals);  // [round32(bs)] low words, then residuals
   uint32_t *pk = lo + ((a.bs + 31u) & ~31u);              // packed body words
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t tid = group_rank<G>(), nt = group_size<G>();
   const uint64_t base = b * a.bs;
   const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
   const uint64_t *src = reinterpret_cast<const uint64_t *>(a.values) + base;
@@ -304,7 +306,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       };
       if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, four in flight per thread
         const uint32_t np = len / 2;
-#pragma unroll 4
+#pragma unroll (UR)
         for (uint32_t q = ct; q < np; q += cn) {
           const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
           visit(((uint64_t)v.y << 32) | v.x, 2 * q);
@@ -315,7 +317,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
         for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
       }
       u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
-      sub_reduce2<3, 4>(rmx, rmn, sm.red);
+      group_sub_reduce2<3, 4, G>(rmx, rmn, sm.red);
       dmax = (int64_t)(uint64_t)rmx;
       dmin = (int64_t)(uint64_t)rmn;
       const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
@@ -341,7 +343,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       };
       if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
         const uint32_t np = len / 2;
-#pragma unroll 2
+#pragma unroll (UE)
         for (uint32_t q = ct; q < np; q += cn) {
           const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
           visit(((uint64_t)v.y << 32) | v.x, 2 * q);
@@ -352,7 +354,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
         for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
       }
       u128 sy = ((u128)shi << 32) + slo, siy = ((u128)thi << 32) + tlo;
-      sub_reduce2<0, 0>(sy, siy, sm.red);
+      group_sub_reduce2<0, 0, G>(sy, siy, sm.red);
       // lr_int_T::caltheta (lr.h:79-83) on exact moments
       const double md = __uint2double_rn(len);
       const uint64_t m = len;
@@ -387,7 +389,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
         if ((ct & 31) == 0) sm.signs[i0 / 32 + ct / 32] = ballot;
       }
       u128 rmax = rm32, none = 0;
-      sub_reduce2<1, 5>(rmax, none, sm.red);
+      group_sub_reduce2<1, 5, G>(rmax, none, sm.red);
       l = rmax ? bits_of((uint64_t)rmax) + 1 : 0;
     } else {
       const bool fast = model_in_range(m0, m1, 0.0, len);
@@ -400,7 +402,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
         rm = r > rm ? r : rm;
       }
       u128 rmax = rm, none = 0;
-      sub_reduce2<1, 5>(rmax, none, sm.red);
+      group_sub_reduce2<1, 5, G>(rmax, none, sm.red);
       l = rmax ? bits_of((uint64_t)rmax) + 1 : 0;
       if (l > TB) l = TB;
     }
@@ -514,15 +516,16 @@ __device__ __forceinline__ uint32_t legacy_residuals(const EncSmem<T> &sm, doubl
 }
 
 // Encodes block b of the column described by `a` with one thread group: the
-// whole CTA (G = 256) or one warp (G = 32, for small blocks).  The caller
+// whole CTA (G = 256), a sub-group of 64 or 128 threads, or one warp (G = 32).
+// U is the unroll depth of the u64 LeCo path (encode_block_l64).  The caller
 // guarantees that every block of the column with a smaller index was handed
 // to a group that has already started (ticket order), which makes the
 // look-back wait finite.  smem_raw: enc_smem_bytes(a.bs, sizeof(T)) bytes
 // owned by this group.
-template <typename T, int CODEC, int G = 256>
+template <typename T, int CODEC, int G = 256, int U = 2>
 __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
   if constexpr (CODEC == kLinear && sizeof(T) == 8 && G != 32) {
-    encode_block_l64<G>(a, b, smem_raw);
+    encode_block_l64<G, U>(a, b, smem_raw);
     return;
   }
   constexpr int S = sizeof(T);

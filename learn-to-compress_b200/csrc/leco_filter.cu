@@ -551,14 +551,15 @@ __global__ void __launch_bounds__(256) zonemap_kernel(DecodeLaunch a, uint64_t *
   }
   uint64_t mn = ~0ull, mx = 0;
   if (CODEC == kDelta && !raw) {
-    const DeltaChunk c = delta_chunk_start<256>(words, h, len);
-    uint64_t run = c.run;
-    for (uint32_t k = c.k0; k < c.k1; ++k) {
-      const uint64_t v = run & TM;
-      mn = v < mn ? v : mn;
-      mx = v > mx ? v : mx;
-      if (h.l && k + 1 < len) run += apply_signed(0, load_field(words, h.body_bit + (uint64_t)k * h.l, h.l), h.l);
-    }
+    delta_tiles<T, 256>(words, h, len, 0, len, [&](uint32_t k0, const auto *vs) {
+#pragma unroll
+      for (int j = 0; j < kDeltaSpan; ++j)
+        if (k0 + j < len) {
+          const uint64_t v = (uint64_t)vs[j] & TM;
+          mn = v < mn ? v : mn;
+          mx = v > mx ? v : mx;
+        }
+    });
   } else {
     const uint32_t l = raw ? TB : h.l;
     for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {

@@ -52,27 +52,38 @@ struct ServeItem {
 };
 constexpr uint32_t kServeChunk = 4096;
 
+// Delta lookups: the prefix walk of each lookup is shared by a warp (lane j adds
+// fields j, j+32, ...), the CTA's warps taking the chunk's lookups in turn.
 template <typename T>
 __device__ __forceinline__ void delta_lookups(const ServeCol &c, const uint64_t *idx, uint64_t m, T *out, uint32_t *error) {
   constexpr int S = sizeof(T);
   constexpr uint32_t TB = 8u * S;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(c.payload);
-  for (uint64_t i = threadIdx.x; i < m; i += blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t i = threadIdx.x >> 5; i < m; i += blockDim.x >> 5) {
     const uint64_t g = __ldg(idx + i);
     if (g >= c.n) {
-      out[i] = 0;
-      atomicOr(error, kErrBadIndex);
+      if (lane == 0) {
+        out[i] = 0;
+        atomicOr(error, kErrBadIndex);
+      }
       continue;
     }
     const uint64_t b = g / c.bs;
     const uint32_t k = (uint32_t)(g - b * c.bs);
     const BlockHdr h = c.dir ? from_dir<kDelta, S>(c.dir, b) : parse_header<kDelta, S>(c.payload, __ldg(c.offsets + b));
     uint64_t v = h.base;
-    if (h.l == TB) v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);
-    else if (h.l > TB) atomicOr(error, kErrBadHeader);
-    else if (h.l)
-      for (uint32_t j = 0; j < k; ++j) v += apply_signed(0, load_field(words, h.body_bit + (uint64_t)j * h.l, h.l), h.l);
-    out[i] = (T)v;
+    if (h.l == TB) {
+      v = load_field(words, h.body_bit + (uint64_t)k * TB, TB);
+    } else if (h.l > TB) {
+      if (lane == 0) atomicOr(error, kErrBadHeader);
+    } else {
+      uint64_t part = 0;
+#pragma unroll 4
+      for (uint32_t j = lane; j < k; j += 32) part += delta_field<uint64_t>(words, h, h.l ? k + 1 : 0, j);
+      v += warp_sum_u64(part);
+    }
+    if (lane == 0) out[i] = (T)v;
   }
 }
 

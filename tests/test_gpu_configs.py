@@ -8,7 +8,8 @@
   (experiments/leco_int_fix_template.cpp:158-173 decode, :194-206 random access).
 * The batching configuration at its full column count: 4096 columns of mixed
   type, family and codec (lengths log-uniform 1K-4M, capped at 32768 values so
-  the oracle finishes in seconds) through one persistent batch pass; every
+  the oracle finishes in seconds), each with the autotune table's block size,
+  threads per block and unroll depth, through one persistent batch pass; every
   column's bytes are compared with the oracle's images, not only with the
   single-column path.
 * The variable-length / degree-2 configuration at 5M keys: the host and GPU
@@ -58,8 +59,8 @@ def test_batch_config_4096_columns_against_oracle(lc, orc, dev):
     cols, host = [], []
     for x, codec, _ in workloads.batch_columns(4096, seed=3, max_len=32768):
         s = x.dtype.itemsize
-        bs = autotune.pick_block_size(codec, s, len(x), autotune.classify(x))
-        cols.append((to_dev(x, dev), codec, bs))
+        bs, g, u = autotune.pick(codec, s, len(x), autotune.classify(x))
+        cols.append((to_dev(x, dev), codec, bs, g, u))
         host.append(x)
     b = lc.Batch(cols, fit_mode=lc.FIT_REFERENCE)
     b.encode()
@@ -67,7 +68,7 @@ def test_batch_config_4096_columns_against_oracle(lc, orc, dev):
     torch.cuda.synchronize()
     lc.check()
     nbad = 0
-    for x, (xd, codec, bs), c in zip(host, cols, b.cols):
+    for x, (xd, codec, bs, _, _), c in zip(host, cols, b.cols):
         s, n = x.dtype.itemsize, len(x)
         opay, ooff = orc.encode_column(codec, x, bs)
         heads = opay[ooff[:-1].astype(np.int64)] if len(opay) else np.zeros(0, np.uint8)
