@@ -14,8 +14,9 @@ length bucket):
 
 G and U are chosen by timing a batch pass (encode + decode, replayed as a CUDA
 graph) over a batch of columns of that shape for every feasible (G, U) -- a
-combination is feasible when the 256/G blocks of an item fit the batch
-engine's 200 KB of shared memory per CTA -- keeping the engine's default
+combination is feasible when the 256/G blocks of an item fit in the ~72 KB of
+shared memory that keep three CTAs per SM (the batch encode kernel sizes every
+CTA for the largest item) -- keeping the engine's default
 (G = 32 for blocks of <= 512 values, else 256; U = 2) unless another is more
 than 2 % faster.  The table is produced on a B200 by
 ``python -m leco_b200.autotune`` (import name of this package) and committed as
@@ -39,6 +40,10 @@ UNROLLS = (1, 2, 4)
 FAMILIES = ("linear", "step", "walk", "uniform")
 LEN_BUCKETS = tuple(1 << k for k in range(10, 23, 2))  # 1K .. 4M
 BATCH_MAX_SMEM = 200 * 1024  # shared memory one work item may use (leco_batch.cu)
+# The batch encode kernel takes the largest item's shared memory for every CTA, so
+# the tuner keeps each choice within what the default launch already needs for the
+# largest blocks (16384 u32 / 8192 u64 values, ~69 KB): three CTAs per SM.
+TUNE_MAX_SMEM = 72 * 1024
 
 
 def max_block(dtype_bytes: int) -> int:
@@ -53,8 +58,8 @@ def enc_smem_bytes(bs: int, s: int) -> int:
     return (b + 15) // 16 * 16
 
 
-def feasible(bs: int, s: int, group: int) -> bool:
-    return enc_smem_bytes(bs, s) * (256 // group) <= BATCH_MAX_SMEM
+def feasible(bs: int, s: int, group: int, limit: int = TUNE_MAX_SMEM) -> bool:
+    return enc_smem_bytes(bs, s) * (256 // group) <= limit
 
 
 def default_group(bs: int) -> int:

@@ -22,182 +22,13 @@
 #include <string>
 #include <vector>
 
-#include "leco_decode.cuh"
-#include "leco_encode.cuh"
+#include "leco_batch.cuh"
 
 namespace leco {
-
-struct DevCol {
-  int32_t codec, dtype;
-  uint32_t bs, seq;
-  uint32_t group, unroll;  // threads per block (32, 64, 128, 256), unroll depth (1, 2, 4)
-  uint32_t slice, pad;     // encoder shared memory per group (bytes)
-  uint64_t n;
-  const void *values;
-  void *out;
-  uint8_t *payload;
-  uint64_t payload_cap;
-  uint64_t *offsets;
-  leco_dir_entry *dir;
-  double polyX[10];
-};
-
-__device__ __forceinline__ uint32_t find_column(const uint64_t *__restrict__ prefix, uint32_t ncols, uint64_t gb) {
-  uint32_t lo = 0, hi = ncols;  // largest c with prefix[c] <= gb
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(prefix + mid) <= gb) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-#define LECO_BATCH_DISPATCH(codec, dtype, FN, ...)                 \
-  do {                                                             \
-    if ((dtype) == 4) {                                            \
-      switch (codec) {                                             \
-        case kLinear: FN<uint32_t, kLinear>(__VA_ARGS__); break;   \
-        case kFor: FN<uint32_t, kFor>(__VA_ARGS__); break;         \
-        case kDelta: FN<uint32_t, kDelta>(__VA_ARGS__); break;     \
-        case kPoly2: FN<uint32_t, kPoly2>(__VA_ARGS__); break;     \
-      }                                                            \
-    } else {                                                       \
-      switch (codec) {                                             \
-        case kLinear: FN<uint64_t, kLinear>(__VA_ARGS__); break;   \
-        case kFor: FN<uint64_t, kFor>(__VA_ARGS__); break;         \
-        case kDelta: FN<uint64_t, kDelta>(__VA_ARGS__); break;     \
-        case kPoly2: FN<uint64_t, kPoly2>(__VA_ARGS__); break;     \
-      }                                                            \
-    }                                                              \
-  } while (0)
-
-struct BatchArgs {
-  const DevCol *cols;
-  const uint64_t *prefix;  // [ncols + 1] blocks before each column
-  const uint64_t *items;   // [nitems] (column << 32) | first block
-  uint32_t ncols;
-  uint64_t nitems;
-  uint64_t total;          // blocks in the batch
-  uint64_t *status;        // [total] look-back words (zeroed per encode pass)
-  unsigned long long *ticket;  // zeroed per pass
-  double *models;          // [total * 3] sequential-fit models
-  uint32_t *error;
-};
-
-template <typename T, int CODEC, int G, int U>
-__device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b,
-                                                 uint8_t *smem) {
-  EncodeArgs a;
-  a.values = c.values;
-  a.n = c.n;
-  a.bs = c.bs;
-  const uint64_t p0 = __ldg(B.prefix + ci);
-  a.nb = __ldg(B.prefix + ci + 1) - p0;
-  a.payload = c.payload;
-  a.payload_cap = c.payload_cap;
-  a.offsets = c.offsets;
-  a.dir = c.dir;
-  a.seq_models = c.seq ? B.models + p0 * 3 : nullptr;
-  for (int i = 0; i < 10; ++i) a.polyX[i] = c.polyX[i];
-  a.status = B.status + p0;
-  a.ticket = nullptr;
-  a.error = B.error;
-  encode_block<T, CODEC, G, U>(a, b, smem);
-}
-// The unroll depth changes only the u64 LeCo encoder; other codecs take one instance.
-template <typename T, int CODEC, int G>
-__device__ __forceinline__ void batch_encode_u(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
-  if constexpr (CODEC == kLinear && sizeof(T) == 8 && G != 32) {
-    switch (c.unroll) {
-      case 1: batch_encode_one<T, CODEC, G, 1>(B, c, ci, b, smem); return;
-      case 4: batch_encode_one<T, CODEC, G, 4>(B, c, ci, b, smem); return;
-      default: batch_encode_one<T, CODEC, G, 2>(B, c, ci, b, smem); return;
-    }
-  } else {
-    batch_encode_one<T, CODEC, G, 2>(B, c, ci, b, smem);
-  }
-}
-template <typename T, int CODEC>
-__device__ __forceinline__ void batch_encode_any(const BatchArgs &B, const DevCol &c, uint32_t ci, uint64_t b, uint8_t *smem) {
-  switch (c.group) {
-    case 32: batch_encode_u<T, CODEC, 32>(B, c, ci, b, smem); return;
-    case 64: batch_encode_u<T, CODEC, 64>(B, c, ci, b, smem); return;
-    case 128: batch_encode_u<T, CODEC, 128>(B, c, ci, b, smem); return;
-    default: batch_encode_u<T, CODEC, 256>(B, c, ci, b, smem); return;
-  }
-}
-
-template <typename T, int CODEC, int G, int U>
-__device__ __forceinline__ void batch_decode_one(const BatchArgs &B, const DevCol &c, uint64_t b) {
-  DecodeLaunch a{c.payload, c.offsets, c.n, c.bs, 0, c.n, c.out, B.error};
-  decode_block<T, CODEC, G, U>(a, b);
-}
-// The unroll depth changes the narrow-field decoder; Delta blocks take one instance.
-template <typename T, int CODEC, int G>
-__device__ __forceinline__ void batch_decode_u(const BatchArgs &B, const DevCol &c, uint64_t b) {
-  if constexpr (CODEC != kDelta) {
-    switch (c.unroll) {
-      case 1: batch_decode_one<T, CODEC, G, 1>(B, c, b); return;
-      case 4: batch_decode_one<T, CODEC, G, 4>(B, c, b); return;
-      default: batch_decode_one<T, CODEC, G, 2>(B, c, b); return;
-    }
-  } else {
-    batch_decode_one<T, CODEC, G, 2>(B, c, b);
-  }
-}
-template <typename T, int CODEC>
-__device__ __forceinline__ void batch_decode_any(const BatchArgs &B, const DevCol &c, uint64_t b) {
-  switch (c.group) {
-    case 32: batch_decode_u<T, CODEC, 32>(B, c, b); return;
-    case 64: batch_decode_u<T, CODEC, 64>(B, c, b); return;
-    case 128: batch_decode_u<T, CODEC, 128>(B, c, b); return;
-    default: batch_decode_u<T, CODEC, 256>(B, c, b); return;
-  }
-}
 
 template <typename T, int CODEC>
 __device__ __forceinline__ void batch_seq_one(const DevCol &c, uint64_t b, double *models) {
   seq_fit_block<T, CODEC>(reinterpret_cast<const T *>(c.values), c.n, c.bs, b, c.polyX, models);
-}
-
-// Persistent encode: one ticket = one work item; group g of the CTA takes block
-// first + g of the item with its own slice of shared memory.
-__global__ void __launch_bounds__(256) batch_encode_kernel(BatchArgs B) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  __shared__ unsigned long long item;
-  for (;;) {
-    if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
-    __syncthreads();
-    const uint64_t it = item;
-    __syncthreads();
-    if (it >= B.nitems) break;
-    const uint64_t e = __ldg(B.items + it);
-    const uint32_t ci = (uint32_t)(e >> 32);
-    const DevCol &c = B.cols[ci];
-    const uint32_t gi = threadIdx.x / c.group;
-    const uint64_t b = (e & 0xffffffffull) + gi;
-    if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci))
-      LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_encode_any, B, c, ci, b, smem + (size_t)gi * c.slice);
-    __syncthreads();  // shared memory is reused by the next item
-  }
-}
-
-// Persistent decode: one ticket = one work item, as the encoder.
-__global__ void __launch_bounds__(256) batch_decode_kernel(BatchArgs B) {
-  __shared__ unsigned long long item;
-  for (;;) {
-    if (threadIdx.x == 0) item = atomicAdd(B.ticket, 1ull);
-    __syncthreads();
-    const uint64_t it = item;
-    __syncthreads();
-    if (it >= B.nitems) break;
-    const uint64_t e = __ldg(B.items + it);
-    const uint32_t ci = (uint32_t)(e >> 32);
-    const DevCol &c = B.cols[ci];
-    const uint64_t b = (e & 0xffffffffull) + threadIdx.x / c.group;
-    if (b < __ldg(B.prefix + ci + 1) - __ldg(B.prefix + ci)) LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_decode_any, B, c, b);
-    __syncthreads();  // the Delta row scan's shared scratch is reused by the next item
-  }
 }
 
 // Sequential reference fits for every block of the columns that need them.

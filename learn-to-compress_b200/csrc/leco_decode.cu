@@ -249,9 +249,8 @@ __global__ void __launch_bounds__(256) gather_delta_kernel(GatherLaunch a) {
       v = 0;
       if (lane == 0) atomicOr(a.error, kErrBadHeader);
     } else {
-      uint64_t part = 0;
-#pragma unroll 4
-      for (uint32_t j = lane; j < k; j += 32) part += delta_field<uint64_t>(words, h, h.l ? k + 1 : 0, j);
+      uint64_t part = 0;  // fields j < k are the deltas before value k
+      if (h.l && k) part = h.l > 32 ? delta_walk_part<true>(words, h, k, lane) : delta_walk_part<false>(words, h, k, lane);
       v = h.base + warp_sum_u64(part);
     }
     if (lane == 0) out[i] = (T)v;

@@ -88,22 +88,45 @@ __device__ __forceinline__ uint64_t *delta_scan_scratch() {
 }
 
 // Signed Delta field i of a block (0 for fields that are not deltas, i.e. i < 0 or
-// i >= len - 1), in the value type's modular arithmetic.  Fields of up to 32 bits
-// are read through 32-bit words.
-template <typename A>
+// i >= len - 1), in the value type's modular arithmetic.  The field read is clamped
+// into the block's fields and always issued, so a run of these calls keeps all its
+// loads in flight; WIDE: fields of more than 32 bits (read through 64-bit words,
+// else 32-bit words).  Needs l > 0 and len >= 2.
+template <typename A, bool WIDE>
 __device__ __forceinline__ A delta_field(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, int64_t i) {
   const uint32_t l = h.l;
-  if (i < 0 || (uint64_t)i + 1 >= len || !l) return (A)0;
-  const uint64_t bit = h.body_bit + (uint64_t)i * l;
+  const int64_t ic = i < 0 ? 0 : (i > (int64_t)len - 2 ? (int64_t)len - 2 : i);
+  const uint64_t bit = h.body_bit + (uint64_t)ic * l;
   uint64_t f;
-  if (l <= 32) {
+  if (WIDE) {
+    f = load_field(words, bit, l);
+  } else {
     const uint32_t *w = reinterpret_cast<const uint32_t *>(words) + (bit >> 5);
     f = __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(bit & 31)) & (uint32_t)lowmask(l);
-  } else {
-    f = load_field(words, bit, l);
   }
   const uint64_t mag = f & lowmask(l - 1);
-  return ((f >> (l - 1)) & 1ull) ? (A)mag : (A)(0 - mag);
+  const A d = ((f >> (l - 1)) & 1ull) ? (A)mag : (A)(0 - mag);
+  return (i >= 0 && i == ic) ? d : (A)0;
+}
+
+// This lane's share of the prefix walk of Delta random access (read_Delta_int,
+// bit_read.h:1292-1317): the sum of fields lane, lane + 32, ... below k.  Four
+// reads in flight per lane; the warp sums the shares.
+template <bool WIDE>
+__device__ __forceinline__ uint64_t delta_walk_part(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t k,
+                                                    int lane) {
+  uint64_t part = 0;
+  for (uint32_t j0 = 0; j0 < k; j0 += 128) {  // k >= 1 here, so the block has fields 0 .. k-1
+    uint64_t d[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t j = j0 + 32 * q + lane;
+      d[q] = delta_field<uint64_t, WIDE>(words, h, k + 1, j);
+      if (j >= k) d[q] = 0;
+    }
+    part += d[0] + d[1] + d[2] + d[3];
+  }
+  return part;
 }
 
 // Delta_int<T>::decodeArray8 (delta_integer_template.h:89-127): value k =
@@ -115,10 +138,10 @@ __device__ __forceinline__ A delta_field(const uint64_t *__restrict__ words, con
 // then the warps' totals through shared memory) plus the carry of the tiles before
 // gives its first value.  EMIT(k0, v) receives the DS values k0 .. k0+DS-1 (some
 // may lie outside [lo, hi) or past the block); the group must call this together.
-constexpr int kDeltaSpan = 16;
-template <typename T, int G, typename Emit>
-__device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, uint32_t lo,
-                                            uint32_t hi, Emit emit) {
+constexpr int kDeltaSpan = 8;
+template <typename T, int G, bool WIDE, typename Emit>
+__device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len,
+                                              uint32_t lo, uint32_t hi, Emit emit) {
   using A = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;  // arithmetic mod 2^(8S)
   constexpr int DS = kDeltaSpan;
   uint64_t *wtot = delta_scan_scratch() + (GroupOf<G>::sub ? 10 * group_index<G>() : 0);
@@ -127,12 +150,13 @@ __device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, 
   const uint32_t GS = group_size<G>(), NW = GS / 32;  // NW <= 8: whole-CTA groups here have <= 256 threads
   const uint32_t TW = DS * GS;                         // values per tile
   const uint32_t t1 = (hi + TW - 1) / TW;               // tiles up to the last value wanted
+  const bool any = h.l && len >= 2;                      // a block of one value (or l = 0) has no deltas
   A carry = (A)h.base;
   for (uint32_t tl = 0; tl < t1; ++tl) {
     const uint32_t k0 = tl * TW + tid * DS;
     A v[DS];
 #pragma unroll
-    for (int j = 0; j < DS; ++j) v[j] = delta_field<A>(words, h, len, (int64_t)k0 - 1 + j);
+    for (int j = 0; j < DS; ++j) v[j] = any ? delta_field<A, WIDE>(words, h, len, (int64_t)k0 - 1 + j) : (A)0;
 #pragma unroll
     for (int j = 1; j < DS; ++j) v[j] += v[j - 1];  // inclusive prefix inside the span
     const A tot = v[DS - 1];
@@ -171,6 +195,12 @@ __device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, 
     }
     carry += tile_sum;
   }
+}
+template <typename T, int G, typename Emit>
+__device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, uint32_t lo,
+                                            uint32_t hi, Emit emit) {
+  if (h.l > 32) delta_tiles_w<T, G, true>(words, h, len, lo, hi, emit);
+  else delta_tiles_w<T, G, false>(words, h, len, lo, hi, emit);
 }
 
 // Streams CNT values (a whole number of 16-byte chunks, 16-byte aligned) to out[o0...].

@@ -7,6 +7,8 @@
 // Leco_int_poly<T,2>::encodeArray8_int (poly_fix_integer_template.h:28-91),
 // packers write_delta_int_T / write_FOR_int_T (bit_write.h:257-390).
 #pragma once
+#include <type_traits>
+
 #include "leco_device.cuh"
 #include "leco_internal.h"
 
@@ -254,6 +256,24 @@ __device__ __forceinline__ void write_image_packed(uint8_t *payload, uint64_t go
   }
 }
 
+// (int64_t)(m0 + m1*i) under conversion rule R: 0 = every prediction of the block
+// lies in [0, 2^51), both conversions on the FP64 pipe (exact); 1 = in range, plain
+// truncation; 2 = the x86 out-of-range rule (f2i_x86).
+template <int R>
+__device__ __forceinline__ int64_t lin_pred(double m0, double m1, uint32_t i) {
+  if (R == 0) return trunc_nonneg_fp64(pred_linear_fp64(m0, m1, i));
+  const double p = pred_linear(m0, m1, i);
+  return R == 1 ? __double2ll_rz(p) : f2i_x86(p);
+}
+// Calls fn(std::integral_constant<int, R>) with the cheapest rule valid for the
+// block's len predictions, so the loops inside fn carry no per-value test.
+template <typename Fn>
+__device__ __forceinline__ void with_pred_rule(double m0, double m1, uint32_t len, Fn fn) {
+  if (preds_nonneg(m0, m1, len)) fn(std::integral_constant<int, 0>{});
+  else if (model_in_range(m0, m1, 0.0, len)) fn(std::integral_constant<int, 1>{});
+  else fn(std::integral_constant<int, 2>{});
+}
+
 // Leco_int<uint64_t>::encodeArray8_int (piecewise_fix_integer_template.h:27-140)
 // for one block with a whole CTA, the same image as the generic encode_block:
 //  * warp 0 takes the block's exclusive byte offset by look-back from the start,
@@ -295,27 +315,30 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     double m0, m1;
     auto mid_pass = [&](bool stage) -> bool {  // true: residuals before the shift span < 2^30
       int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
-      const bool fast = model_in_range(m0, m1, 0.0, len);
-      auto visit = [&](uint64_t y, uint32_t i) {
-        if (stage) lo[swz32(i)] = (uint32_t)y;
-        const double p = pred_linear(m0, m1, i);
-        const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
-        const int64_t d = (int64_t)(y - (uint64_t)pr);
-        dmax = d > dmax ? d : dmax;
-        dmin = d < dmin ? d : dmin;
-      };
-      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, four in flight per thread
-        const uint32_t np = len / 2;
+      // One loop per conversion rule, chosen once per block: predictions in [0, 2^51)
+      // take both conversions on the FP64 pipe (exact); other in-range predictions
+      // the plain truncation; the rest the x86 out-of-range rule.
+      with_pred_rule(m0, m1, len, [&](auto rule) {
+        auto visit = [&](uint64_t y, uint32_t i) {
+          if (stage) lo[swz32(i)] = (uint32_t)y;
+          const int64_t pr = lin_pred<decltype(rule)::value>(m0, m1, i);
+          const int64_t d = (int64_t)(y - (uint64_t)pr);
+          dmax = d > dmax ? d : dmax;
+          dmin = d < dmin ? d : dmin;
+        };
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {  // 16-byte loads, 2U in flight per thread
+          const uint32_t np = len / 2;
 #pragma unroll (UR)
-        for (uint32_t q = ct; q < np; q += cn) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
-          visit(((uint64_t)v.y << 32) | v.x, 2 * q);
-          visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+          for (uint32_t q = ct; q < np; q += cn) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+            visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+            visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+          }
+          if ((len & 1) && ct == 0) visit(__ldg(src + len - 1), len - 1);
+        } else {
+          for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
         }
-        if ((len & 1) && ct == 0) visit(__ldg(src + len - 1), len - 1);
-      } else {
-        for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
-      }
+      });
       u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
       group_sub_reduce2<3, 4, G>(rmx, rmn, sm.red);
       dmax = (int64_t)(uint64_t)rmx;
@@ -597,14 +620,14 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
       if (CODEC == kLinear) {
         // ---- midpoint shift (piecewise_fix_integer_template.h:36-46) -----------
         int64_t dmax = (int64_t)0x8000000000000000ull, dmin = 0x7fffffffffffffffll;
-        const bool fast = model_in_range(m0, m1, 0.0, len);
-        for (uint32_t i = tid; i < len; i += nt) {
-          const double p = pred_linear(m0, m1, i);
-          const int64_t pr = fast ? __double2ll_rz(p) : f2i_x86(p);
-          int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)pr);
-          dmax = d > dmax ? d : dmax;
-          dmin = d < dmin ? d : dmin;
-        }
+        with_pred_rule(m0, m1, len, [&](auto rule) {
+          for (uint32_t i = tid; i < len; i += nt) {
+            const int64_t pr = lin_pred<decltype(rule)::value>(m0, m1, i);
+            int64_t d = (int64_t)((uint64_t)sm.vals[i] - (uint64_t)pr);
+            dmax = d > dmax ? d : dmax;
+            dmin = d < dmin ? d : dmin;
+          }
+        });
         u128 rmx = (u128)(uint64_t)dmax, rmn = (u128)(uint64_t)dmin;
         group_reduce2<3, 4, G>(rmx, rmn, sm.red);
         dmax = (int64_t)(uint64_t)rmx;
@@ -640,30 +663,34 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
           if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
         }
         rmax = rm32;
-      } else
-      for (uint32_t i0 = 0; i0 < len; i0 += nt) {
-        const uint32_t i = i0 + tid;
-        bool pos = false;
-        if (i < len) {
-          const uint64_t y = (uint64_t)sm.vals[i];
-          uint64_t r;
-          if (CODEC == kLinear) {
-            const double p = pred_linear(m0, m1, i);
-            const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
-            pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
-            r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
-          } else {
-            const double p = pred_poly2(m0, m1, m2, __uint2double_rn(i));
-            const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
-            pos = (int64_t)y > pred;
-            r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+      } else {
+        auto resid_loop = [&](auto rule) {
+          for (uint32_t i0 = 0; i0 < len; i0 += nt) {
+            const uint32_t i = i0 + tid;
+            bool pos = false;
+            if (i < len) {
+              const uint64_t y = (uint64_t)sm.vals[i];
+              uint64_t r;
+              if (CODEC == kLinear) {
+                const int64_t pred = lin_pred<decltype(rule)::value>(m0, m1, i);
+                pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
+                r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+              } else {
+                const double p = pred_poly2(m0, m1, m2, __uint2double_rn(i));
+                const int64_t pred = fast ? __double2ll_rz(p) : f2i_x86(p);
+                pos = (int64_t)y > pred;
+                r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
+              }
+              r &= (S == 8 ? ~0ull : 0xffffffffull);
+              sm.vals[i] = (T)r;
+              rmax = r > rmax ? r : rmax;
+            }
+            const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+            if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
           }
-          r &= (S == 8 ? ~0ull : 0xffffffffull);
-          sm.vals[i] = (T)r;
-          rmax = r > rmax ? r : rmax;
-        }
-        const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
-        if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
+        };
+        if (CODEC == kLinear) with_pred_rule(m0, m1, len, resid_loop);
+        else resid_loop(std::integral_constant<int, 2>{});
       }
       rmax = (uint64_t)group_reduce<1, G>((u128)rmax, sm.red);
       l = rmax ? bits_of(rmax) + 1 : 0;
