@@ -261,7 +261,8 @@ int leco_sum(int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_o
 // ---- predicate pushdown -------------------------------------------------------------
 
 uint64_t leco_filter_workspace_bytes(uint64_t n, uint32_t block_size) {
-  return leco_num_blocks(n, block_size) * 8 + 64;
+  const uint64_t nb = leco_num_blocks(n, block_size);
+  return (nb + (nb + 31) / 32) * 8 + 64;  // per-block counts, per-group totals
 }
 
 static int filter_setup(const char *fn, int codec, int dtype, const uint8_t *d_payload, const uint64_t *d_offsets,
@@ -287,12 +288,11 @@ static int filter_setup(const char *fn, int codec, int dtype, const uint8_t *d_p
   L.out = d_out;
   L.cap = d_out ? out_cap : 0;
   L.count = d_count;
-  L.status = reinterpret_cast<uint64_t *>(d_ws);
-  L.ticket = reinterpret_cast<uint32_t *>(L.status + nb);
+  L.counts = reinterpret_cast<uint64_t *>(d_ws);
+  L.group_tot = L.counts + nb;
   L.error = err;
   L.max_windows = 65536;
   L.vec_out = (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
-  LECO_CUDA(cudaMemsetAsync(d_ws, 0, nb * 8 + 8, st));
   if (!nb) LECO_CUDA(cudaMemsetAsync(d_count, 0, 8, st));
   return LECO_OK;
 }

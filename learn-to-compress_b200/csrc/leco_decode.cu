@@ -51,6 +51,14 @@ __device__ __forceinline__ uint64_t sum_block_direct(const DecodeLaunch &a, uint
   const bool raw = h.l == TB;
   const uint32_t l = raw ? TB : h.l;
   uint64_t acc = 0;
+  if (CODEC == kDelta && !raw) {
+    delta_tiles<T, 256>(words, h, len, 0, len, [&](uint32_t k0, const auto *v) {
+#pragma unroll
+      for (int j = 0; j < kDeltaSpan; ++j)
+        if (k0 + j < len) acc += (uint64_t)(T)v[j];
+    });
+    return acc;
+  }
   for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) {
     const uint64_t f = l ? load_field(words, h.body_bit + (uint64_t)k * l, l) : 0;
     acc += (uint64_t)(T)(raw ? f : value_from_field<CODEC, S>(h, k, f));
@@ -69,7 +77,9 @@ struct StageMeta {
 // blockIdx.x + gridDim.x, ...; thread 0 stages the next block's image (header +
 // packed body) into the other half of a double buffer with one cp.async.bulk
 // while the CTA decodes the current one out of shared memory.  Blocks that do
-// not fit the buffer, wide (l > 32) and Delta blocks take the direct path.
+// not fit the buffer and wide (l > 32) blocks take the direct path.  Delta blocks
+// run the row scan (delta_tiles), which synchronises the CTA, so for Delta the
+// CTA decodes a block only when every thread's wait succeeded.
 // SUM: the compressed-domain sum instead -- the values are added up, not stored,
 // and each CTA adds its total to *d_sum once.
 template <typename T, int CODEC, bool SUM = false>
@@ -115,17 +125,39 @@ __global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint
     if (tid == 0 && has_next) issue(blk + gridDim.x, cur ^ 1);
     const bool ok = mbar_wait_bounded(&bar[cur], cur ? ph1 : ph0);
     if (cur) ph1 ^= 1; else ph0 ^= 1;
-    if (ok) {  // a thread whose wait gave up touches neither the buffer nor the output
+    // a thread whose wait gave up touches neither the buffer nor the output; Delta
+    // blocks are decoded by all threads or by none (their scan has CTA barriers)
+    const bool go = CODEC == kDelta ? __syncthreads_and(ok) != 0 : ok;
+    if (go) {
       const StageMeta m = meta[cur];
       const uint8_t *sb = (cur ? buf1 : buf0);
       const uint32_t l = sb[m.hoff];
       const uint64_t base = blk * a.bs;
       const uint32_t len = (uint32_t)umin64(a.bs, a.n - base);
       const bool raw = l == 8u * S;
-      const bool narrow = (CODEC != kDelta) && (l <= 32) && (!raw || S == 4);
+      const bool narrow = (l <= 32) && (!raw || S == 4);
       if (m.direct || !narrow) {
         if (SUM) acc += sum_block_direct<T, CODEC>(a, blk);
         else decode_block<T, CODEC>(a, blk);
+      } else if (CODEC == kDelta && !raw) {
+        BlockHdr h;
+        h.l = l;
+        h.a0 = h.a1 = h.a2 = 0;
+        uint64_t w = 0;
+  #pragma unroll
+        for (int j = 0; j < S; ++j) w |= (uint64_t)sb[m.hoff + 1 + j] << (8 * j);
+        h.base = w;
+        h.body_bit = (uint64_t)(m.hoff + Hdr<CODEC, S>::bytes) * 8;
+        const uint64_t *sw = reinterpret_cast<const uint64_t *>(sb);
+        if (SUM) {
+          delta_tiles<T, 256, true>(sw, h, len, 0, len, [&](uint32_t k0, const auto *v) {
+  #pragma unroll
+            for (int j = 0; j < kDeltaSpan; ++j)
+              if (k0 + j < len) acc += (uint64_t)(T)v[j];
+          });
+        } else {
+          delta_tiles<T, 256, true>(sw, h, len, 0, len, DeltaStore<T>{out, base, 0, len});
+        }
       } else {
         BlockHdr h;
         h.l = l;
@@ -317,7 +349,7 @@ static void run_decode(const DecodeLaunch &L, cudaStream_t st) {
   const uint64_t b0 = L.first / L.bs, b1 = (L.first + L.count - 1) / L.bs;
   const uint64_t nblk = b1 - b0 + 1;
   const bool staged = L.first == 0 && L.count == L.n && (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 &&
-                      CODEC != kDelta && CODEC != kLegacy && nblk >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
+                      CODEC != kLegacy && nblk >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
   if (!staged) {
     if (L.bs <= kWarpBlock) decode_kernel_warp<T, CODEC><<<(unsigned)((nblk + 7) / 8), 256, 0, st>>>(L, nblk);
     else decode_kernel<T, CODEC><<<(unsigned)nblk, 256, 0, st>>>(L);
@@ -338,7 +370,7 @@ template <typename T, int CODEC>
 static void run_sum(const DecodeLaunch &L, uint64_t *d_sum, cudaStream_t st) {
   const uint64_t nb = (L.n + L.bs - 1) / L.bs;
   if (!nb) return;
-  const bool staged = (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 && CODEC != kDelta && CODEC != kLegacy &&
+  const bool staged = (reinterpret_cast<uintptr_t>(L.payload) & 15) == 0 && CODEC != kLegacy &&
                       nb >= 1024 && L.bs > kWarpBlock && staged_decode_enabled();
   if (!staged) {
     sum_kernel<T, CODEC><<<(unsigned)nb, 256, 0, st>>>(L, d_sum);

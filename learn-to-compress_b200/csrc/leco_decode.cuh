@@ -79,6 +79,21 @@ __device__ __forceinline__ uint64_t value_from_field(const BlockHdr &h, uint32_t
   return h.l ? apply_signed((uint64_t)pred, f, h.l) : (uint64_t)pred;
 }
 
+// Streams CNT values (a whole number of 16-byte chunks, 16-byte aligned) to out[o0...].
+template <typename T, int CNT>
+__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v) {
+  if (sizeof(T) == 8) {
+#pragma unroll
+    for (int c = 0; c < CNT / 2; ++c)
+      __stcs(reinterpret_cast<ulonglong2 *>(out + o0 + 2 * c), make_ulonglong2(v[2 * c], v[2 * c + 1]));
+  } else {
+#pragma unroll
+    for (int c = 0; c < CNT / 4; ++c)
+      __stcs(reinterpret_cast<uint4 *>(out + o0 + 4 * c),
+             make_uint4((uint32_t)v[4 * c], (uint32_t)v[4 * c + 1], (uint32_t)v[4 * c + 2], (uint32_t)v[4 * c + 3]));
+  }
+}
+
 // Scratch of the Delta scan: 10 words for each of up to four groups of a CTA.  One
 // non-template function, so every kernel holds a single copy however many decoder
 // instances it contains.
@@ -91,9 +106,11 @@ __device__ __forceinline__ uint64_t *delta_scan_scratch() {
 // i >= len - 1), in the value type's modular arithmetic.  The field read is clamped
 // into the block's fields and always issued, so a run of these calls keeps all its
 // loads in flight; WIDE: fields of more than 32 bits (read through 64-bit words,
-// else 32-bit words).  Needs l > 0 and len >= 2.
-template <typename A, bool WIDE>
+// else 32-bit words); SMEM: `words` is a staged copy in shared memory (narrow
+// fields only).  Needs l > 0 and len >= 2.
+template <typename A, bool WIDE, bool SMEM = false>
 __device__ __forceinline__ A delta_field(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, int64_t i) {
+  static_assert(!(WIDE && SMEM), "staged Delta blocks have fields of at most 32 bits");
   const uint32_t l = h.l;
   const int64_t ic = i < 0 ? 0 : (i > (int64_t)len - 2 ? (int64_t)len - 2 : i);
   const uint64_t bit = h.body_bit + (uint64_t)ic * l;
@@ -102,7 +119,8 @@ __device__ __forceinline__ A delta_field(const uint64_t *__restrict__ words, con
     f = load_field(words, bit, l);
   } else {
     const uint32_t *w = reinterpret_cast<const uint32_t *>(words) + (bit >> 5);
-    f = __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(bit & 31)) & (uint32_t)lowmask(l);
+    const uint32_t w0 = SMEM ? w[0] : __ldg(w), w1 = SMEM ? w[1] : __ldg(w + 1);
+    f = __funnelshift_r(w0, w1, (uint32_t)(bit & 31)) & (uint32_t)lowmask(l);
   }
   const uint64_t mag = f & lowmask(l - 1);
   const A d = ((f >> (l - 1)) & 1ull) ? (A)mag : (A)(0 - mag);
@@ -139,7 +157,7 @@ __device__ __forceinline__ uint64_t delta_walk_part(const uint64_t *__restrict__
 // gives its first value.  EMIT(k0, v) receives the DS values k0 .. k0+DS-1 (some
 // may lie outside [lo, hi) or past the block); the group must call this together.
 constexpr int kDeltaSpan = 8;
-template <typename T, int G, bool WIDE, typename Emit>
+template <typename T, int G, bool WIDE, bool SMEM, typename Emit>
 __device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len,
                                               uint32_t lo, uint32_t hi, Emit emit) {
   using A = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;  // arithmetic mod 2^(8S)
@@ -156,7 +174,7 @@ __device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words
     const uint32_t k0 = tl * TW + tid * DS;
     A v[DS];
 #pragma unroll
-    for (int j = 0; j < DS; ++j) v[j] = any ? delta_field<A, WIDE>(words, h, len, (int64_t)k0 - 1 + j) : (A)0;
+    for (int j = 0; j < DS; ++j) v[j] = any ? delta_field<A, WIDE, SMEM>(words, h, len, (int64_t)k0 - 1 + j) : (A)0;
 #pragma unroll
     for (int j = 1; j < DS; ++j) v[j] += v[j - 1];  // inclusive prefix inside the span
     const A tot = v[DS - 1];
@@ -196,27 +214,36 @@ __device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words
     carry += tile_sum;
   }
 }
-template <typename T, int G, typename Emit>
+// SMEM: `words` is a staged copy of the block in shared memory, whose fields are
+// at most 32 bits wide.
+template <typename T, int G, bool SMEM = false, typename Emit>
 __device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, const BlockHdr &h, uint32_t len, uint32_t lo,
                                             uint32_t hi, Emit emit) {
-  if (h.l > 32) delta_tiles_w<T, G, true>(words, h, len, lo, hi, emit);
-  else delta_tiles_w<T, G, false>(words, h, len, lo, hi, emit);
+  if (SMEM || h.l <= 32) delta_tiles_w<T, G, false, SMEM>(words, h, len, lo, hi, emit);
+  else delta_tiles_w<T, G, true, false>(words, h, len, lo, hi, emit);
 }
-
-// Streams CNT values (a whole number of 16-byte chunks, 16-byte aligned) to out[o0...].
-template <typename T, int CNT>
-__device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *v) {
-  if (sizeof(T) == 8) {
+// Emitter of delta_tiles that stores the values of [lo, hi) to out[obase + k]:
+// 16-byte stores for a span wholly inside and aligned, else one value at a time.
+template <typename T>
+struct DeltaStore {
+  T *out;
+  uint64_t obase;
+  uint32_t lo, hi;
+  template <typename A>
+  __device__ __forceinline__ void operator()(uint32_t k0, const A *v) const {
+    T *o = out + obase + k0;
+    if (k0 >= lo && k0 + kDeltaSpan <= hi && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+      uint64_t w[kDeltaSpan];
 #pragma unroll
-    for (int c = 0; c < CNT / 2; ++c)
-      __stcs(reinterpret_cast<ulonglong2 *>(out + o0 + 2 * c), make_ulonglong2(v[2 * c], v[2 * c + 1]));
-  } else {
+      for (int j = 0; j < kDeltaSpan; ++j) w[j] = (uint64_t)v[j];
+      store_vals<T, kDeltaSpan>(out, obase + k0, w);
+    } else {
 #pragma unroll
-    for (int c = 0; c < CNT / 4; ++c)
-      __stcs(reinterpret_cast<uint4 *>(out + o0 + 4 * c),
-             make_uint4((uint32_t)v[4 * c], (uint32_t)v[4 * c + 1], (uint32_t)v[4 * c + 2], (uint32_t)v[4 * c + 3]));
+      for (int j = 0; j < kDeltaSpan; ++j)
+        if (k0 + j >= lo && k0 + j < hi) o[j] = (T)v[j];
+    }
   }
-}
+};
 
 // True when every prediction of the block is a finite double inside
 // (-2^63, 2^63), so the x86 out-of-range rule of f2i_x86 can never apply:
@@ -331,19 +358,7 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   const bool raw = h.l == TB;
 
   if (CODEC == kDelta && !raw) {
-    delta_tiles<T, G>(words, h, len, lo, hi, [&](uint32_t k0, const auto *v) {
-      T *o = out + obase + k0;
-      if (k0 >= lo && k0 + kDeltaSpan <= hi && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
-        uint64_t w[kDeltaSpan];
-#pragma unroll
-        for (int j = 0; j < kDeltaSpan; ++j) w[j] = (uint64_t)v[j];
-        store_vals<T, kDeltaSpan>(out, obase + k0, w);
-      } else {
-#pragma unroll
-        for (int j = 0; j < kDeltaSpan; ++j)
-          if (k0 + j >= lo && k0 + j < hi) o[j] = (T)v[j];
-      }
-    });
+    delta_tiles<T, G>(words, h, len, lo, hi, DeltaStore<T>{out, obase, lo, hi});
     return;
   }
 

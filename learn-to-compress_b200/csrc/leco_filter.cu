@@ -12,15 +12,13 @@
 // The output is uint32 global indices b*block_size + k, blocks in order, each
 // block's indices in the order the reference emits them.
 //
-// One warp per block, blocks taken in ticket order; the output offset of a
-// block is the exclusive prefix of the match counts, found by decoupled
-// look-back (the single-pass scan the encoder uses for byte offsets).  Before
-// reading any field, a block (or window) is classified from its model's value
-// bounds, its FOR header or the zone map: all indices match, none do, or the
-// values must be read.  Read blocks are evaluated twice: a counting pass that
-// keeps the match bitmap in shared memory and, once the offset is known, a
-// writing pass (bitmap read back, or the windows evaluated again from
-// L1-resident fields).
+// Three launches: a counting pass (one warp per 32 blocks), an exclusive scan of
+// the per-group totals, and a writing pass (one warp per block with matches),
+// whose output position is its group's prefix plus the counts of the group's
+// earlier blocks.  Before reading any field, a block (or window) is classified
+// from its model's value bounds, its FOR header or the zone map: all indices
+// match, none do, or the values must be read.  Read blocks (and window loops)
+// are evaluated in both passes; every other block reads only its plan.
 #include <algorithm>
 
 #include "leco_decode.cuh"
@@ -92,11 +90,7 @@ __device__ __forceinline__ bool single_pred(int pred, uint64_t v, uint64_t f1, u
   return v > f1 && f2 > f1 && ((v - f1 - 1) % base) + 1 < f2 - f1;
 }
 
-// One warp per block.  A CTA takes kFB consecutive blocks by one ticket; its
-// warps are then independent: each counts its block, finds its output offset by
-// look-back (the CTA's earlier warps and earlier CTAs are all resident or done,
-// so every wait ends) and writes; no CTA barrier after the ticket.
-constexpr int kFB = kFT / 32;            // warps (blocks in flight) per CTA
+constexpr int kFB = kFT / 32;            // warps per CTA
 constexpr uint32_t kFWin = 32;           // windows per chunk (close range), one per lane
 
 // How a window's values relate to its bounds, decided from the block model
@@ -393,14 +387,12 @@ __device__ __forceinline__ BlockPlan shfl_plan(const BlockPlan &q, int src) {
   return p;
 }
 
-// Matches of one block (warp-uniform), keeping the match bitmap of a read
-// single-window block in `mask`.
-template <int S, int CODEC>
-__device__ __forceinline__ uint64_t count_block(const FilterLaunch &a, const BlockPlan &p, uint32_t *mask) {
-  const uint32_t lane = threadIdx.x & 31;
-  if (p.pred == kPredWindows) return window_loop<S, CODEC, false>(a, p, 0);
-  if (p.mode == kAll) return p.hi - p.lo;
-  if (p.mode != kEval) return 0;
+// Evaluates a read single-window block [p.lo, p.hi) 32*kFU indices per step,
+// all fields of a step in flight.  Counts; with WRITE also stores the matches
+// from out position `run` on (positions at or past cap are dropped).
+template <int S, int CODEC, bool WRITE>
+__device__ __forceinline__ uint64_t eval_block(const FilterLaunch &a, const BlockPlan &p, uint64_t run) {
+  const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
   const uint64_t step = a.base & (S == 8 ? ~0ull : 0xffffffffull);
   uint64_t cnt = 0;
@@ -415,17 +407,28 @@ __device__ __forceinline__ uint64_t count_block(const FilterLaunch &a, const Blo
     }
 #pragma unroll
     for (int u = 0; u < kFU; ++u) {
-      if (lane == u) mask[((s0 - p.lo) >> 5) + u] = m[u];
+      if (WRITE && ((m[u] >> lane) & 1u)) {
+        const uint64_t pos = run + cnt + __popc(m[u] & lt);
+        if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + s0 + u * 32 + lane);
+      }
       cnt += __popc(m[u]);
     }
   }
   return cnt;
 }
 
-// Writes the matches of one block from output position `run` on.
+// Matches of one block (warp-uniform).
 template <int S, int CODEC>
-__device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPlan &p, const uint32_t *mask, uint64_t run) {
-  const uint32_t lane = threadIdx.x & 31;
+__device__ __forceinline__ uint64_t count_block(const FilterLaunch &a, const BlockPlan &p) {
+  if (p.pred == kPredWindows) return window_loop<S, CODEC, false>(a, p, 0);
+  if (p.mode == kAll) return p.hi - p.lo;
+  if (p.mode != kEval) return 0;
+  return eval_block<S, CODEC, false>(a, p, 0);
+}
+
+// Writes the matches of one block from output position `run` on (warp-uniform).
+template <int S, int CODEC>
+__device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPlan &p, uint64_t run) {
   if (p.pred == kPredWindows) {
     window_loop<S, CODEC, true>(a, p, run);
     return;
@@ -434,90 +437,94 @@ __device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPl
     write_run(a, run, (uint32_t)(p.vbase + p.lo), p.hi - p.lo);
     return;
   }
-  const uint32_t nwords = (p.hi - p.lo + 31) >> 5;
-  const uint32_t lt = (1u << lane) - 1u;
-  for (uint32_t w0 = 0; w0 < nwords; w0 += kFU) {
-    uint32_t m[kFU];
-#pragma unroll
-    for (int u = 0; u < kFU; ++u) m[u] = w0 + u < nwords ? mask[w0 + u] : 0u;
-#pragma unroll
-    for (int u = 0; u < kFU; ++u) {
-      if ((m[u] >> lane) & 1u) {
-        const uint64_t pos = run + __popc(m[u] & lt);
-        if (pos < a.cap) a.out[pos] = (uint32_t)(p.vbase + p.lo + (w0 + u) * 32 + lane);
-      }
-      run += __popc(m[u]);
-    }
-  }
+  if (p.mode == kEval) eval_block<S, CODEC, true>(a, p, run);
 }
 
-// One warp per group of a.group consecutive blocks (at most 32).  A CTA takes
-// kFB groups by one ticket.  Lane j plans block j of its warp's group (all
-// header, offset and zone-map loads of the group in flight at once), the warp
-// counts its blocks one after another, the CTA finds its output offset by one
-// look-back over CTAs (earlier CTAs are resident or done, so every wait ends),
-// and every warp writes its blocks.
+// ---- pass 1: match counts --------------------------------------------------------
+// One warp per group of 32 consecutive blocks: lane j plans block j (all header,
+// offset and zone-map loads of the group in flight at once); blocks decided by
+// their plan are counted from it, the others (read blocks, window loops) by the
+// whole warp one after another.  Writes counts[b] and the group's total.
 template <int S, int CODEC>
-__global__ void __launch_bounds__(kFT, 3) filter_kernel(FilterLaunch a, int close) {
-  extern __shared__ __align__(16) uint32_t fmask[];
-  __shared__ uint32_t cta_ticket;
-  __shared__ uint64_t warp_tot[kFB], warp_excl[kFB];
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t *mask = fmask + (size_t)warp * a.group * a.mask_words;
-  if (threadIdx.x == 0) cta_ticket = atomicAdd(a.ticket, 1u);
-  __syncthreads();
-  const uint64_t grp = (uint64_t)cta_ticket * kFB + warp;
-  const uint64_t b0 = grp * a.group;
-  // warps past the column still take part in the CTA's barriers, with no blocks
-  const uint32_t nblk = b0 < a.nb ? (uint32_t)umin64(a.group, a.nb - b0) : 0u;
-
-  // ---- counting -----------------------------------------------------------------
+__global__ void __launch_bounds__(kFT) filter_count_kernel(FilterLaunch a, int close) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t g = (uint64_t)blockIdx.x * kFB + (threadIdx.x >> 5);
+  const uint64_t b0 = g * 32;
+  if (b0 >= a.nb) return;  // whole warps only
+  const uint32_t nblk = (uint32_t)umin64(32, a.nb - b0);
   BlockPlan mine;
-  if (lane < nblk) mine = plan_block<S, CODEC>(a, b0 + lane, close);
   uint64_t mycnt = 0;
-  for (uint32_t j = 0; j < nblk; ++j) {
-    const BlockPlan p = shfl_plan(mine, j);
-    const uint64_t c = count_block<S, CODEC>(a, p, mask + j * a.mask_words);
-    if (lane == j) mycnt = c;
+  bool read = false;
+  if (lane < nblk) {
+    mine = plan_block<S, CODEC>(a, b0 + lane, close);
+    read = mine.pred == kPredWindows || mine.mode == kEval;
+    if (!read && mine.mode == kAll) mycnt = mine.hi - mine.lo;
   }
-
-  // ---- output offset: the CTA's total by look-back over CTAs, then the warps' ------
-  // (one look-back per CTA: a per-warp look-back over all warps of a single wave
-  // walks back through ~warps/32 windows of aggregates, one L2 round trip each)
+  for (uint32_t need = __ballot_sync(0xffffffffu, read); need; need &= need - 1) {
+    const int j = __ffs(need) - 1;
+    const BlockPlan p = shfl_plan(mine, j);
+    const uint64_t c = count_block<S, CODEC>(a, p);
+    if (lane == (uint32_t)j) mycnt = c;
+  }
+  if (lane < nblk) a.counts[b0 + lane] = mycnt;
   const uint64_t tot = warp_sum_u64(mycnt);
-  if (lane == 0) warp_tot[warp] = tot;
-  __syncthreads();
-  if (warp == 0) {
-    const uint64_t wt = lane < kFB ? warp_tot[lane] : 0;
-    uint64_t inc = wt;
-    for (int d = 1; d < kFB; d <<= 1) {
-      const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
-      if (lane >= (uint32_t)d) inc += y;
-    }
-    const uint64_t cta_tot = __shfl_sync(0xffffffffu, inc, kFB - 1);
-    const uint64_t cexcl = lookback_prefix(a.status, cta_ticket, cta_tot, a.error);
-    if (lane < kFB) warp_excl[lane] = cexcl == ~0ull ? ~0ull : cexcl + inc - wt;
-    const uint64_t groups = (a.nb + a.group - 1) / a.group;
-    if (lane == 0 && cexcl != ~0ull && ((uint64_t)cta_ticket + 1) * kFB >= groups) *a.count = cexcl + cta_tot;
-  }
-  __syncthreads();
-  const uint64_t excl = warp_excl[warp];
-  if (excl == ~0ull) return;  // a predecessor never published: error word set
-  if (!tot) return;
-  uint64_t inc = mycnt;
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
-    if (lane >= (uint32_t)d) inc += y;
-  }
-  const uint64_t myoff = excl + inc - mycnt;
-  __syncwarp();  // bitmap words written by other lanes
+  if (lane == 0) a.group_tot[g] = tot;
+}
 
-  // ---- writing ------------------------------------------------------------------
-  for (uint32_t j = 0; j < nblk; ++j) {
-    if (!__shfl_sync(0xffffffffu, mycnt, j)) continue;
-    const BlockPlan p = shfl_plan(mine, j);
-    write_block<S, CODEC>(a, p, mask + j * a.mask_words, __shfl_sync(0xffffffffu, myoff, j));
+// ---- pass 2: exclusive scan of the group totals (one CTA of 1024 threads) ----------
+// group_tot[g] becomes the output position of group g's first match; *count the
+// total number of matches.
+__global__ void __launch_bounds__(1024) filter_scan_kernel(uint64_t *group_tot, uint64_t ngroups, uint64_t *count) {
+  __shared__ uint64_t wsum[33];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t carry = 0;
+  for (uint64_t base = 0; base < ngroups; base += 1024) {
+    const uint64_t i = base + tid;
+    const uint64_t v = i < ngroups ? group_tot[i] : 0;
+    uint64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint64_t x = wsum[lane];
+      uint64_t xi = x;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, xi, o);
+        if (lane >= (uint32_t)o) xi += y;
+      }
+      wsum[lane] = xi - x;
+      if (lane == 31) wsum[32] = xi;
+    }
+    __syncthreads();
+    if (i < ngroups) group_tot[i] = carry + wsum[warp] + incl - v;
+    carry += wsum[32];
+    __syncthreads();  // wsum is rewritten by the next chunk
   }
+  if (tid == 0) *count = carry;
+}
+
+// ---- pass 3: writing ------------------------------------------------------------------
+// One warp per block with matches: its output position is its group's prefix plus
+// the counts of the group's earlier blocks; the block is planned again and its
+// matches written (runs of indices with 16-byte stores, read blocks re-evaluated).
+template <int S, int CODEC>
+__global__ void __launch_bounds__(kFT) filter_write_kernel(FilterLaunch a, int close) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t b = (uint64_t)blockIdx.x * kFB + (threadIdx.x >> 5);
+  if (b >= a.nb) return;  // whole warps only
+  if (!__ldg(a.counts + b)) return;
+  const uint64_t g = b >> 5;
+  const uint32_t j = (uint32_t)(b & 31);
+  const uint64_t before = lane < j ? __ldg(a.counts + (g << 5) + lane) : 0;
+  const uint64_t run = __ldg(a.group_tot + g) + warp_sum_u64(before);
+  BlockPlan mine;
+  if (lane == 0) mine = plan_block<S, CODEC>(a, b, close);
+  write_block<S, CODEC>(a, shfl_plan(mine, 0), run);
 }
 
 // ---- zone map: per-block minimum and maximum of the decoded values -------------------
@@ -579,12 +586,10 @@ __global__ void __launch_bounds__(256) zonemap_kernel(DecodeLaunch a, uint64_t *
 
 template <int S, int CODEC>
 static int run_filter(FilterLaunch L, int close, cudaStream_t st) {
-  L.mask_words = (L.bs + 127) / 128 * 4;
-  L.group = std::max(1u, std::min(32u, 1024u / L.mask_words));  // 4 KB of bitmaps per warp
-  const int smem = (int)(kFB * L.group * L.mask_words * 4);
-  if (cudaFuncSetAttribute(filter_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
-  const uint64_t groups = (L.nb + L.group - 1) / L.group;
-  filter_kernel<S, CODEC><<<(unsigned)((groups + kFB - 1) / kFB), kFT, smem, st>>>(L, close);
+  const uint64_t groups = (L.nb + 31) / 32;
+  filter_count_kernel<S, CODEC><<<(unsigned)((groups + kFB - 1) / kFB), kFT, 0, st>>>(L, close);
+  filter_scan_kernel<<<1, 1024, 0, st>>>(L.group_tot, groups, L.count);
+  filter_write_kernel<S, CODEC><<<(unsigned)((L.nb + kFB - 1) / kFB), kFT, 0, st>>>(L, close);
   return 0;
 }
 

@@ -60,12 +60,10 @@ struct FilterLaunch {
   uint32_t *out;
   uint64_t cap;
   uint64_t *count;
-  uint64_t *status;      // look-back words, nb of them, zeroed
-  uint32_t *ticket;      // zeroed
+  uint64_t *counts;      // [nb] matches per block (workspace)
+  uint64_t *group_tot;   // [ceil(nb/32)] matches per group of 32 blocks, then their exclusive prefix (workspace)
   uint32_t *error;
   uint32_t max_windows;  // close-range LeCo: windows per block before kErrLimit (a multiple of 32)
-  uint32_t mask_words;   // per-block match bitmap words (set by the launcher)
-  uint32_t group;        // blocks per warp (set by the launcher)
   int vec_out;           // out is 16-byte aligned: runs of indices are written with 16-byte stores
 };
 

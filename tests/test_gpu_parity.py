@@ -226,7 +226,8 @@ def test_reference_fit_large_columns(lc, orc, dev, s, codec, bs, shift):
 def test_staged_decode_large_mixed(lc, orc, dev, s):
     """Columns of >= 1024 blocks take the persistent TMA-staged decoder; mix
     narrow blocks (staged), blocks wider than 32 bits and raw blocks (decoded
-    from global memory) in one column."""
+    from global memory) in one column.  Delta blocks run the row scan on the
+    staged copy (narrow) or on global memory (wide, raw)."""
     import torch
     rng = np.random.default_rng(99 + s)
     dt = np.uint64 if s == 8 else np.uint32
@@ -240,7 +241,7 @@ def test_staged_decode_large_mixed(lc, orc, dev, s):
     x = x.astype(np.uint64)
     unif = rng.integers(0, top, n, dtype=np.uint64)
     x = np.where(seg == 2, unif, x).astype(dt)                # raw blocks
-    for codec in (0, 1, 3):
+    for codec in (0, 1, 2, 3):
         for bs in (1000, 2048):
             col = lc.encode(to_dev(x, dev), codec, bs, lc.FIT_EXACT)
             assert col.nblocks >= 1024
