@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter", "gather"],
+    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter", "gather", "codecs"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
@@ -661,6 +661,72 @@ def run_gather(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_codecs(args, world, rank, local):
+    """Each fixed-block codec (LeCo linear, FOR, Delta, degree-2) on the decode
+    workload's column (200M u64 keys, 4096-value blocks) and on its low 32 bits
+    as u32: bulk decode, 2^24 uniform lookups (2^20 for Delta, whose random
+    access walks the block), compressed-domain sum, encode (reference fit);
+    every result checked against the keys."""
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    x64 = workloads.piecewise_linear_u64(n, seed=2 + rank, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def ev(fn, reps=5):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {}
+    with ClockSampler(local) as clk:
+        for s, x in ((8, x64), (4, (x64 & 0xFFFFFFFF).to(torch.int32))):
+            out = torch.empty_like(x)
+            for name, codec in (("leco", lc.LINEAR), ("for", lc.FOR), ("delta", lc.DELTA), ("poly2", lc.POLY2)):
+                col = lc.encode(x, codec, BS, lc.FIT_REFERENCE)
+                m = (1 << 20) if codec == lc.DELTA else RA_BATCH
+                idx = torch.randint(0, n, (m,), device=dev)
+                ra = torch.empty(m, dtype=x.dtype, device=dev)
+                r = {"ratio": round(col.nbytes / (n * s), 5),
+                     "encode_ms": round(ev(lambda: lc.encode(x, codec, BS, lc.FIT_REFERENCE, payload=col.payload), 3), 4),
+                     "decode_ms": round(ev(lambda: col.decode(out=out)), 4),
+                     "sum_ms": round(ev(lambda: col.sum()), 4),
+                     "lookups": m, "gather_ms": round(ev(lambda: col.gather(idx, out=ra)), 4)}
+                col = lc.encode(x, codec, BS, lc.FIT_REFERENCE)
+                assert torch.equal(col.decode(out=out), x), (name, s)
+                assert torch.equal(col.gather(idx, out=ra), x[idx]), (name, s)
+                mask = 0xFFFFFFFFFFFFFFFF if s == 8 else 0xFFFFFFFF
+                want = int((x.to(torch.int64) & mask).sum().item()) & 0xFFFFFFFFFFFFFFFF
+                assert col.sum() == want, (name, s)
+                r["decode_gbs"] = round(n * s / r["decode_ms"] / 1e6, 1)
+                r["mlookups_s"] = round(m / r["gather_ms"] / 1e3, 1)
+                res[f"{name}_u{8 * s}"] = r
+                del col
+    lc.check()
+    if rank == 0:
+        head = res["delta_u64"]
+        line = {"metric": f"fixed-block codecs on {n // 1_000_000}M keys: decode GB/s, random access, sum, encode",
+                "value": head["decode_gbs"], "unit": "GB/s", "n_gpus": world, "steps": 5, "warmup": 2,
+                "ms_per_step": head["decode_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u64+u32", "data": "synthetic",
+                "config": {"workload": f"{n} piecewise-linear keys (u64, and their low 32 bits as u32), {BS}-value "
+                                       "blocks, each codec; value = Delta u64 decode", "keys": n},
+                "clocks": clk.summary(), **res}
+        print(json.dumps(line), flush=True)
+
+
 def to_np_u64(t):
     return t.cpu().numpy().view(np.uint64)
 
@@ -685,6 +751,9 @@ def main():
         return
     if args.workload == "gather":
         run_gather(args, world, rank, local)
+        return
+    if args.workload == "codecs":
+        run_codecs(args, world, rank, local)
         return
 
     import torch

@@ -51,14 +51,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = os.environ.get("NVCC", "nvcc")
     extra = ["-Xptxas=-v"] if verbose else []
     jobs = []
+    newest_header = max(os.path.getmtime(f) for f in headers() + [__file__])
     for src in sources():
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
-        jobs.append((obj, [nvcc, *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]))
+        # an object is reused only when it is newer than its source, every header and this script
+        fresh = (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
+                 and os.path.getmtime(obj) >= newest_header)
+        jobs.append((obj, None if fresh else [nvcc, *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]))
     if verbose:
         for _, cmd in jobs:
-            print(" ".join(cmd), file=sys.stderr)
-    procs = [subprocess.Popen(cmd) for _, cmd in jobs]
-    failed = [" ".join(cmd) for p, (_, cmd) in zip(procs, jobs) if p.wait() != 0]
+            if cmd:
+                print(" ".join(cmd), file=sys.stderr)
+    procs = [(subprocess.Popen(cmd), cmd) for _, cmd in jobs if cmd]
+    failed = [" ".join(cmd) for p, cmd in procs if p.wait() != 0]
     if failed:
         raise subprocess.CalledProcessError(1, failed[0])
     subprocess.check_call([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *[o for o, _ in jobs], "-lpthread"])

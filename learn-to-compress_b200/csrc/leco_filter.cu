@@ -440,6 +440,11 @@ __device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPl
   if (p.mode == kEval) eval_block<S, CODEC, true>(a, p, run);
 }
 
+// counts[b]: the block's match count in the low 40 bits; a block whose matches are
+// one run of indices [lo, lo + count) known from its plan alone also carries
+// kRunFlag and lo (bits 40..62), so the writing pass needs no second plan for it.
+constexpr uint64_t kCountMask = (1ull << 40) - 1, kRunFlag = 1ull << 63;
+
 // ---- pass 1: match counts --------------------------------------------------------
 // One warp per group of 32 consecutive blocks: lane j plans block j (all header,
 // offset and zone-map loads of the group in flight at once); blocks decided by
@@ -466,7 +471,10 @@ __global__ void __launch_bounds__(kFT) filter_count_kernel(FilterLaunch a, int c
     const uint64_t c = count_block<S, CODEC>(a, p);
     if (lane == (uint32_t)j) mycnt = c;
   }
-  if (lane < nblk) a.counts[b0 + lane] = mycnt;
+  if (lane < nblk) {
+    const bool run = !read && mine.mode == kAll && mycnt;
+    a.counts[b0 + lane] = mycnt | (run ? kRunFlag | ((uint64_t)mine.lo << 40) : 0);
+  }
   const uint64_t tot = warp_sum_u64(mycnt);
   if (lane == 0) a.group_tot[g] = tot;
 }
@@ -510,18 +518,24 @@ __global__ void __launch_bounds__(1024) filter_scan_kernel(uint64_t *group_tot, 
 
 // ---- pass 3: writing ------------------------------------------------------------------
 // One warp per block with matches: its output position is its group's prefix plus
-// the counts of the group's earlier blocks; the block is planned again and its
-// matches written (runs of indices with 16-byte stores, read blocks re-evaluated).
+// the counts of the group's earlier blocks.  A single run of indices is written
+// straight from counts[b] (16-byte stores); other blocks are planned again and
+// their matches written (read blocks and window loops evaluated again).
 template <int S, int CODEC>
 __global__ void __launch_bounds__(kFT) filter_write_kernel(FilterLaunch a, int close) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t b = (uint64_t)blockIdx.x * kFB + (threadIdx.x >> 5);
   if (b >= a.nb) return;  // whole warps only
-  if (!__ldg(a.counts + b)) return;
+  const uint64_t w = __ldg(a.counts + b);
+  if (!(w & kCountMask)) return;
   const uint64_t g = b >> 5;
   const uint32_t j = (uint32_t)(b & 31);
-  const uint64_t before = lane < j ? __ldg(a.counts + (g << 5) + lane) : 0;
+  const uint64_t before = lane < j ? __ldg(a.counts + (g << 5) + lane) & kCountMask : 0;
   const uint64_t run = __ldg(a.group_tot + g) + warp_sum_u64(before);
+  if (w & kRunFlag) {
+    write_run(a, run, (uint32_t)(b * a.bs + ((w >> 40) & 0x7fffff)), (uint32_t)(w & kCountMask));
+    return;
+  }
   BlockPlan mine;
   if (lane == 0) mine = plan_block<S, CODEC>(a, b, close);
   write_block<S, CODEC>(a, shfl_plan(mine, 0), run);
