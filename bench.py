@@ -661,6 +661,58 @@ def run_gather(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def per_block_calls(lc, x, threads: int, nblocks: int = 200):
+    """The reference drivers' calling pattern: one call per 4096-value u64 LeCo
+    block.  Times the C ABI's per-block calls (leco_block_encode / _decode /
+    _random: host buffers, one launch and a synchronize each) against the
+    compiled reference's encodeArray8_int / decodeArray8 / randomdecodeArray8 on
+    one host thread, on the same blocks (microseconds per call)."""
+    import ctypes
+
+    R = reference_lib()
+    L = lc.lib()
+    xh = x[: nblocks * BS].cpu().numpy().view(np.uint64)
+    blocks = [np.ascontiguousarray(xh[i * BS:(i + 1) * BS]) for i in range(nblocks)]
+    buf = np.zeros(BS * 8 * 2 + 256, np.uint8)
+    out = np.zeros(BS, np.uint64)
+    v = np.zeros(1, np.uint64)
+    P = ctypes.c_void_p
+    imgs = []
+    t0 = time.perf_counter()
+    for b in blocks:
+        nb = L.leco_block_encode(0, 8, P(b.ctypes.data), BS, lc.FIT_REFERENCE, P(buf.ctypes.data))
+        imgs.append(buf[:nb].tobytes())
+    t_enc = (time.perf_counter() - t0) / nblocks
+    t0 = time.perf_counter()
+    for img in imgs:
+        a = np.frombuffer(img, np.uint8)
+        lc._check(L.leco_block_decode(0, 8, P(a.ctypes.data), len(img), BS, P(out.ctypes.data)))
+    t_dec = (time.perf_counter() - t0) / nblocks
+    assert np.array_equal(out, blocks[-1])
+    t0 = time.perf_counter()
+    for i, img in enumerate(imgs):
+        a = np.frombuffer(img, np.uint8)
+        lc._check(L.leco_block_random(0, 8, P(a.ctypes.data), len(img), BS, (i * 997) % BS, P(v.ctypes.data)))
+    t_ra = (time.perf_counter() - t0) / nblocks
+    res = {"blocks": nblocks, "gpu_encode_us": round(t_enc * 1e6, 1), "gpu_decode_us": round(t_dec * 1e6, 1),
+           "gpu_random_us": round(t_ra * 1e6, 1)}
+    if R is not None:
+        t0 = time.perf_counter()
+        rimgs = [R.encode_block(0, b) for b in blocks]
+        res["reference_encode_us"] = round((time.perf_counter() - t0) / nblocks * 1e6, 1)
+        assert rimgs == imgs, "per-block images differ from the reference's"
+        t0 = time.perf_counter()
+        for img in rimgs:
+            R.decode_block(0, img, BS, 8)
+        res["reference_decode_us"] = round((time.perf_counter() - t0) / nblocks * 1e6, 1)
+        t0 = time.perf_counter()
+        for i, img in enumerate(rimgs):
+            R.random_block(0, img, (i * 997) % BS, 8)
+        res["reference_random_us"] = round((time.perf_counter() - t0) / nblocks * 1e6, 1)
+        res["reference_threads"] = 1
+    return res
+
+
 def run_codecs(args, world, rank, local):
     """Each fixed-block codec (LeCo linear, FOR, Delta, degree-2) on the decode
     workload's column (200M u64 keys, 4096-value blocks) and on its low 32 bits
@@ -715,6 +767,7 @@ def run_codecs(args, world, rank, local):
                 res[f"{name}_u{8 * s}"] = r
                 del col
     lc.check()
+    res["per_block_calls"] = per_block_calls(lc, x64, threads=host_threads())
     if rank == 0:
         head = res["delta_u64"]
         line = {"metric": f"fixed-block codecs on {n // 1_000_000}M keys: decode GB/s, random access, sum, encode",

@@ -94,11 +94,11 @@ __device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *
   }
 }
 
-// Scratch of the Delta scan: 10 words for each of up to four groups of a CTA.  One
-// non-template function, so every kernel holds a single copy however many decoder
-// instances it contains.
+// Scratch of the Delta scan: two halves of 8 warp totals for each of up to four
+// groups of a CTA.  One non-template function, so every kernel holds a single copy
+// however many decoder instances it contains.
 __device__ __forceinline__ uint64_t *delta_scan_scratch() {
-  __shared__ uint64_t s[4 * 10];
+  __shared__ uint64_t s[4 * 16];
   return s;
 }
 
@@ -162,7 +162,7 @@ __device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words
                                               uint32_t lo, uint32_t hi, Emit emit) {
   using A = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;  // arithmetic mod 2^(8S)
   constexpr int DS = kDeltaSpan;
-  uint64_t *wtot = delta_scan_scratch() + (GroupOf<G>::sub ? 10 * group_index<G>() : 0);
+  uint64_t *wtot = delta_scan_scratch() + (GroupOf<G>::sub ? 16 * group_index<G>() : 0);
   const uint32_t tid = group_rank<G>();
   const int lane = tid & 31, warp = tid >> 5;
   const uint32_t GS = group_size<G>(), NW = GS / 32;  // NW <= 8: whole-CTA groups here have <= 256 threads
@@ -189,22 +189,20 @@ __device__ __forceinline__ void delta_tiles_w(const uint64_t *__restrict__ words
       before += incl - tot;
       tile_sum = __shfl_sync(0xffffffffu, incl, 31);
     } else {
-      if (lane == 31) wtot[warp] = incl;
+      // one barrier per tile: every warp reads all warp totals of the tile; the two
+      // halves of the scratch alternate, so a warp writes a half again only after the
+      // next tile's barrier, which every warp passes after its reads of this one
+      uint64_t *wt = wtot + 8 * (tl & 1);
+      if (lane == 31) wt[warp] = incl;
       group_sync<G>();
-      if (warp == 0) {
-        A x = lane < (int)NW ? (A)wtot[lane] : (A)0, xi = x;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const A y = __shfl_up_sync(0xffffffffu, xi, o);
-          if (lane >= o) xi += y;
-        }
-        if (lane < (int)NW) wtot[lane] = xi - x;
-        if (lane == (int)NW - 1) wtot[NW] = xi;
+      A bw = 0;
+      tile_sum = 0;
+      for (uint32_t w = 0; w < NW; ++w) {
+        const A t = (A)wt[w];
+        tile_sum += t;
+        if (w < (uint32_t)warp) bw += t;
       }
-      group_sync<G>();
-      before += (A)wtot[warp] + (incl - tot);
-      tile_sum = (A)wtot[NW];
-      group_sync<G>();  // wtot is rewritten by the next tile
+      before += bw + (incl - tot);
     }
     if (k0 + DS > lo && k0 < hi) {
 #pragma unroll

@@ -102,6 +102,7 @@ struct BlockPlan {
   BlockHdr h;
   uint64_t vbase;
   uint32_t len, lo, hi;
+  uint32_t ra;    // single window, kEval: every index in [ra, hi) matches without reading (ra == hi: none)
   int pred;
   int mode;       // single window: kNone / kAll / kEval
   bool raw;
@@ -189,7 +190,7 @@ __device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t 
   p.raw = p.h.l == TB;
   p.pred = kPredAbove;
   p.mode = kEval;
-  p.lo = p.hi = 0;
+  p.lo = p.hi = p.ra = 0;
   p.f1 = a.f1 & TM;
   p.f2 = a.f2 & TM;
   p.bounded = CODEC == kLinear && !p.raw && p.h.l <= 61 && pred_in_range<kLinear>(p.h, p.len + 1);
@@ -200,7 +201,7 @@ __device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t 
     return p;
   }
   if (!close) {
-    p.hi = p.len;
+    p.hi = p.ra = p.len;
     if (a.zone && __ldg(a.zone + b) <= p.f1) {  // the experiment's zone-map skip (:247-249)
       p.mode = kNone;
     } else if (!p.raw && CODEC == kFor) {
@@ -221,13 +222,20 @@ __device__ __forceinline__ BlockPlan plan_block(const FilterLaunch &a, uint64_t 
           int64_t vmin, vmax;
           leco_value_bounds(p.h, p.lo, p.hi - 1, vmin, vmax);
           p.mode = classify<S>(vmin, vmax, p.f1, 0, false);
+          if (p.mode == kEval && p.h.a1 > 0) {
+            // predictions increase with k, so "every value at k is above the filter" turns
+            // true at one index and stays true: only the indices before it are read
+            const int64_t m = p.h.l ? (((int64_t)1 << (p.h.l - 1)) - 1) : 0;
+            p.ra = first_change(p.lo, p.hi, false, [&](uint32_t k) { return surely_above<S>(p.h, m, k, p.f1); });
+          }
         }
       }
     }
     if (p.mode == kNone) p.hi = p.lo;
+    if (p.mode != kEval || p.ra < p.lo || p.ra > p.hi) p.ra = p.hi;  // a split only for read blocks
     return p;
   }
-  p.hi = p.len;
+  p.hi = p.ra = p.len;
   if (CODEC == kFor) {
     p.pred = kPredModulo;
     return p;
@@ -378,6 +386,7 @@ __device__ __forceinline__ BlockPlan shfl_plan(const BlockPlan &q, int src) {
   p.len = __shfl_sync(0xffffffffu, q.len, src);
   p.lo = __shfl_sync(0xffffffffu, q.lo, src);
   p.hi = __shfl_sync(0xffffffffu, q.hi, src);
+  p.ra = __shfl_sync(0xffffffffu, q.ra, src);
   p.pred = __shfl_sync(0xffffffffu, q.pred, src);
   p.mode = __shfl_sync(0xffffffffu, q.mode, src);
   p.raw = __shfl_sync(0xffffffffu, (int)q.raw, src) != 0;
@@ -391,18 +400,19 @@ __device__ __forceinline__ BlockPlan shfl_plan(const BlockPlan &q, int src) {
 // all fields of a step in flight.  Counts; with WRITE also stores the matches
 // from out position `run` on (positions at or past cap are dropped).
 template <int S, int CODEC, bool WRITE>
-__device__ __forceinline__ uint64_t eval_block(const FilterLaunch &a, const BlockPlan &p, uint64_t run) {
+__device__ __forceinline__ uint64_t eval_block(const FilterLaunch &a, const BlockPlan &p, uint32_t k0, uint32_t k1,
+                                               uint64_t run) {
   const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
   const uint64_t step = a.base & (S == 8 ? ~0ull : 0xffffffffull);
   uint64_t cnt = 0;
-  for (uint32_t s0 = p.lo; s0 < p.hi; s0 += 32 * kFU) {
+  for (uint32_t s0 = k0; s0 < k1; s0 += 32 * kFU) {
     uint32_t m[kFU];
 #pragma unroll
     for (int u = 0; u < kFU; ++u) {
       const uint32_t k = s0 + u * 32 + lane;
       bool fl = false;
-      if (k < p.hi) fl = single_pred<S>(p.pred, filter_value<S, CODEC>(words, p.h, p.raw, k), p.f1, p.f2, step);
+      if (k < k1) fl = single_pred<S>(p.pred, filter_value<S, CODEC>(words, p.h, p.raw, k), p.f1, p.f2, step);
       m[u] = __ballot_sync(0xffffffffu, fl);
     }
 #pragma unroll
@@ -423,7 +433,7 @@ __device__ __forceinline__ uint64_t count_block(const FilterLaunch &a, const Blo
   if (p.pred == kPredWindows) return window_loop<S, CODEC, false>(a, p, 0);
   if (p.mode == kAll) return p.hi - p.lo;
   if (p.mode != kEval) return 0;
-  return eval_block<S, CODEC, false>(a, p, 0);
+  return eval_block<S, CODEC, false>(a, p, p.lo, p.ra, 0) + (p.hi - p.ra);
 }
 
 // Writes the matches of one block from output position `run` on (warp-uniform).
@@ -437,7 +447,10 @@ __device__ __forceinline__ void write_block(const FilterLaunch &a, const BlockPl
     write_run(a, run, (uint32_t)(p.vbase + p.lo), p.hi - p.lo);
     return;
   }
-  if (p.mode == kEval) eval_block<S, CODEC, true>(a, p, run);
+  if (p.mode == kEval) {
+    run += eval_block<S, CODEC, true>(a, p, p.lo, p.ra, run);
+    if (p.ra < p.hi) write_run(a, run, (uint32_t)(p.vbase + p.ra), p.hi - p.ra);
+  }
 }
 
 // counts[b]: the block's match count in the low 40 bits; a block whose matches are
@@ -481,7 +494,8 @@ __global__ void __launch_bounds__(kFT) filter_count_kernel(FilterLaunch a, int c
 
 // ---- pass 2: exclusive scan of the group totals (one CTA of 1024 threads) ----------
 // group_tot[g] becomes the output position of group g's first match; *count the
-// total number of matches.
+// total number of matches.  (A decoupled look-back over the groups inside pass 1
+// was measured slower: its chain of waits took longer than this launch.)
 __global__ void __launch_bounds__(1024) filter_scan_kernel(uint64_t *group_tot, uint64_t ngroups, uint64_t *count) {
   __shared__ uint64_t wsum[33];
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
