@@ -379,7 +379,10 @@ int leco_gather_host(int codec, int dtype, const uint8_t *h_payload, const uint6
                      uint32_t block_size, const uint64_t *h_idx, uint64_t m, void *h_out);
 
 /* ---- per-block drop-in (one reference block, host buffers) ------------
- * Byte-for-byte the reference methods' contracts; used by include/leco_codecs.hpp. */
+ * Byte-for-byte the reference methods' contracts; used by include/leco_codecs.hpp.
+ * Synchronous.  Each calling thread keeps one stream, a device buffer and a pinned
+ * host buffer (both grow to the largest block seen) for these calls, from its first
+ * per-block call on a device until leco_thread_release() or the end of the process. */
 
 /* <Codec>::encodeArray8_int(data, length, res, nvalue): returns bytes written
  * to h_out (which must hold leco_block_bytes(..., 8*dtype, length)), or a
@@ -390,6 +393,10 @@ int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_byt
 /* <Codec>::randomdecodeArray8(in, to_find, NULL, 0) into *h_value. */
 int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
                       uint32_t to_find, void *h_value);
+/* Frees the calling thread's per-block stream and buffers (no counterpart in the
+ * reference, whose per-block calls need no resources).  Call it before a thread
+ * that made per-block calls exits, if the process goes on. */
+int leco_thread_release(void);
 
 /* Leco_int<T> / FOR_int<T>::filter_range(in, length, filter, out, block_id)
  * (close = 0; piecewise_fix_integer_template.h:206-252, FOR_integer_template.h:115-160) or

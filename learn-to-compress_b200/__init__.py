@@ -79,6 +79,7 @@ SIGNATURES = [
     ("leco_block_encode", ctypes.c_int64, [_I, _I, _P, _U32, _I, _P]),
     ("leco_block_decode", _I, [_I, _I, _P, _U64, _U32, _P]),
     ("leco_block_random", _I, [_I, _I, _P, _U64, _U32, _U32, _P]),
+    ("leco_thread_release", _I, []),
     ("leco_validate_host", _I, [_I, _I, _P, _U64, _P, _U64, _U32, _P]),
     ("leco_container_write", _I, [ctypes.c_char_p, _P, _P, _P, _P]),
     ("leco_container_info_read", _I, [ctypes.c_char_p, _P]),

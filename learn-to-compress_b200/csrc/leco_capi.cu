@@ -547,24 +547,140 @@ int leco_gather_host(int codec, int dtype, const uint8_t *h_payload, const uint6
 }
 
 // ---- per-block drop-in -----------------------------------------------------------------
+// The reference's drivers call the codec once per block.  Each calling thread keeps one
+// stream, one device buffer and one pinned host buffer (both only grow) for these calls,
+// created on its first per-block call on a device and kept until leco_thread_release()
+// or the process ends, so a call costs its copies, one launch and one synchronize.
+
+namespace {
+
+struct BlockCtx {
+  int device = -1;
+  cudaStream_t st = nullptr;
+  uint8_t *d = nullptr;  // device buffer
+  uint64_t dcap = 0;
+  uint8_t *h = nullptr;  // pinned host staging
+  uint64_t hcap = 0;
+};
+thread_local BlockCtx t_block;
+
+void block_ctx_free(BlockCtx &c) {
+  if (c.st) cudaStreamSynchronize(c.st);
+  if (c.d) cudaFree(c.d);
+  if (c.h) cudaFreeHost(c.h);
+  if (c.st) cudaStreamDestroy(c.st);
+  c = BlockCtx{};
+}
+
+uint64_t round256(uint64_t x) { return (x + 255) & ~255ull; }
+
+// The calling thread's context on the current device, with at least dev_bytes of device
+// and host_bytes of pinned host memory.
+int block_ctx(uint64_t dev_bytes, uint64_t host_bytes, BlockCtx *&out) {
+  int dev = 0;
+  LECO_CUDA(cudaGetDevice(&dev));
+  BlockCtx &c = t_block;
+  if (c.device != dev) {
+    if (c.device >= 0) {  // the thread moved to another device: free on the old one
+      LECO_CUDA(cudaSetDevice(c.device));
+      block_ctx_free(c);
+      LECO_CUDA(cudaSetDevice(dev));
+    }
+    LECO_CUDA(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+    c.device = dev;
+  }
+  if (c.dcap < dev_bytes) {
+    if (c.d) LECO_CUDA(cudaFree(c.d));
+    c.d = nullptr;
+    c.dcap = 0;
+    const uint64_t cap = std::max<uint64_t>(dev_bytes, 1ull << 20);
+    if (cudaMalloc(&c.d, cap) != cudaSuccess) return fail(LECO_ERR_NOMEM, "per-block call: device allocation failed");
+    c.dcap = cap;
+  }
+  if (c.hcap < host_bytes) {
+    if (c.h) LECO_CUDA(cudaFreeHost(c.h));
+    c.h = nullptr;
+    c.hcap = 0;
+    const uint64_t cap = std::max<uint64_t>(host_bytes, 1ull << 20);
+    if (cudaHostAlloc(&c.h, cap, cudaHostAllocDefault) != cudaSuccess)
+      return fail(LECO_ERR_NOMEM, "per-block call: pinned host allocation failed");
+    c.hcap = cap;
+  }
+  out = &c;
+  return LECO_OK;
+}
+
+// Copies a block image to the start of the context's device buffer with LECO_PAYLOAD_SLACK
+// zero bytes after it, then offsets {0, in_bytes} and `extra` (nextra words) at
+// round256(in_bytes + slack): one pinned staging copy, one upload.
+void stage_block(BlockCtx &c, const uint8_t *h_in, uint64_t in_bytes, const uint64_t *extra = nullptr, int nextra = 0) {
+  const uint64_t pb = round256(in_bytes + LECO_PAYLOAD_SLACK);
+  memcpy(c.h, h_in, in_bytes);
+  memset(c.h + in_bytes, 0, pb - in_bytes);
+  uint64_t *tail = reinterpret_cast<uint64_t *>(c.h + pb);
+  tail[0] = 0;
+  tail[1] = in_bytes;
+  for (int i = 0; i < nextra; ++i) tail[2 + i] = extra[i];
+  cudaMemcpyAsync(c.d, c.h, pb + 8 * (2 + nextra), cudaMemcpyHostToDevice, c.st);
+}
+
+}  // namespace
+
+int leco_thread_release(void) {
+  if (t_block.device < 0) return LECO_OK;
+  int dev = 0;
+  LECO_CUDA(cudaGetDevice(&dev));
+  LECO_CUDA(cudaSetDevice(t_block.device));
+  block_ctx_free(t_block);
+  LECO_CUDA(cudaSetDevice(dev));
+  return LECO_OK;
+}
 
 int64_t leco_block_encode(int codec, int dtype, const void *h_values, uint32_t length, int fit_mode, uint8_t *h_out) {
+  if (!h_values || !h_out) return fail(LECO_ERR_ARG, "leco_block_encode: null pointer");
   if (!length || length > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, "leco_block_encode: length must be in 1..16384");
+  if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, "leco_block_encode: dtype must be LECO_U32 or LECO_U64");
+  const uint64_t vb = round256((uint64_t)length * dtype);
   const uint64_t cap = leco_max_payload_bytes(codec, dtype, length, length);
-  std::vector<uint8_t> tmp(cap);
-  uint64_t off[2], bytes = 0;
-  int rc = leco_encode_host(codec, dtype, h_values, length, length, fit_mode, tmp.data(), cap, off, &bytes);
+  const uint64_t wsb = leco_encode_workspace_bytes(codec, dtype, length, length, fit_mode);
+  BlockCtx *c = nullptr;
+  int rc = block_ctx(vb + 256 + round256(cap) + round256(wsb), vb + 256 + round256(cap), c);
   if (rc) return rc;
-  memcpy(h_out, tmp.data(), bytes);
+  uint8_t *dv = c->d, *doff = c->d + vb, *dp = doff + 256, *dws = dp + round256(cap);
+  memcpy(c->h, h_values, (uint64_t)length * dtype);
+  cudaMemcpyAsync(dv, c->h, (uint64_t)length * dtype, cudaMemcpyHostToDevice, c->st);
+  const leco_stream_t ls = reinterpret_cast<leco_stream_t>(c->st);
+  rc = leco_encode(codec, dtype, dv, length, length, fit_mode, dp, cap, reinterpret_cast<uint64_t *>(doff), nullptr, dws,
+                   wsb, ls);
+  if (rc) return rc;
+  // offsets and the image come back in one copy: [offsets (256)][image (cap)]
+  cudaMemcpyAsync(c->h, doff, 256 + cap, cudaMemcpyDeviceToHost, c->st);
+  if ((rc = leco_check(ls)) != LECO_OK) return rc;  // synchronizes the stream
+  uint64_t off[2];
+  memcpy(off, c->h, 16);
+  const uint64_t bytes = off[1];
+  if (bytes > cap) return fail(LECO_ERR_CORRUPT, "leco_block_encode: image larger than its bound");
+  memcpy(h_out, c->h + 256, bytes);
   return (int64_t)bytes;
 }
 
 int leco_block_decode(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length, void *h_out) {
   if (!h_in || !h_out || !length) return fail(LECO_ERR_ARG, "leco_block_decode: bad argument");
-  std::vector<uint8_t> tmp(in_bytes + LECO_PAYLOAD_SLACK, 0);
-  memcpy(tmp.data(), h_in, in_bytes);
-  uint64_t off[2] = {0, in_bytes};
-  return leco_decode_host(codec, dtype, tmp.data(), off, length, length, h_out);
+  if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, "leco_block_decode: dtype must be LECO_U32 or LECO_U64");
+  const uint64_t pb = round256(in_bytes + LECO_PAYLOAD_SLACK), ob = (uint64_t)length * dtype;
+  BlockCtx *c = nullptr;
+  int rc = block_ctx(pb + 256 + ob, std::max(pb + 256, ob), c);
+  if (rc) return rc;
+  uint8_t *dp = c->d, *dout = c->d + pb + 256;
+  uint64_t *doff = reinterpret_cast<uint64_t *>(c->d + pb);
+  stage_block(*c, h_in, in_bytes);
+  const leco_stream_t ls = reinterpret_cast<leco_stream_t>(c->st);
+  rc = leco_decode(codec, dtype, dp, doff, length, length, dout, ls);
+  if (rc) return rc;
+  cudaMemcpyAsync(c->h, dout, ob, cudaMemcpyDeviceToHost, c->st);
+  if ((rc = leco_check(ls)) != LECO_OK) return rc;  // synchronizes the stream
+  memcpy(h_out, c->h, ob);
+  return LECO_OK;
 }
 
 int64_t leco_block_filter(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
@@ -620,11 +736,23 @@ int64_t leco_block_filter(int codec, int dtype, const uint8_t *h_in, uint64_t in
 int leco_block_random(int codec, int dtype, const uint8_t *h_in, uint64_t in_bytes, uint32_t length,
                       uint32_t to_find, void *h_value) {
   if (!h_in || !h_value || to_find >= length) return fail(LECO_ERR_ARG, "leco_block_random: bad argument");
-  std::vector<uint8_t> tmp(in_bytes + LECO_PAYLOAD_SLACK, 0);
-  memcpy(tmp.data(), h_in, in_bytes);
-  uint64_t off[2] = {0, in_bytes};
-  uint64_t idx = to_find;
-  return leco_gather_host(codec, dtype, tmp.data(), off, length, length, &idx, 1, h_value);
+  if (!dtype_ok(dtype)) return fail(LECO_ERR_ARG, "leco_block_random: dtype must be LECO_U32 or LECO_U64");
+  const uint64_t pb = round256(in_bytes + LECO_PAYLOAD_SLACK);
+  BlockCtx *c = nullptr;
+  int rc = block_ctx(pb + 512, pb + 256, c);
+  if (rc) return rc;
+  uint8_t *dp = c->d;
+  uint64_t *doff = reinterpret_cast<uint64_t *>(c->d + pb);
+  uint64_t *didx = doff + 2, *dout = doff + 4;
+  const uint64_t idx = to_find;
+  stage_block(*c, h_in, in_bytes, &idx, 1);  // the index lands at didx
+  const leco_stream_t ls = reinterpret_cast<leco_stream_t>(c->st);
+  rc = leco_gather(codec, dtype, dp, doff, nullptr, length, length, didx, 1, dout, ls);
+  if (rc) return rc;
+  cudaMemcpyAsync(c->h, dout, 8, cudaMemcpyDeviceToHost, c->st);
+  if ((rc = leco_check(ls)) != LECO_OK) return rc;  // synchronizes the stream
+  memcpy(h_value, c->h, (uint64_t)dtype);
+  return LECO_OK;
 }
 
 }  // extern "C"
