@@ -56,9 +56,7 @@ __device__ __forceinline__ BlockHdr parse_header(const uint8_t *__restrict__ pay
 }
 
 template <int CODEC, int S>
-__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b) {
-  const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
-  const ulonglong2 q0 = __ldg(p), q1 = __ldg(p + 1);
+__device__ __forceinline__ BlockHdr dir_entry_fields(ulonglong2 q0, ulonglong2 q1) {
   BlockHdr h;
   h.body_bit = q0.x & ((1ull << 48) - 1);
   h.l = (uint32_t)(q0.x >> 56);
@@ -67,6 +65,17 @@ __device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ 
   h.a2 = __longlong_as_double((long long)q1.y);
   h.base = S == 8 ? q0.y : (q0.y & 0xffffffffull);
   return h;
+}
+template <int CODEC, int S>
+__device__ __forceinline__ BlockHdr from_dir(const leco_dir_entry *__restrict__ dir, uint64_t b) {
+  const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
+  return dir_entry_fields<CODEC, S>(__ldg(p), __ldg(p + 1));
+}
+// The same with an L2 eviction policy on the entry's two loads.
+template <int CODEC, int S>
+__device__ __forceinline__ BlockHdr from_dir_hint(const leco_dir_entry *__restrict__ dir, uint64_t b, uint64_t pol) {
+  const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(dir + b);
+  return dir_entry_fields<CODEC, S>(ld_nc_hint_v2(p, pol), ld_nc_hint_v2(p + 1, pol));
 }
 
 // Value k of a non-raw, non-Delta block given its field f (bulk decode rules).
@@ -432,6 +441,7 @@ __device__ __forceinline__ void gather_lookups(const GatherLaunch &a, uint64_t f
   const uint64_t *words = reinterpret_cast<const uint64_t *>(a.payload);
   T *out = reinterpret_cast<T *>(a.out);
   const bool small = a.n <= 0xffffffffull;
+  const uint64_t stream_pol = l2_evict_first_policy(), dir_pol = l2_evict_last_policy();
   for (uint64_t i0 = first_i; i0 < a.m; i0 += G * U) {
     uint64_t g[U], b[U];
     uint32_t k[U];
@@ -440,7 +450,7 @@ __device__ __forceinline__ void gather_lookups(const GatherLaunch &a, uint64_t f
     for (int u = 0; u < U; ++u) {
       const uint64_t i = i0 + (uint64_t)u * G;
       live[u] = i < a.m;
-      g[u] = live[u] ? __ldg(a.idx + i) : 0;
+      g[u] = live[u] ? ld_nc_hint(a.idx + i, stream_pol) : 0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -463,7 +473,8 @@ __device__ __forceinline__ void gather_lookups(const GatherLaunch &a, uint64_t f
     BlockHdr h[U];
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      h[u] = a.dir ? from_dir<CODEC, S>(a.dir, b[u]) : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b[u]));
+      h[u] = a.dir ? from_dir_hint<CODEC, S>(a.dir, b[u], dir_pol)
+                   : parse_header<CODEC, S>(a.payload, __ldg(a.offsets + b[u]));
     uint64_t lo[U], hi[U];
     uint32_t sh[U], l[U];
 #pragma unroll
@@ -480,7 +491,7 @@ __device__ __forceinline__ void gather_lookups(const GatherLaunch &a, uint64_t f
     for (int u = 0; u < U; ++u) {
       if (!live[u]) continue;
       const uint64_t f = funnel64(lo[u], hi[u], sh[u]) & lowmask(l[u]);
-      out[i0 + (uint64_t)u * G] = (T)ra_value<CODEC, S>(h[u], k[u], f, a.error);
+      st_hint<T>(out + i0 + (uint64_t)u * G, (T)ra_value<CODEC, S>(h[u], k[u], f, a.error), stream_pol);
     }
   }
 }

@@ -401,6 +401,39 @@ __device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// ---- L2 eviction priorities for random access ---------------------------------
+// A batch of lookups streams its indices in and its results out once, while every
+// lookup also reads its block's 32-byte directory entry (a small, hot table).  The
+// streams are marked evict-first and the directory evict-last, so the streams do not
+// push the directory out of L2 and each lookup pays DRAM only for its payload sector.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t ld_nc_hint(const uint64_t *p, uint64_t pol) {
+  uint64_t v;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ ulonglong2 ld_nc_hint_v2(const void *p, uint64_t pol) {
+  ulonglong2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ void st_hint(T *p, T v, uint64_t pol) {
+  if constexpr (sizeof(T) == 8)
+    asm volatile("st.global.L2::cache_hint.b64 [%0], %1, %2;" ::"l"(p), "l"((uint64_t)v), "l"(pol) : "memory");
+  else
+    asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"((uint32_t)v), "l"(pol) : "memory");
+}
+
 }  // namespace leco
 
 namespace leco {

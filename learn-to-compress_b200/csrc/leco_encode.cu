@@ -22,8 +22,9 @@
 
 namespace leco {
 
+// u64 LeCo blocks are held to 40 registers, six CTAs per SM (their shared memory allows six).
 template <typename T, int CODEC>
-__global__ void __launch_bounds__(256) encode_kernel(EncodeArgs a) {
+__global__ void __launch_bounds__(256, (CODEC == kLinear && sizeof(T) == 8) ? 6 : 1) encode_kernel(EncodeArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   __shared__ uint64_t ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1u);

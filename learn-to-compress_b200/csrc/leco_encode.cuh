@@ -274,6 +274,155 @@ __device__ __forceinline__ void with_pred_rule(double m0, double m1, uint32_t le
   else fn(std::integral_constant<int, 2>{});
 }
 
+// ---- u64 LeCo blocks, 32-bit path: values staged whole, rows packed in place ---------
+// The block's values are copied into shared memory as 16-byte pairs (values 2q, 2q+1)
+// with cp.async, every copy of a thread in flight at once.  Rows of 32 values are 256
+// bytes; pair j of row t sits in 16-byte slot j ^ (t mod 16) of the row, so that a warp
+// over 32 consecutive pairs (two rows) and a warp over 32 rows (the same pair of each)
+// both spread over the banks.  The residual pass writes the pair's two signed 32-bit
+// residuals over the first 8 bytes of its slot; the packer then turns row t, which
+// only its own thread reads, into L words written from word t mod 32 of the row on.
+__device__ __forceinline__ uint32_t pair16_slot(uint32_t q) { return q ^ ((q >> 4) & 15u); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint4 lds_v4(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint2 lds_v2(uint32_t a) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts_v2(uint32_t a, uint32_t x, uint32_t y) {
+  asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(a), "r"(x), "r"(y));
+}
+__device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v) { asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v)); }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Max, min and bitwise or of int32 values over the encoding warps (warps 1.. of the
+// group; warp 0 runs the look-back).  `slots`: 96 ints of shared memory that no thread
+// still reads (the two reductions of one block use different slots).
+template <int G>
+__device__ __forceinline__ void enc_reduce3(int32_t &mx, int32_t &mn, uint32_t &ov, int32_t *slots) {
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  mn = __reduce_min_sync(0xffffffffu, mn);
+  ov = __reduce_or_sync(0xffffffffu, ov);
+  const uint32_t nw = group_size<G>() / 32 - 1;
+  if (nw == 1) {
+    __syncwarp();  // orders the warp's shared-memory writes before the next phase
+    return;
+  }
+  const uint32_t w = (group_rank<G>() >> 5) - 1;
+  if ((threadIdx.x & 31) == 0) {
+    slots[w] = mx;
+    slots[32 + w] = mn;
+    slots[64 + w] = (int32_t)ov;
+  }
+  group_sub_sync<G>();
+  for (uint32_t k = 0; k < nw; ++k) {
+    mx = max(mx, slots[k]);
+    mn = min(mn, slots[32 + k]);
+    ov |= (uint32_t)slots[64 + k];
+  }
+}
+
+// Field of signed residual r (|r| < 2^(L-1)): the magnitude with the sign bit
+// (r > 0, "data[i] > pred") at bit L-1 (write_delta_int_T, bit_write.h:257-323).
+template <int L>
+__device__ __forceinline__ uint32_t lin_field(uint32_t r) {
+  return (int32_t)r > 0 ? (r | (1u << (L - 1))) : (uint32_t)(-(int32_t)r);
+}
+// Adds field f of row position j (bits [j*L, j*L + L) of the row's bit stream) to the
+// row's words; fields are disjoint and come in increasing j, so adding is or-ing.
+template <int L>
+__device__ __forceinline__ void place_field(uint32_t (&w)[L], uint32_t f, int j) {
+  const int p = j * L, q = p >> 5, s = p & 31;
+  w[q] += f << s;
+  if (s + L > 32) w[q + 1] += f >> (32 - s);
+}
+// Packs rows t0, t0 + step, ... < rows (32 signed residuals each, zeros past the
+// block's end) into L words, written over row t from word t mod 32 on (bank t + k for
+// word k).  Every shift is a compile-time constant.
+template <int L>
+__device__ __forceinline__ void pack_rows_width(uint32_t vb, uint32_t rows, uint32_t t0, uint32_t step) {
+  for (uint32_t t = t0; t < rows; t += step) {
+    const uint32_t x = t & 15u, row = vb + t * 256u;
+    uint32_t w[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) w[k] = 0;
+#pragma unroll
+    for (int jj = 0; jj < 16; ++jj) {
+      const uint2 v = lds_v2(row + (((uint32_t)jj ^ x) << 4));
+      place_field<L>(w, lin_field<L>(v.x), 2 * jj);
+      place_field<L>(w, lin_field<L>(v.y), 2 * jj + 1);
+    }
+    const uint32_t o = row + (t & 31u) * 4u;
+#pragma unroll
+    for (int k = 0; k < L; ++k) sts_u32(o + 4u * k, w[k]);
+  }
+}
+// One call per block and thread: the width is uniform over the block.
+static __device__ __noinline__ void pack_rows_dispatch(uint32_t l, uint32_t vb, uint32_t rows, uint32_t t0, uint32_t step) {
+  switch (l) {
+#define LECO_PACK_CASE(L) \
+  case L: pack_rows_width<L>(vb, rows, t0, step); break;
+    LECO_PACK_CASE(1) LECO_PACK_CASE(2) LECO_PACK_CASE(3) LECO_PACK_CASE(4) LECO_PACK_CASE(5) LECO_PACK_CASE(6)
+    LECO_PACK_CASE(7) LECO_PACK_CASE(8) LECO_PACK_CASE(9) LECO_PACK_CASE(10) LECO_PACK_CASE(11) LECO_PACK_CASE(12)
+    LECO_PACK_CASE(13) LECO_PACK_CASE(14) LECO_PACK_CASE(15) LECO_PACK_CASE(16) LECO_PACK_CASE(17)
+    LECO_PACK_CASE(18) LECO_PACK_CASE(19) LECO_PACK_CASE(20) LECO_PACK_CASE(21) LECO_PACK_CASE(22)
+    LECO_PACK_CASE(23) LECO_PACK_CASE(24) LECO_PACK_CASE(25) LECO_PACK_CASE(26) LECO_PACK_CASE(27)
+    LECO_PACK_CASE(28) LECO_PACK_CASE(29) LECO_PACK_CASE(30) LECO_PACK_CASE(31) LECO_PACK_CASE(32)
+#undef LECO_PACK_CASE
+    default: break;
+  }
+}
+
+// write_image_packed for rows packed by pack_rows_dispatch: body word k is word
+// k mod L of row t = k / L, at v32[t*64 + t mod 32 + k mod L]; words past the last
+// row read as zero (the image's zero tail).  k / L is a multiply-high by
+// ceil(2^32 / L), exact for k < 2^16 (a block body has at most 16384 words).
+__device__ __forceinline__ void write_image_rows(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
+                                                 const uint8_t *hdr, const uint32_t *v32, uint32_t L, uint32_t rows,
+                                                 uint32_t rank, uint32_t nthreads) {
+  const uint32_t M = L > 1 ? 0xffffffffu / L + 1u : 0u, nw = rows * L;
+  auto word = [&](uint32_t k) -> uint32_t {
+    const uint32_t t = L > 1 ? __umulhi(k, M) : k;
+    return k < nw ? v32[t * 64u + (t & 31u) + (k - t * L)] : 0u;
+  };
+  const uint64_t gend = goff + size;
+  const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
+  const uint64_t body0 = goff + H;
+  for (uint64_t c = c0 + rank; c < c1; c += nthreads) {
+    const uint64_t cb = c << 4;
+    if (cb >= body0 && cb + 16 <= gend) {
+      const uint32_t q = (uint32_t)(cb - body0), qw = q >> 2, sh = (q & 3u) * 8u;
+      const uint32_t w0 = word(qw), w1 = word(qw + 1), w2 = word(qw + 2), w3 = word(qw + 3), w4 = word(qw + 4);
+      *reinterpret_cast<uint4 *>(payload + cb) = make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                                                            __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
+    } else {
+      for (int j = 0; j < 16; ++j) {
+        const uint64_t g = cb + j;
+        if (g < goff || g >= gend) continue;
+        const uint64_t i = g - goff;
+        if (i < H) {
+          payload[g] = hdr[i];
+        } else {
+          const uint32_t bi = (uint32_t)(i - H);
+          payload[g] = (uint8_t)(word(bi >> 2) >> ((bi & 3u) * 8u));
+        }
+      }
+    }
+  }
+}
+
 // Leco_int<uint64_t>::encodeArray8_int (piecewise_fix_integer_template.h:27-140)
 // for one block with a whole CTA, the same image as the generic encode_block:
 //  * warp 0 takes the block's exclusive byte offset by look-back from the start,
@@ -344,35 +493,86 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       dmax = (int64_t)(uint64_t)rmx;
       dmin = (int64_t)(uint64_t)rmn;
       const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
-      m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
+      m0 = __dadd_rn(m0, __dmul_rn(__ll2double_rn(mid), 0.5));  // x * 0.5 rounds exactly as x / 2.0
       return dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
     };
-    bool narrow_range;
+    // ---- 32-bit path (16-byte aligned blocks whose predictions lie in [0, 2^51)) -----
+    const uint32_t vb = smem_u32(sm.vals), np = len >> 1;
+    // The block's values into their pair slots, every copy of this thread in flight.
+    auto stage_pairs = [&]() {
+      for (uint32_t q = ct; q < np; q += cn) cp_async16(vb + 16u * pair16_slot(q), src + 2 * q);
+      if ((len & 1) && ct == 0) cp_async8(vb + 16u * pair16_slot(np), src + len - 1);
+      cp_async_wait_all();
+      group_sub_sync<G>();
+    };
+    // Midpoint pass over the staged values: every d = y - pred is taken in 64 bits but
+    // its max and min in 32 bits, with a check that each d fits in an int32 (its high
+    // word is the sign extension of its low word).  Returns false (model untouched)
+    // when some d does not fit; the 64-bit pass then runs instead.
+    int32_t *slots = reinterpret_cast<int32_t *>(sm.red);  // two sets of 96 ints
+    bool narrow_range = false;
+    auto mid_pass32 = [&]() -> bool {
+      int32_t mx = INT32_MIN, mn = INT32_MAX;
+      uint32_t bad = 0;
+      auto visit = [&](uint64_t y, uint32_t i) {
+        const double p = pred_linear_fp64(m0, m1, i);
+        // y - trunc(p): the magic-number sum holds 2^52 + trunc(p) (its bits minus 0x433 << 52)
+        const uint64_t d = y - (uint64_t)__double_as_longlong(__dadd_rz(p, 4503599627370496.0)) + 0x4330000000000000ull;
+        const uint32_t dl = (uint32_t)d;
+        bad |= (uint32_t)(d >> 32) ^ (uint32_t)((int32_t)dl >> 31);
+        mx = max(mx, (int32_t)dl);
+        mn = min(mn, (int32_t)dl);
+      };
+#pragma unroll 2
+      for (uint32_t q = ct; q < np; q += cn) {
+        const uint4 v = lds_v4(vb + 16u * pair16_slot(q));
+        visit(((uint64_t)v.y << 32) | v.x, 2 * q);
+        visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
+      }
+      if ((len & 1) && ct == 0) {
+        const uint2 v = lds_v2(vb + 16u * pair16_slot(np));
+        visit(((uint64_t)v.y << 32) | v.x, len - 1);
+      }
+      enc_reduce3<G>(mx, mn, bad, slots);
+      if (bad) return false;
+      const int64_t mid = (int64_t)mx + (int64_t)mn;
+      m0 = __dadd_rn(m0, __dmul_rn(__ll2double_rn(mid), 0.5));  // x * 0.5 rounds exactly as x / 2.0
+      narrow_range = (int64_t)mx - (int64_t)mn < (1ll << 30);
+      return true;
+    };
+    const bool al16 = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    bool pairs = false;  // the 32-bit midpoint pass ran over the staged pairs
     if (a.seq_models) {
       m0 = a.seq_models[b * 3 + 0];
       m1 = a.seq_models[b * 3 + 1];
-      narrow_range = mid_pass(true);
+      if (al16 && preds_nonneg(m0, m1, len)) {
+        stage_pairs();
+        pairs = mid_pass32();
+      }
+      if (!pairs) narrow_range = mid_pass(true);
     } else {
       // Moments in 32-bit halves of y: a thread sees at most 16384 values, each
       // i*y_lo, i*y_hi < 2^46, so the 64-bit partial sums stay below 2^60.
       uint64_t slo = 0, shi = 0, tlo = 0, thi = 0;
       auto visit = [&](uint64_t y, uint32_t i) {
-        lo[swz32(i)] = (uint32_t)y;
         const uint32_t yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
         slo += yl;
         shi += yh;
         tlo += (uint64_t)yl * i;
         thi += (uint64_t)yh * i;
       };
-      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-        const uint32_t np = len / 2;
+      if (al16) {
+        stage_pairs();
 #pragma unroll (UE)
         for (uint32_t q = ct; q < np; q += cn) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+          const uint4 v = lds_v4(vb + 16u * pair16_slot(q));
           visit(((uint64_t)v.y << 32) | v.x, 2 * q);
           visit(((uint64_t)v.w << 32) | v.z, 2 * q + 1);
         }
-        if ((len & 1) && ct == 0) visit(__ldg(src + len - 1), len - 1);
+        if ((len & 1) && ct == 0) {
+          const uint2 v = lds_v2(vb + 16u * pair16_slot(np));
+          visit(((uint64_t)v.y << 32) | v.x, len - 1);
+        }
       } else {
         for (uint32_t i = ct; i < len; i += cn) visit(__ldg(src + i), i);
       }
@@ -388,13 +588,45 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
       const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
       m1 = __ddiv_rn(ccc, xxx);
       m0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(m1, sumx)), md);
-      narrow_range = mid_pass(false);
+      pairs = al16 && preds_nonneg(m0, m1, len) && mid_pass32();
+      if (!pairs) narrow_range = mid_pass(true);  // stages the low words in the row layout of pack_rows
     }
 
     // ---- residuals (:51-72) and width (:108-117) -------------------------------------
-    const bool r32 = narrow_range && preds_nonneg(m0, m1, len);
+    const bool narrow = narrow_range && preds_nonneg(m0, m1, len);
+    const bool r32 = narrow && !pairs, r32p = narrow && pairs;
     uint32_t l;
-    if (r32) {
+    if (r32p) {
+      // Signed 32-bit residuals from the staged low words, written over the first 8
+      // bytes of each pair slot; the packer takes magnitude and sign from them.  Every
+      // slot of the last row past the block's end holds zeros.
+      int32_t rmx = 0, rmn = 0;
+#pragma unroll 2
+      for (uint32_t q = ct; q < np; q += cn) {
+        const uint32_t at = vb + 16u * pair16_slot(q);
+        const uint4 v = lds_v4(at);
+        const int32_t r0 = (int32_t)(v.x - (uint32_t)trunc_nonneg_fp64(pred_linear_fp64(m0, m1, 2 * q)));
+        const int32_t r1 = (int32_t)(v.z - (uint32_t)trunc_nonneg_fp64(pred_linear_fp64(m0, m1, 2 * q + 1)));
+        rmx = max(rmx, max(r0, r1));
+        rmn = min(rmn, min(r0, r1));
+        sts_v2(at, (uint32_t)r0, (uint32_t)r1);
+      }
+      const uint32_t qend = (len + 31u) / 32u * 16u;  // pairs of the rows
+      for (uint32_t q = np + ct; q < qend; q += cn) {
+        const uint32_t at = vb + 16u * pair16_slot(q);
+        int32_t r0 = 0;
+        if (2 * q < len) {  // the odd last value
+          r0 = (int32_t)(lds_v2(at).x - (uint32_t)trunc_nonneg_fp64(pred_linear_fp64(m0, m1, 2 * q)));
+          rmx = max(rmx, r0);
+          rmn = min(rmn, r0);
+        }
+        sts_v2(at, (uint32_t)r0, 0u);
+      }
+      uint32_t none = 0;
+      enc_reduce3<G>(rmx, rmn, none, slots + 96);
+      const uint32_t rm = max((uint32_t)rmx, (uint32_t)(-rmn));  // every |r| < 2^31
+      l = rm ? bits_of(rm) + 1 : 0;
+    } else if (r32) {
       uint32_t rm32 = 0;
       for (uint32_t i0 = 0; i0 < len; i0 += cn) {
         const uint32_t i = i0 + ct;
@@ -435,7 +667,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     if (ct == 0) {
       if (b > 0) st_relaxed(&a.status[b], kFlagAgg | size);  // successors need not wait for our prefix
       sm.bcast[2] = size;
-      sm.bcast[3] = l | ((uint64_t)r32 << 8);
+      sm.bcast[3] = l | ((uint64_t)r32 << 8) | ((uint64_t)r32p << 9);
       model[0] = m0;
       model[1] = m1;
       sm.hdr[0] = (uint8_t)l;
@@ -447,13 +679,16 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
         }
       }
     }
-    if (r32 && l > 0) pack_rows(lo, sm.signs, pk, len, l, ct, cn);  // residuals and signs: after the reduction's barriers
+    // residuals (and signs) are complete: the width reductions ended with a barrier
+    if (r32 && l > 0) pack_rows(lo, sm.signs, pk, len, l, ct, cn);
+    if (r32p && l > 0) pack_rows_dispatch(l, smem_u32(sm.vals), (len + 31) / 32, ct, cn);
   }
   group_sync<G>();
 
   const uint64_t size = sm.bcast[2], goff = sm.bcast[1];
   const uint32_t l = (uint32_t)(sm.bcast[3] & 0xff);
   const bool r32 = (sm.bcast[3] >> 8) & 1, raw = l == TB, rows = r32 && l > 0;
+  const bool rows_p = ((sm.bcast[3] >> 9) & 1) && l > 0;
   const uint32_t H = raw ? 1u : 17u;
   const double m0 = model[0], m1 = model[1];
   if (goff == ~0ull) return;  // look-back gave up (error word set)
@@ -466,6 +701,8 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
   // ---- body ----------------------------------------------------------------------
   if (raw) {
     write_image(a.payload, goff, size, H, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return __ldg(src + k); }, tid, nt);
+  } else if (rows_p) {
+    write_image_rows(a.payload, goff, size, H, sm.hdr, lo, l, (len + 31) / 32, tid, nt);
   } else if (rows) {
     write_image_packed(a.payload, goff, size, H, sm.hdr, pk, tid, nt);
   } else {
@@ -518,7 +755,7 @@ __device__ __forceinline__ uint32_t legacy_residuals(const EncSmem<T> &sm, doubl
   u128 rmx = (u128)(uint64_t)(int64_t)dmax, rmn = (u128)(uint64_t)(int64_t)dmin;
   group_reduce2<3, 4, G>(rmx, rmn, sm.red);
   const int32_t mid = (int32_t)((uint32_t)(uint64_t)rmx + (uint32_t)(uint64_t)rmn);
-  m0 = __dadd_rn(m0, __ddiv_rn(__int2double_rn(mid), 2.0));
+  m0 = __dadd_rn(m0, __dmul_rn(__int2double_rn(mid), 0.5));  // x * 0.5 rounds exactly as x / 2.0
   fast = model_in_range(m0, m1, 0.0, len);
   uint32_t emax = 0;
   for (uint32_t i0 = 0; i0 < len; i0 += nt) {
@@ -634,7 +871,7 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
         dmin = (int64_t)(uint64_t)rmn;
         narrow_range = dmax >= dmin && (uint64_t)(dmax - dmin) < (1ull << 30);
         const int64_t mid = (int64_t)((uint64_t)dmax + (uint64_t)dmin);
-        m0 = __dadd_rn(m0, __ddiv_rn(__ll2double_rn(mid), 2.0));
+        m0 = __dadd_rn(m0, __dmul_rn(__ll2double_rn(mid), 0.5));  // x * 0.5 rounds exactly as x / 2.0
       }
       // ---- residuals (…_integer_template.h:51-72, poly :37-58) -----------------
       uint64_t rmax = 0;
