@@ -116,7 +116,8 @@ uint64_t leco_block_bytes(int codec, int dtype, uint32_t l, uint32_t nvalues);
  * entries).  Replaces the driver loop over <Codec>::encodeArray8_int
  * (experiments/leco_int_fix_template.cpp:111-127).  One single-pass kernel
  * (plus a sequential-fit kernel for LECO_FIT_REFERENCE columns whose FP64 sums
- * round), a block-size prefix sum by decoupled look-back through d_workspace. */
+ * round), a block-size prefix sum by decoupled look-back through d_workspace.
+ * d_payload must be 16-byte aligned (the images are written in 16-byte stores). */
 int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t block_size, int fit_mode,
                 uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, leco_dir_entry *d_dir,
                 void *d_workspace, uint64_t workspace_bytes, leco_stream_t stream);

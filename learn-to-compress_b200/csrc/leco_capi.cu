@@ -146,8 +146,8 @@ int leco_encode(int codec, int dtype, const void *d_values, uint64_t n, uint32_t
   if (!block_size || block_size > LECO_MAX_BLOCK) return fail(LECO_ERR_ARG, "leco_encode: block_size must be in 1..16384");
   if (n == 0) return fail(LECO_ERR_ARG, "leco_encode: n must be > 0");
   if (!d_values || !d_payload || !d_offsets || !d_workspace) return fail(LECO_ERR_ARG, "leco_encode: null pointer");
-  if ((reinterpret_cast<uintptr_t>(d_payload) & 7) || (reinterpret_cast<uintptr_t>(d_values) & (dtype - 1)))
-    return fail(LECO_ERR_ARG, "leco_encode: payload must be 8-byte aligned and values aligned to their size");
+  if ((reinterpret_cast<uintptr_t>(d_payload) & 15) || (reinterpret_cast<uintptr_t>(d_values) & (dtype - 1)))
+    return fail(LECO_ERR_ARG, "leco_encode: payload must be 16-byte aligned and values aligned to their size");
   if (fit_mode != LECO_FIT_REFERENCE && fit_mode != LECO_FIT_EXACT) return fail(LECO_ERR_ARG, "leco_encode: bad fit_mode");
   const uint64_t nb = leco_num_blocks(n, block_size);
   if (nb > 0xffffffffull) return fail(LECO_ERR_ARG, "leco_encode: too many blocks");

@@ -22,9 +22,16 @@
 
 namespace leco {
 
-// u64 LeCo blocks are held to 40 registers, six CTAs per SM (their shared memory allows six).
+// CTAs per SM the encoder's register budget is set for: six (40 registers) for u64 LeCo
+// blocks, whose shared memory allows six, and for the other u32 codecs; five (48) for
+// the other u64 codecs; four (64) for degree-2 blocks.
 template <typename T, int CODEC>
-__global__ void __launch_bounds__(256, (CODEC == kLinear && sizeof(T) == 8) ? 6 : 1) encode_kernel(EncodeArgs a) {
+constexpr int enc_min_ctas() {
+  return CODEC == kPoly2 ? 4 : (sizeof(T) == 4 || CODEC == kLinear) ? 6 : 5;
+}
+
+template <typename T, int CODEC>
+__global__ void __launch_bounds__(256, enc_min_ctas<T, CODEC>()) encode_kernel(EncodeArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   __shared__ uint64_t ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1u);
@@ -32,6 +39,9 @@ __global__ void __launch_bounds__(256, (CODEC == kLinear && sizeof(T) == 8) ? 6 
   const uint64_t b = ticket;
   if (b >= a.nb) return;
   encode_block<T, CODEC>(a, b, smem_raw);
+  // block 0 has published its inclusive prefix: its first warp stays on as the prefix
+  // publisher for the rest of the column
+  if (b == 0 && threadIdx.x < 32 && a.nb > 1) publish_prefixes(a.status, a.nb, a.error);
 }
 
 // Small blocks: one warp per block, eight blocks per CTA, each warp with its

@@ -109,6 +109,89 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint64_t b
   return excl;
 }
 
+// Prefix publisher, one warp.  A block's own look-back ends at the nearest inclusive
+// prefix, but those lag: a block publishes its inclusive prefix only when its own
+// look-back is done, so with ~900 blocks in flight each look-back sums long runs of
+// totals.  This warp walks the status words in block order (128 per step, lane i
+// holding blocks j + 4i .. j + 4i + 3) and turns every published total into an
+// inclusive prefix as soon as it and all blocks before it have published, so the blocks
+// find one among their nearest predecessors.  Every value it writes is the one the
+// block's own look-back would publish.  Block 0's inclusive prefix must be published
+// (by this warp) before the call.  Returns after block nb - 1, or sets kErrTimeout on a
+// wait that exceeds the spin limit.
+__device__ __forceinline__ void publish_prefixes(uint64_t *status, uint64_t nb, uint32_t *error,
+                                                 uint32_t spin_limit = kSpinLimit) {
+  constexpr int K = 4;
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  uint64_t run = ld_relaxed(&status[0]) & kValMask;  // inclusive prefix before block j
+  uint64_t j = 1;
+  uint32_t spins = 0, ns = 32;
+  while (j < nb) {
+    uint64_t v[K];
+    int first = K * 32;  // this lane's first unpublished position
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint64_t idx = j + K * lane + k;
+      v[k] = idx < nb ? ld_relaxed(&status[idx]) : 0;
+    }
+#pragma unroll
+    for (int k = K - 1; k >= 0; --k)
+      if ((v[k] >> 62) == 0) first = K * lane + k;
+    const int n = __reduce_min_sync(0xffffffffu, first);  // published run j .. j + n - 1
+    if (n == 0) {
+      if (++spins > spin_limit) {
+        if (lane == 0) atomicOr(error, kErrTimeout);
+        return;
+      }
+      __nanosleep(ns);
+      if (ns < 256) ns <<= 1;
+      continue;
+    }
+    spins = 0;
+    ns = 32;
+    // Segmented inclusive scan: an inclusive prefix restarts the sum.  Lane-local first...
+    uint64_t p[K];
+    bool f[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint64_t val = v[k] & kValMask;
+      const bool fl = (v[k] >> 62) == 2;
+      p[k] = (k == 0 || fl) ? val : p[k - 1] + val;
+      f[k] = fl || (k > 0 && f[k - 1]);
+    }
+    // ... then over the lanes' totals
+    uint64_t tp = p[K - 1];
+    int tf = f[K - 1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint64_t q = __shfl_up_sync(0xffffffffu, tp, d);
+      const int fq = __shfl_up_sync(0xffffffffu, tf, d);
+      if (lane >= d && !tf) {
+        tp += q;
+        tf = fq;
+      }
+    }
+    uint64_t ep = __shfl_up_sync(0xffffffffu, tp, 1);
+    int ef = __shfl_up_sync(0xffffffffu, tf, 1);
+    if (lane == 0) {
+      ep = 0;
+      ef = 0;
+    }
+    if (!ef) ep += run;
+    uint64_t last = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint64_t fin = f[k] ? p[k] : ep + p[k];
+      const int pos = K * lane + k;
+      if (pos < n && (v[k] >> 62) == 1) st_relaxed(&status[j + pos], kFlagIncl | fin);
+      if (pos == n - 1) last = fin;
+    }
+    run = __shfl_sync(0xffffffffu, last, (n - 1) / K);
+    j += n;
+  }
+}
+
 // True when every prediction of a len-value block with model (a0, a1, a2) is a
 // finite double inside (-2^62, 2^62): the x86 out-of-range rule cannot apply.
 __device__ __forceinline__ bool model_in_range(double a0, double a1, double a2, uint32_t len) {
@@ -385,17 +468,55 @@ static __device__ __noinline__ void pack_rows_dispatch(uint32_t l, uint32_t vb, 
   }
 }
 
-// write_image_packed for rows packed by pack_rows_dispatch: body word k is word
-// k mod L of row t = k / L, at v32[t*64 + t mod 32 + k mod L]; words past the last
-// row read as zero (the image's zero tail).  k / L is a multiply-high by
-// ceil(2^32 / L), exact for k < 2^16 (a block body has at most 16384 words).
-__device__ __forceinline__ void write_image_rows(uint8_t *payload, uint64_t goff, uint64_t size, uint32_t H,
-                                                 const uint8_t *hdr, const uint32_t *v32, uint32_t L, uint32_t rows,
-                                                 uint32_t rank, uint32_t nthreads) {
+// Stores bytes [lo, hi) of the 16-byte chunk (w0..w3, little-endian) at dst (16-byte
+// aligned) with the fewest aligned stores: the chunk's other bytes belong to the
+// neighbouring block's image, written by another CTA.
+__device__ __forceinline__ void store_chunk_bytes(uint8_t *dst, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
+                                                  uint32_t lo, uint32_t hi) {
+  for (uint32_t pos = lo; pos < hi;) {
+    const uint32_t rem = hi - pos, wi = pos >> 2, sh = (pos & 3u) * 8u;
+    const uint32_t w = wi == 0 ? w0 : wi == 1 ? w1 : wi == 2 ? w2 : w3;
+    if ((pos & 7u) == 0 && rem >= 8) {
+      const uint32_t wn = wi == 0 ? w1 : w3;
+      *reinterpret_cast<uint64_t *>(dst + pos) = ((uint64_t)wn << 32) | w;
+      pos += 8;
+    } else if ((pos & 3u) == 0 && rem >= 4) {
+      *reinterpret_cast<uint32_t *>(dst + pos) = w;
+      pos += 4;
+    } else if ((pos & 1u) == 0 && rem >= 2) {
+      *reinterpret_cast<uint16_t *>(dst + pos) = (uint16_t)(w >> sh);
+      pos += 2;
+    } else {
+      dst[pos] = (uint8_t)(w >> sh);
+      pos += 1;
+    }
+  }
+}
+
+// Writes the image [goff, goff + size) of a non-raw LeCo block (17-byte header in hdr,
+// 4-byte aligned, bytes 17.. zero) whose body rows were packed by pack_rows_dispatch:
+// body word k is word k mod L of row t = k / L, at v32[t*64 + t mod 32 + k mod L]; words
+// past the last row read as zero (the image's zero tail).  k / L is a multiply-high by
+// ceil(2^32 / L), exact for k < 2^16 (a block body has at most 16384 words).  16-byte
+// chunks inside the body are funnel-shifted from body words; the chunks holding the
+// header or shared with a neighbouring image from image words (header words, then body
+// words shifted by the header's 17 bytes), stored byte-exactly.
+__device__ __forceinline__ void write_image_rows(uint8_t *payload, uint64_t goff, uint64_t size, const uint8_t *hdr,
+                                                 const uint32_t *v32, uint32_t L, uint32_t rows, uint32_t rank,
+                                                 uint32_t nthreads) {
+  constexpr uint32_t H = 17;
   const uint32_t M = L > 1 ? 0xffffffffu / L + 1u : 0u, nw = rows * L;
   auto word = [&](uint32_t k) -> uint32_t {
     const uint32_t t = L > 1 ? __umulhi(k, M) : k;
     return k < nw ? v32[t * 64u + (t & 31u) + (k - t * L)] : 0u;
+  };
+  const uint32_t *hw = reinterpret_cast<const uint32_t *>(hdr);
+  // image word m: image bytes 4m .. 4m+3 (m < 0: before the image, never stored)
+  auto img = [&](int32_t m) -> uint32_t {
+    if (m < 0) return 0u;
+    if (m < 4) return hw[m];
+    if (m == 4) return (hw[4] & 0xffu) | (word(0) << 8);
+    return __funnelshift_r(word((uint32_t)m - 5u), word((uint32_t)m - 4u), 24);
   };
   const uint64_t gend = goff + size;
   const uint64_t c0 = goff >> 4, c1 = (gend + 15) >> 4;
@@ -408,16 +529,18 @@ __device__ __forceinline__ void write_image_rows(uint8_t *payload, uint64_t goff
       *reinterpret_cast<uint4 *>(payload + cb) = make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
                                                             __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
     } else {
-      for (int j = 0; j < 16; ++j) {
-        const uint64_t g = cb + j;
-        if (g < goff || g >= gend) continue;
-        const uint64_t i = g - goff;
-        if (i < H) {
-          payload[g] = hdr[i];
-        } else {
-          const uint32_t bi = (uint32_t)(i - H);
-          payload[g] = (uint8_t)(word(bi >> 2) >> ((bi & 3u) * 8u));
-        }
+      const int32_t e = (int32_t)((int64_t)cb - (int64_t)goff);  // image offset of the chunk (>= -15)
+      const int32_t m0 = e >> 2;                                 // floor(e / 4)
+      const uint32_t sh = (uint32_t)(e & 3) * 8u;
+      const uint32_t i0 = img(m0), i1 = img(m0 + 1), i2 = img(m0 + 2), i3 = img(m0 + 3), i4 = img(m0 + 4);
+      const uint32_t lo = cb < goff ? (uint32_t)(goff - cb) : 0u;
+      const uint32_t hi = cb + 16 > gend ? (uint32_t)(gend - cb) : 16u;
+      if (lo == 0 && hi == 16) {
+        *reinterpret_cast<uint4 *>(payload + cb) = make_uint4(__funnelshift_r(i0, i1, sh), __funnelshift_r(i1, i2, sh),
+                                                              __funnelshift_r(i2, i3, sh), __funnelshift_r(i3, i4, sh));
+      } else {
+        store_chunk_bytes(payload + cb, __funnelshift_r(i0, i1, sh), __funnelshift_r(i1, i2, sh),
+                          __funnelshift_r(i2, i3, sh), __funnelshift_r(i3, i4, sh), lo, hi);
       }
     }
   }
@@ -702,7 +825,7 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
   if (raw) {
     write_image(a.payload, goff, size, H, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return __ldg(src + k); }, tid, nt);
   } else if (rows_p) {
-    write_image_rows(a.payload, goff, size, H, sm.hdr, lo, l, (len + 31) / 32, tid, nt);
+    write_image_rows(a.payload, goff, size, sm.hdr, lo, l, (len + 31) / 32, tid, nt);
   } else if (rows) {
     write_image_packed(a.payload, goff, size, H, sm.hdr, pk, tid, nt);
   } else {
