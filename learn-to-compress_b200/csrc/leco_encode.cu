@@ -57,11 +57,44 @@ __global__ void __launch_bounds__(256) encode_kernel_warp(EncodeArgs a, uint32_t
   encode_block<T, CODEC, 32>(a, b, smem_raw + (size_t)w * slice);
 }
 
+// The model of a len-value block from the sums of the reference's fit loop (linear:
+// sum y, sum i*y; poly: the three Y sums): lr_int_T::caltheta (lr.h:79-83) with the
+// x sums in closed form -- sum i and sum i*i are exact integers below 2^53 at every
+// step of the reference's loop (i < 16384), so these are the same doubles -- or the
+// degree-2 solve.
+template <int CODEC>
+__device__ __forceinline__ void store_seq_model(double *m, double s0, double s1, double s2, uint32_t len, uint32_t bs,
+                                                const PolyX &px) {
+  if (CODEC == kLinear) {
+    const double md = __uint2double_rn(len);
+    const uint64_t ml = len;
+    const double sumx = __ull2double_rn(ml * (ml - 1) / 2), sumxx = __ull2double_rn((ml - 1) * ml * (2 * ml - 1) / 6);
+    const double ccc = __dsub_rn(__dmul_rn(s1, md), __dmul_rn(sumx, s0));
+    const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
+    const double t1 = __ddiv_rn(ccc, xxx);
+    m[0] = __ddiv_rn(__dsub_rn(s0, __dmul_rn(t1, sumx)), md);
+    m[1] = t1;
+    m[2] = 0.0;
+  } else {
+    const double *X = px.x + (len == bs ? 0 : 5);
+    double Y[3] = {s0, s1, s2}, c[3];
+    poly2_solve(X, Y, c);
+    m[0] = c[0];
+    m[1] = c[1];
+    m[2] = c[2];
+  }
+}
+
 // Sequential reference fits, one warp per 32 blocks: each step the warp loads a
 // 32 x 32 tile (32 consecutive values of each of its 32 blocks, coalesced) into
 // shared memory while the next tile is already in flight to registers; lane j
 // then adds the 32 values of block j to its running sums in order, exactly the
 // reference's loop (lr.h:72-77; Y sums of polynomial_regression_internals.hpp:129-137).
+// A full tile's 32 conversions and products are taken before its adds, so the
+// lane's critical path is the add chains alone (the loop that waited on a load and
+// a conversion at every step took ~200 us per block of 4096 values).  Twelve warps
+// per SM (registers) hold a whole 200M-value column's 1526 warps in one wave, where
+// the loads are in flight across warps; a lone warp waits for each next tile.
 template <typename T, int CODEC>
 __global__ void __launch_bounds__(128) seq_fit_tiled_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs,
                                                             uint64_t nb, PolyX px, double *__restrict__ models) {
@@ -81,7 +114,7 @@ __global__ void __launch_bounds__(128) seq_fit_tiled_kernel(const T *__restrict_
       nxt[r] = (b0 + r < nb && i < bs && g < n) ? __ldg(values + g) : (T)0;
     }
   };
-  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;  // linear: sumx sumy sumxx sumxy; poly: Y0 Y1 Y2
+  double s0 = 0, s1 = 0, s2 = 0;  // linear: sumy sumxy; poly: Y0 Y1 Y2
   uint32_t maxlen = len;
   for (int m = 16; m; m >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
   fetch(0);
@@ -91,47 +124,141 @@ __global__ void __launch_bounds__(128) seq_fit_tiled_kernel(const T *__restrict_
     __syncwarp();
     if (t0 + 32 < maxlen) fetch(t0 + 32);
     const uint32_t cnt = len > t0 ? (len - t0 < 32 ? len - t0 : 32) : 0;
-    for (uint32_t c = 0; c < cnt; ++c) {
-      const uint32_t i = t0 + c;
-      const double di = __uint2double_rn(i), yi = to_double<T>(tile[w][lane][c]);
+    const double dt0 = u32_to_double_fp64(t0);
+    if (cnt == 32) {
+      // y_i * i (linear) or the three Y terms (poly), all before the first add
+      double yv[32], pv[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        yv[c] = to_double<T>(tile[w][lane][c]);
+        pv[c] = __dmul_rn(__dadd_rn(dt0, (double)c), yv[c]);  // i = t0 + c exactly
+      }
       if (CODEC == kLinear) {
-        s0 = __dadd_rn(s0, di);
-        s1 = __dadd_rn(s1, yi);
-        s2 = __dadd_rn(s2, __dmul_rn(di, di));
-        s3 = __dadd_rn(s3, __dmul_rn(di, yi));
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          s0 = __dadd_rn(s0, yv[c]);
+          s1 = __dadd_rn(s1, pv[c]);
+        }
       } else {
-        s0 = __dadd_rn(s0, __dmul_rn(1.0, yi));
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const double di = __dadd_rn(dt0, (double)c);
+          s0 = __dadd_rn(s0, yv[c]);  // the reference's 1.0 * y is y
+          s1 = __dadd_rn(s1, pv[c]);
+          s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yv[c]));
+        }
+      }
+    } else {
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const double di = __dadd_rn(dt0, __uint2double_rn(c)), yi = to_double<T>(tile[w][lane][c]);
+        s0 = __dadd_rn(s0, yi);
         s1 = __dadd_rn(s1, __dmul_rn(di, yi));
-        s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yi));
+        if (CODEC != kLinear) s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yi));
       }
     }
     __syncwarp();
   }
-  if (!len) return;
-  double *m = models + mine * 3;
-  if (CODEC == kLinear) {
-    const double md = __uint2double_rn(len);
-    const double ccc = __dsub_rn(__dmul_rn(s3, md), __dmul_rn(s0, s1));
-    const double xxx = __dsub_rn(__dmul_rn(s2, md), __dmul_rn(s0, s0));
-    const double t1 = __ddiv_rn(ccc, xxx);
-    m[0] = __ddiv_rn(__dsub_rn(s1, __dmul_rn(t1, s0)), md);
-    m[1] = t1;
-    m[2] = 0.0;
-  } else {
-    const double *X = px.x + (len == bs ? 0 : 5);
-    double Y[3] = {s0, s1, s2}, c[3];
-    poly2_solve(X, Y, c);
-    m[0] = c[0];
-    m[1] = c[1];
-    m[2] = c[2];
-  }
+  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px);
 }
 
+// The same fits with a deeper pipeline per warp, for columns whose warps fit in one
+// wave of this kernel (four CTAs per SM): one warp per CTA, lane j fits block b0 + j,
+// and a ring of kFitStages stages holds the next tiles of all 32 blocks (row j: block
+// b0 + j, padded by 16 bytes so that the lanes' 16-byte reads of their own rows spread
+// over the banks).  A stage is filled by coalesced 16-byte cp.async copies (one group
+// per stage) and read after the warp has waited for its group, so a lone warp's add
+// chains are no longer held up by its loads (one block of 4096 values: ~60 us instead
+// of ~110 us).  Needs 16-byte aligned values and bs * sizeof(T) a multiple of 16.
+// Tiles of fewer than 32 values (a block's last when bs is not a multiple of 32, the
+// column's short last block) are read from global memory directly.
+constexpr int kFitStages = 6;
+template <typename T>
+__host__ __device__ constexpr uint32_t fit_row_bytes() { return 32u * sizeof(T) + 16u; }
+template <typename T>
+__host__ __device__ constexpr uint32_t fit_smem_bytes() { return (uint32_t)kFitStages * 32u * fit_row_bytes<T>(); }
+
 template <typename T, int CODEC>
-__global__ void __launch_bounds__(128) seq_fit_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t nb,
-                                                       PolyX px, double *__restrict__ models) {
-  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < nb) seq_fit_block<T, CODEC>(values, n, bs, b, px.x, models);
+__global__ void __launch_bounds__(32) seq_fit_ring_kernel(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t nb,
+                                                          PolyX px, double *__restrict__ models) {
+  constexpr uint32_t S = sizeof(T), RB = fit_row_bytes<T>(), SB = 32u * RB;
+  constexpr uint32_t CPR = 32u * S / 16u;  // 16-byte chunks per row: 16 (u64) or 8 (u32)
+  constexpr uint32_t RPI = 32u / CPR;      // rows per copy instruction
+  extern __shared__ __align__(128) uint8_t ring[];
+  const uint32_t lane = threadIdx.x;
+  const uint64_t b0 = (uint64_t)blockIdx.x * 32, mine = b0 + lane;
+  const uint32_t len = mine < nb ? (uint32_t)umin64(bs, n - mine * bs) : 0;
+  const uint32_t ntiles = (__reduce_max_sync(0xffffffffu, len) + 31) / 32;
+  const uint32_t sring = smem_u32(ring);
+  // tile t of every row whose 32 values all exist; instruction q copies rows
+  // RPI*q .. RPI*q + RPI-1, lane k of a row's CPR lanes its k-th 16 bytes
+  auto issue = [&](uint32_t t) {
+    if (t < ntiles) {
+      const uint32_t k = lane % CPR, s = t % kFitStages;
+#pragma unroll
+      for (uint32_t q = 0; q < CPR; ++q) {
+        const uint32_t r = RPI * q + lane / CPR;
+        const uint32_t lr = __shfl_sync(0xffffffffu, len, r);
+        if (lr >= 32 * (t + 1))
+          cp_async16(sring + s * SB + r * RB + 16 * k, values + (b0 + r) * bs + 32 * t + k * (16 / S));
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  for (uint32_t t = 0; t < (uint32_t)kFitStages; ++t) issue(t);
+  double s0 = 0, s1 = 0, s2 = 0;  // linear: sumy sumxy; poly: Y0 Y1 Y2
+  for (uint32_t t = 0; t < ntiles; ++t) {
+    const uint32_t s = t % kFitStages;
+    asm volatile("cp.async.wait_group %0;" ::"n"(kFitStages - 1) : "memory");  // tile t's group has landed
+    __syncwarp();
+    const uint32_t cnt = len > 32 * t ? min(32u, len - 32 * t) : 0u;
+    const uint8_t *src = ring + s * SB + lane * RB;
+    const double dt0 = u32_to_double_fp64(32 * t);
+    if (cnt == 32) {
+      double yv[32], pv[32];
+#pragma unroll
+      for (int q = 0; q < (int)CPR; ++q) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(src + 16 * q);
+        if (S == 8) {
+          yv[2 * q] = to_double<T>((T)(((uint64_t)v.y << 32) | v.x));
+          yv[2 * q + 1] = to_double<T>((T)(((uint64_t)v.w << 32) | v.z));
+        } else {
+          yv[4 * q] = to_double<T>((T)v.x);
+          yv[4 * q + 1] = to_double<T>((T)v.y);
+          yv[4 * q + 2] = to_double<T>((T)v.z);
+          yv[4 * q + 3] = to_double<T>((T)v.w);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 32; ++c) pv[c] = __dmul_rn(__dadd_rn(dt0, (double)c), yv[c]);  // i = 32t + c exactly
+      if (CODEC == kLinear) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          s0 = __dadd_rn(s0, yv[c]);
+          s1 = __dadd_rn(s1, pv[c]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const double di = __dadd_rn(dt0, (double)c);
+          s0 = __dadd_rn(s0, yv[c]);  // the reference's 1.0 * y is y
+          s1 = __dadd_rn(s1, pv[c]);
+          s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yv[c]));
+        }
+      }
+    } else {
+      const T *tv = values + mine * bs + 32 * t;  // not staged
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const double di = __dadd_rn(dt0, __uint2double_rn(c)), yi = to_double<T>(__ldg(tv + c));
+        s0 = __dadd_rn(s0, yi);
+        s1 = __dadd_rn(s1, __dmul_rn(di, yi));
+        if (CODEC != kLinear) s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yi));
+      }
+    }
+    __syncwarp();  // every lane's reads of this stage are done before it is refilled
+    issue(t + kFitStages);
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px);
 }
 
 // ---- host launchers ---------------------------------------------------------------
@@ -146,8 +273,22 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
   for (int i = 0; i < 10; ++i) a.polyX[i] = px.x[i] = L.polyX[i];
   if (L.seq_models && (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy)) {
     // four warps per CTA, 32 blocks per warp (the legacy codec fits as LINEAR does)
-    seq_fit_tiled_kernel<T, CODEC == kLegacy ? kLinear : CODEC><<<(unsigned)((L.nb + 127) / 128), 128, 0, st>>>(
-        reinterpret_cast<const T *>(L.values), L.n, L.bs, L.nb, px, L.seq_models);
+    constexpr int FC = CODEC == kLegacy ? kLinear : CODEC;
+    const uint64_t warps = (L.nb + 31) / 32;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (warps <= 4ull * (uint64_t)sms && (reinterpret_cast<uintptr_t>(L.values) & 15) == 0 &&
+        ((uint64_t)L.bs * sizeof(T)) % 16 == 0) {
+      constexpr uint32_t fsm = fit_smem_bytes<T>();
+      if (fsm > 48 * 1024)
+        cudaFuncSetAttribute(seq_fit_ring_kernel<T, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+      seq_fit_ring_kernel<T, FC><<<(unsigned)warps, 32, fsm, st>>>(reinterpret_cast<const T *>(L.values), L.n, L.bs,
+                                                                   L.nb, px, L.seq_models);
+    } else {
+      seq_fit_tiled_kernel<T, FC><<<(unsigned)((L.nb + 127) / 128), 128, 0, st>>>(
+          reinterpret_cast<const T *>(L.values), L.n, L.bs, L.nb, px, L.seq_models);
+    }
     a.seq_models = L.seq_models;
   }
   const uint32_t smem = enc_smem_bytes(L.bs, sizeof(T));

@@ -622,11 +622,17 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     // ---- 32-bit path (16-byte aligned blocks whose predictions lie in [0, 2^51)) -----
     const uint32_t vb = smem_u32(sm.vals), np = len >> 1;
     // The block's values into their pair slots, every copy of this thread in flight.
-    auto stage_pairs = [&]() {
+    auto issue_pairs = [&]() {
       for (uint32_t q = ct; q < np; q += cn) cp_async16(vb + 16u * pair16_slot(q), src + 2 * q);
       if ((len & 1) && ct == 0) cp_async8(vb + 16u * pair16_slot(np), src + len - 1);
+    };
+    auto land_pairs = [&]() {
       cp_async_wait_all();
       group_sub_sync<G>();
+    };
+    auto stage_pairs = [&]() {
+      issue_pairs();
+      land_pairs();
     };
     // Midpoint pass over the staged values: every d = y - pred is taken in 64 bits but
     // its max and min in 32 bits, with a check that each d fits in an int32 (its high
@@ -666,12 +672,13 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     const bool al16 = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
     bool pairs = false;  // the 32-bit midpoint pass ran over the staged pairs
     if (a.seq_models) {
+      // the values stream into their pair slots while the model is read; they have
+      // landed before either midpoint pass (the 64-bit one overwrites the region)
+      if (al16) issue_pairs();
       m0 = a.seq_models[b * 3 + 0];
       m1 = a.seq_models[b * 3 + 1];
-      if (al16 && preds_nonneg(m0, m1, len)) {
-        stage_pairs();
-        pairs = mid_pass32();
-      }
+      if (al16) land_pairs();
+      if (al16 && preds_nonneg(m0, m1, len)) pairs = mid_pass32();
       if (!pairs) narrow_range = mid_pass(true);
     } else {
       // Moments in 32-bit halves of y: a thread sees at most 16384 values, each
