@@ -309,7 +309,9 @@ int leco_filter_range(int codec, int dtype, const uint8_t *d_payload, const uint
   L.f1 = filter;
   L.zone = d_zone_max;
   L.zone_lo = d_zone_min;
-  if (launch_filter(codec, dtype, L, 0, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range: no kernel");
+  const int lrc = launch_filter(codec, dtype, L, 0, st);
+  if (lrc > 0) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range: no kernel");
+  if (lrc < 0) return cuda_fail((cudaError_t)-lrc, "leco_filter_range: launch");
   LECO_CUDA(cudaGetLastError());
   return LECO_OK;
 }
@@ -328,7 +330,9 @@ int leco_filter_range_close(int codec, int dtype, const uint8_t *d_payload, cons
   L.f2 = filter2;
   L.base = base;
   L.zone = codec == kLinear ? d_zone_min : nullptr;
-  if (launch_filter(codec, dtype, L, 1, st)) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range_close: no kernel");
+  const int lrc = launch_filter(codec, dtype, L, 1, st);
+  if (lrc > 0) return fail(LECO_ERR_UNSUPPORTED, "leco_filter_range_close: no kernel");
+  if (lrc < 0) return cuda_fail((cudaError_t)-lrc, "leco_filter_range_close: launch");
   LECO_CUDA(cudaGetLastError());
   return LECO_OK;
 }

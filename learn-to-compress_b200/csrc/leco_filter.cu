@@ -463,8 +463,16 @@ constexpr uint64_t kCountMask = (1ull << 40) - 1, kRunFlag = 1ull << 63;
 // offset and zone-map loads of the group in flight at once); blocks decided by
 // their plan are counted from it, the others (read blocks, window loops) by the
 // whole warp one after another.  Writes counts[b] and the group's total.
+// The three passes are chained by programmatic dependent launch: each lets the next
+// one be launched as soon as all its CTAs run, and the next one waits for the whole
+// previous grid (griddepcontrol.wait: completed, its writes visible) before it reads
+// anything that grid writes.  The launch gaps between the passes are hidden that way.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <int S, int CODEC>
 __global__ void __launch_bounds__(kFT) filter_count_kernel(FilterLaunch a, int close) {
+  pdl_launch_dependents();
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t g = (uint64_t)blockIdx.x * kFB + (threadIdx.x >> 5);
   const uint64_t b0 = g * 32;
@@ -499,6 +507,8 @@ __global__ void __launch_bounds__(kFT) filter_count_kernel(FilterLaunch a, int c
 __global__ void __launch_bounds__(1024) filter_scan_kernel(uint64_t *group_tot, uint64_t ngroups, uint64_t *count) {
   __shared__ uint64_t wsum[33];
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  pdl_launch_dependents();
+  pdl_wait_prior_grid();  // every group total is written
   uint64_t carry = 0;
   for (uint64_t base = 0; base < ngroups; base += 1024) {
     const uint64_t i = base + tid;
@@ -539,6 +549,7 @@ template <int S, int CODEC>
 __global__ void __launch_bounds__(kFT) filter_write_kernel(FilterLaunch a, int close) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t b = (uint64_t)blockIdx.x * kFB + (threadIdx.x >> 5);
+  pdl_wait_prior_grid();  // the scan (and the counting pass before it) are complete
   if (b >= a.nb) return;  // whole warps only
   const uint64_t w = __ldg(a.counts + b);
   if (!(w & kCountMask)) return;
@@ -616,9 +627,20 @@ template <int S, int CODEC>
 static int run_filter(FilterLaunch L, int close, cudaStream_t st) {
   const uint64_t groups = (L.nb + 31) / 32;
   filter_count_kernel<S, CODEC><<<(unsigned)((groups + kFB - 1) / kFB), kFT, 0, st>>>(L, close);
-  filter_scan_kernel<<<1, 1024, 0, st>>>(L.group_tot, groups, L.count);
-  filter_write_kernel<S, CODEC><<<(unsigned)((L.nb + kFB - 1) / kFB), kFT, 0, st>>>(L, close);
-  return 0;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.stream = st;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(1024);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, filter_scan_kernel, L.group_tot, groups, L.count);
+  cfg.gridDim = dim3((unsigned)((L.nb + kFB - 1) / kFB));
+  cfg.blockDim = dim3(kFT);
+  if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, filter_write_kernel<S, CODEC>, L, close);
+  return e == cudaSuccess ? 0 : -(int)e;
 }
 
 int launch_filter(int codec, int s, const FilterLaunch &L, int close, cudaStream_t st) {

@@ -68,6 +68,7 @@ struct FilterLaunch {
 };
 
 int launch_encode(int codec, int s, const EncodeLaunch &L, cudaStream_t st);
+// 0: launched; 1: no kernel for the codec and type; < 0: -(cudaError_t) of a failed launch
 int launch_filter(int codec, int s, const FilterLaunch &L, int close, cudaStream_t st);
 int launch_zonemap(int codec, int s, const DecodeLaunch &L, uint64_t *zmin, uint64_t *zmax, cudaStream_t st);
 int launch_decode(int codec, int s, const DecodeLaunch &L, cudaStream_t st);
