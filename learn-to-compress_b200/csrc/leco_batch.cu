@@ -26,20 +26,104 @@
 
 namespace leco {
 
-template <typename T, int CODEC>
-__device__ __forceinline__ void batch_seq_one(const DevCol &c, uint64_t b, double *models) {
-  seq_fit_block<T, CODEC>(reinterpret_cast<const T *>(c.values), c.n, c.bs, b, c.polyX, models);
-}
-
-// Sequential reference fits for every block of the columns that need them.
+// Sequential reference fits for every block of the columns that need them, one warp
+// per 32 consecutive blocks of the batch (lane j: block g0 + j, whatever its column):
+// each step the warp loads 32 consecutive values of each of its blocks (one row per
+// block, coalesced; u32 and u64 rows mix) into shared memory while the next step's
+// values are already in flight to registers, and lane j adds its block's values to
+// its running sums in order -- the reference's loop (lr.h:72-77; Y sums of
+// polynomial_regression_internals.hpp:129-137), as seq_fit_tiled_kernel does for one
+// column.  A full step's conversions and products are taken before its adds.  (One
+// thread per block with its own loads waited ~50 ns per value on each load.)
 __global__ void __launch_bounds__(128) batch_seq_fit_kernel(BatchArgs B) {
-  const uint64_t gb = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gb >= B.total) return;
-  const uint32_t ci = find_column(B.prefix, B.ncols, gb);
-  const DevCol &c = B.cols[ci];
-  if (!c.seq) return;
-  const uint64_t p0 = __ldg(B.prefix + ci);
-  LECO_BATCH_DISPATCH(c.codec, c.dtype, batch_seq_one, c, gb - p0, B.models + p0 * 3);
+  __shared__ uint64_t tile[4][32][33];
+  __shared__ const uint8_t *row_ptr[4][32];
+  __shared__ uint32_t row_len[4][32], row_s[4][32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t g0 = ((uint64_t)blockIdx.x * 4 + w) * 32, gb = g0 + lane;
+  if (g0 >= B.total) return;
+  uint32_t len = 0, s = 8, bs = 1;
+  int codec = kLinear;
+  const uint8_t *vals = nullptr;
+  const double *polyX = nullptr;
+  double *model = nullptr;
+  if (gb < B.total) {
+    const uint32_t ci = find_column(B.prefix, B.ncols, gb);
+    const DevCol &c = B.cols[ci];
+    if (c.seq) {
+      const uint64_t b = gb - __ldg(B.prefix + ci);
+      len = (uint32_t)umin64(c.bs, c.n - b * c.bs);
+      s = (uint32_t)c.dtype;
+      bs = c.bs;
+      codec = c.codec;
+      vals = reinterpret_cast<const uint8_t *>(c.values) + b * c.bs * s;
+      polyX = c.polyX;
+      model = B.models + gb * 3;
+    }
+  }
+  row_ptr[w][lane] = vals;
+  row_len[w][lane] = len;
+  row_s[w][lane] = s;
+  const bool poly = codec == kPoly2;
+  const bool any_poly = __any_sync(0xffffffffu, poly && len);
+  const uint32_t maxlen = __reduce_max_sync(0xffffffffu, len);
+  uint64_t nxt[32];
+  auto fetch = [&](uint32_t t0) {
+    const uint32_t i = t0 + lane;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const uint32_t lr = row_len[w][r];
+      uint64_t v = 0;
+      if (i < lr) {
+        const uint8_t *vr = row_ptr[w][r];
+        v = row_s[w][r] == 8 ? __ldg(reinterpret_cast<const uint64_t *>(vr) + i)
+                             : (uint64_t)__ldg(reinterpret_cast<const uint32_t *>(vr) + i);
+      }
+      nxt[r] = v;
+    }
+  };
+  __syncwarp();
+  double s0 = 0, s1 = 0, s2 = 0;  // linear: sumy sumxy; poly: Y0 Y1 Y2
+  if (maxlen) fetch(0);
+  for (uint32_t t0 = 0; t0 < maxlen; t0 += 32) {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) tile[w][r][lane] = nxt[r];
+    __syncwarp();
+    if (t0 + 32 < maxlen) fetch(t0 + 32);
+    const uint32_t cnt = len > t0 ? (len - t0 < 32 ? len - t0 : 32) : 0;
+    const double dt0 = u32_to_double_fp64(t0);
+    if (cnt == 32) {
+      double yv[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) yv[c] = __ull2double_rn(tile[w][lane][c]);  // a u32 value converts the same way
+      if (!any_poly) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          s0 = __dadd_rn(s0, yv[c]);
+          s1 = __dadd_rn(s1, __dmul_rn(__dadd_rn(dt0, (double)c), yv[c]));  // i = t0 + c exactly
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const double di = __dadd_rn(dt0, (double)c);
+          s0 = __dadd_rn(s0, yv[c]);  // the reference's 1.0 * y is y
+          s1 = __dadd_rn(s1, __dmul_rn(di, yv[c]));
+          s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yv[c]));
+        }
+      }
+    } else {
+      for (uint32_t c = 0; c < cnt; ++c) {
+        const double di = __dadd_rn(dt0, __uint2double_rn(c)), yi = __ull2double_rn(tile[w][lane][c]);
+        s0 = __dadd_rn(s0, yi);
+        s1 = __dadd_rn(s1, __dmul_rn(di, yi));
+        if (poly) s2 = __dadd_rn(s2, __dmul_rn(__dmul_rn(di, di), yi));
+      }
+    }
+    __syncwarp();
+  }
+  if (!len) return;
+  if (poly) store_seq_model<kPoly2>(model, s0, s1, s2, len, bs, polyX);
+  else store_seq_model<kLinear>(model, s0, s1, s2, len, bs, polyX);
 }
 
 }  // namespace leco
@@ -220,7 +304,7 @@ int leco_batch_encode(leco_batch *b, leco_stream_t stream) {
   const BatchArgs B = args_of(b, b->err);
   cudaError_t e = cudaMemsetAsync(b->d_ws, 0, b->status_bytes + 256, st);  // look-back words + ticket
   if (e == cudaSuccess && b->any_seq)
-    batch_seq_fit_kernel<<<(unsigned)((B.total + 127) / 128), 128, 0, st>>>(B);
+    batch_seq_fit_kernel<<<(unsigned)((B.total + 127) / 128), 128, 0, st>>>(B);  // four warps of 32 blocks
   if (e == cudaSuccess) batch_encode_kernel<<<b->enc_grid, 256, b->enc_smem, st>>>(B);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? LECO_OK : berr(LECO_ERR_CUDA, std::string("leco_batch_encode: ") + cudaGetErrorString(e));

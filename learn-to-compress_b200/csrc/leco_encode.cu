@@ -57,34 +57,6 @@ __global__ void __launch_bounds__(256) encode_kernel_warp(EncodeArgs a, uint32_t
   encode_block<T, CODEC, 32>(a, b, smem_raw + (size_t)w * slice);
 }
 
-// The model of a len-value block from the sums of the reference's fit loop (linear:
-// sum y, sum i*y; poly: the three Y sums): lr_int_T::caltheta (lr.h:79-83) with the
-// x sums in closed form -- sum i and sum i*i are exact integers below 2^53 at every
-// step of the reference's loop (i < 16384), so these are the same doubles -- or the
-// degree-2 solve.
-template <int CODEC>
-__device__ __forceinline__ void store_seq_model(double *m, double s0, double s1, double s2, uint32_t len, uint32_t bs,
-                                                const PolyX &px) {
-  if (CODEC == kLinear) {
-    const double md = __uint2double_rn(len);
-    const uint64_t ml = len;
-    const double sumx = __ull2double_rn(ml * (ml - 1) / 2), sumxx = __ull2double_rn((ml - 1) * ml * (2 * ml - 1) / 6);
-    const double ccc = __dsub_rn(__dmul_rn(s1, md), __dmul_rn(sumx, s0));
-    const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
-    const double t1 = __ddiv_rn(ccc, xxx);
-    m[0] = __ddiv_rn(__dsub_rn(s0, __dmul_rn(t1, sumx)), md);
-    m[1] = t1;
-    m[2] = 0.0;
-  } else {
-    const double *X = px.x + (len == bs ? 0 : 5);
-    double Y[3] = {s0, s1, s2}, c[3];
-    poly2_solve(X, Y, c);
-    m[0] = c[0];
-    m[1] = c[1];
-    m[2] = c[2];
-  }
-}
-
 // Sequential reference fits, one warp per 32 blocks: each step the warp loads a
 // 32 x 32 tile (32 consecutive values of each of its 32 blocks, coalesced) into
 // shared memory while the next tile is already in flight to registers; lane j
@@ -158,7 +130,7 @@ __global__ void __launch_bounds__(128) seq_fit_tiled_kernel(const T *__restrict_
     }
     __syncwarp();
   }
-  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px);
+  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px.x);
 }
 
 // The same fits with a deeper pipeline per warp, for columns whose warps fit in one
@@ -258,7 +230,7 @@ __global__ void __launch_bounds__(32) seq_fit_ring_kernel(const T *__restrict__ 
     issue(t + kFitStages);
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
-  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px);
+  if (len) store_seq_model<CODEC>(models + mine * 3, s0, s1, s2, len, bs, px.x);
 }
 
 // ---- host launchers ---------------------------------------------------------------

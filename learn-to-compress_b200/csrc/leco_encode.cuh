@@ -622,17 +622,11 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     // ---- 32-bit path (16-byte aligned blocks whose predictions lie in [0, 2^51)) -----
     const uint32_t vb = smem_u32(sm.vals), np = len >> 1;
     // The block's values into their pair slots, every copy of this thread in flight.
-    auto issue_pairs = [&]() {
+    auto stage_pairs = [&]() {
       for (uint32_t q = ct; q < np; q += cn) cp_async16(vb + 16u * pair16_slot(q), src + 2 * q);
       if ((len & 1) && ct == 0) cp_async8(vb + 16u * pair16_slot(np), src + len - 1);
-    };
-    auto land_pairs = [&]() {
       cp_async_wait_all();
       group_sub_sync<G>();
-    };
-    auto stage_pairs = [&]() {
-      issue_pairs();
-      land_pairs();
     };
     // Midpoint pass over the staged values: every d = y - pred is taken in 64 bits but
     // its max and min in 32 bits, with a check that each d fits in an int32 (its high
@@ -672,13 +666,14 @@ __device__ __forceinline__ void encode_block_l64(const EncodeArgs &a, uint64_t b
     const bool al16 = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
     bool pairs = false;  // the 32-bit midpoint pass ran over the staged pairs
     if (a.seq_models) {
-      // the values stream into their pair slots while the model is read; they have
-      // landed before either midpoint pass (the 64-bit one overwrites the region)
-      if (al16) issue_pairs();
+      // (issuing the copies before the model is read was measured slower: the model's
+      // load then queues behind them)
       m0 = a.seq_models[b * 3 + 0];
       m1 = a.seq_models[b * 3 + 1];
-      if (al16) land_pairs();
-      if (al16 && preds_nonneg(m0, m1, len)) pairs = mid_pass32();
+      if (al16 && preds_nonneg(m0, m1, len)) {
+        stage_pairs();
+        pairs = mid_pass32();
+      }
       if (!pairs) narrow_range = mid_pass(true);
     } else {
       // Moments in 32-bit halves of y: a thread sees at most 16384 values, each
@@ -911,7 +906,9 @@ __device__ __forceinline__ uint32_t legacy_residuals(const EncSmem<T> &sm, doubl
 // guarantees that every block of the column with a smaller index was handed
 // to a group that has already started (ticket order), which makes the
 // look-back wait finite.  smem_raw: enc_smem_bytes(a.bs, sizeof(T)) bytes
-// owned by this group.
+// owned by this group.  (Running the look-back in the group's first warp from
+// the block's start, as the u64 LeCo path does, was measured slower here: the
+// other codecs' passes take longer with a warp fewer than the look-back saves.)
 template <typename T, int CODEC, int G = 256, int U = 2>
 __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, uint8_t *smem_raw) {
   if constexpr (CODEC == kLinear && sizeof(T) == 8 && G != 32) {
@@ -1198,52 +1195,40 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
 }
 
 // ---- sequential reference fits (LECO_FIT_REFERENCE) ---------------------------
-// One thread per block runs the reference's own FP64 loop, so the model is
-// bit-identical to lr_int_T::caltheta (lr.h:66-85) or to the Y sums of
-// polynomial_regression_iter (polynomial_regression_internals.hpp:129-137).
+// One lane per block adds the block's values in the reference's own order and FP64
+// operations, so the model is bit-identical to lr_int_T::caltheta (lr.h:66-85) or to
+// the Y sums of polynomial_regression_iter (polynomial_regression_internals.hpp:129-137)
+// (the kernels: seq_fit_tiled_kernel and seq_fit_ring_kernel in leco_encode.cu,
+// batch_seq_fit_kernel in leco_batch.cu).
 struct PolyX {
   double x[10];
 };
 
-template <typename T, int CODEC>
-__device__ __forceinline__ void seq_fit_block(const T *__restrict__ values, uint64_t n, uint32_t bs, uint64_t b,
-                                              const double *polyX, double *__restrict__ models) {
-  const uint64_t base = b * bs;
-  const uint32_t len = (uint32_t)umin64((uint64_t)bs, n - base);
-  const T *y = values + base;
-  if (CODEC == kLinear) {
-    double sumx = 0, sumy = 0, sumxx = 0, sumxy = 0;
-#pragma unroll 4
-    for (uint32_t i = 0; i < len; ++i) {
-      const double di = __uint2double_rn(i), yi = to_double<T>(__ldg(y + i));
-      sumx = __dadd_rn(sumx, di);
-      sumy = __dadd_rn(sumy, yi);
-      sumxx = __dadd_rn(sumxx, __dmul_rn(di, di));
-      sumxy = __dadd_rn(sumxy, __dmul_rn(di, yi));
-    }
+// The model of a len-value block from the sums of the reference's fit loop (linear:
+// sum y, sum i*y; poly: the three Y sums): lr_int_T::caltheta (lr.h:79-83) with the
+// x sums in closed form -- sum i and sum i*i are exact integers below 2^53 at every
+// step of the reference's loop (i < 16384), so these are the same doubles -- or the
+// degree-2 solve with the column's X sums (polyX: full block [0..4], tail block [5..9]).
+template <int CODEC>
+__device__ __forceinline__ void store_seq_model(double *m, double s0, double s1, double s2, uint32_t len, uint32_t bs,
+                                                const double *polyX) {
+  if (CODEC != kPoly2) {
     const double md = __uint2double_rn(len);
-    const double ccc = __dsub_rn(__dmul_rn(sumxy, md), __dmul_rn(sumx, sumy));
+    const uint64_t ml = len;
+    const double sumx = __ull2double_rn(ml * (ml - 1) / 2), sumxx = __ull2double_rn((ml - 1) * ml * (2 * ml - 1) / 6);
+    const double ccc = __dsub_rn(__dmul_rn(s1, md), __dmul_rn(sumx, s0));
     const double xxx = __dsub_rn(__dmul_rn(sumxx, md), __dmul_rn(sumx, sumx));
     const double t1 = __ddiv_rn(ccc, xxx);
-    const double t0 = __ddiv_rn(__dsub_rn(sumy, __dmul_rn(t1, sumx)), md);
-    models[b * 3 + 0] = t0;
-    models[b * 3 + 1] = t1;
-    models[b * 3 + 2] = 0.0;
+    m[0] = __ddiv_rn(__dsub_rn(s0, __dmul_rn(t1, sumx)), md);
+    m[1] = t1;
+    m[2] = 0.0;
   } else {
-    double Y0 = 0, Y1 = 0, Y2 = 0;
-#pragma unroll 4
-    for (uint32_t i = 0; i < len; ++i) {
-      const double di = __uint2double_rn(i), yi = to_double<T>(__ldg(y + i));
-      Y0 = __dadd_rn(Y0, __dmul_rn(1.0, yi));
-      Y1 = __dadd_rn(Y1, __dmul_rn(di, yi));
-      Y2 = __dadd_rn(Y2, __dmul_rn(__dmul_rn(di, di), yi));
-    }
     const double *X = polyX + (len == bs ? 0 : 5);
-    double Y[3] = {Y0, Y1, Y2}, c[3];
+    double Y[3] = {s0, s1, s2}, c[3];
     poly2_solve(X, Y, c);
-    models[b * 3 + 0] = c[0];
-    models[b * 3 + 1] = c[1];
-    models[b * 3 + 2] = c[2];
+    m[0] = c[0];
+    m[1] = c[1];
+    m[2] = c[2];
   }
 }
 
