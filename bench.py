@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="keys per GPU (default: 200M)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="decode", choices=["decode", "batch", "serve", "varlen", "filter", "gather", "codecs"],
+    ap.add_argument("--workload", default="decode",
+                    choices=["decode", "batch", "serve", "varlen", "filter", "gather", "codecs", "encode"],
                     help="decode: the 200M-key LeCo-fix column (default); batch: 4096 mixed columns through "
                          "the persistent batch engine vs per-column launches")
     ap.add_argument("--ncols", type=int, default=4096)
@@ -780,6 +781,61 @@ def run_codecs(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_encode(args, world, rank, local):
+    """LeCo-fix u64 encode of prefixes of the decode workload's column (1 block up to
+    the whole 200M keys, 4096-value blocks) with the reference fit and the exact fit:
+    the reference fit's fixed cost is its sequential add chain, 4096 steps for any
+    number of blocks.  CUDA events, mean of 10 encodes after 3 untimed; each
+    column's decode is checked against its keys."""
+    import torch
+
+    import leco_b200 as lc
+    from leco_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    x = workloads.piecewise_linear_u64(args.n, seed=2 + rank, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def ev(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e3
+
+    res = {}
+    nb_all = (args.n + BS - 1) // BS
+    with ClockSampler(local) as clk:
+        for nblk in (1, 32, 128, 1024, 4096, 12208, nb_all):
+            n = min(args.n, nblk * BS)
+            xs = x[:n]
+            col = lc.encode(xs, lc.LINEAR, BS, lc.FIT_REFERENCE)
+            assert torch.equal(col.decode(), xs)
+            r = {"keys": n,
+                 "reference_fit_us": round(ev(lambda: lc.encode(xs, lc.LINEAR, BS, lc.FIT_REFERENCE, payload=col.payload)), 1),
+                 "exact_fit_us": round(ev(lambda: lc.encode(xs, lc.LINEAR, BS, lc.FIT_EXACT, payload=col.payload)), 1)}
+            r["reference_fit_gbs"] = round(n * 8 / r["reference_fit_us"] / 1e3, 1)
+            res[f"blocks_{nblk}"] = r
+            del col
+    lc.check()
+    if rank == 0:
+        head = res[f"blocks_{nb_all}"]
+        line = {"metric": f"LeCo-fix u64 encode GB/s of input, {args.n // 1_000_000}M keys, reference fit",
+                "value": head["reference_fit_gbs"], "unit": "GB/s", "n_gpus": world, "steps": 10, "warmup": 3,
+                "ms_per_step": round(head["reference_fit_us"] / 1e3, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": f"prefixes of {args.n} u64 piecewise-linear keys, {BS}-value blocks, "
+                                       "LeCo-fix encode, reference and exact fit", "keys": args.n},
+                "clocks": clk.summary(), **res}
+        print(json.dumps(line), flush=True)
+
+
 def to_np_u64(t):
     return t.cpu().numpy().view(np.uint64)
 
@@ -807,6 +863,9 @@ def main():
         return
     if args.workload == "codecs":
         run_codecs(args, world, rank, local)
+        return
+    if args.workload == "encode":
+        run_encode(args, world, rank, local)
         return
 
     import torch
