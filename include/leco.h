@@ -366,7 +366,10 @@ int leco_server_destroy(leco_server *sv);
 
 /* ---- host-buffer entry points (synchronous; allocate device memory) ----
  * These are the reference-facing calls: host in, host out, the same
- * arguments as the reference's per-column driver loops. */
+ * arguments as the reference's per-column driver loops.  Their device memory
+ * comes from a memory pool of this library, one per device, which keeps up to
+ * 1 GiB mapped between calls (so repeated calls do not map their buffers
+ * afresh) until the process ends. */
 
 /* Encodes h_values[n]; writes payload bytes and offsets[nblocks+1] to host
  * buffers; *out_bytes = compressed size. */

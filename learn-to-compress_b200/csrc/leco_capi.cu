@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -404,6 +405,36 @@ int leco_validate_host(int codec, int dtype, const uint8_t *h_payload, uint64_t 
 
 // ---- host-buffer pipelines -------------------------------------------------------------
 
+// Device memory of the host-buffer calls (leco_*_host) comes from a memory pool of this
+// library, one per device, that keeps up to kHostPoolKeep bytes mapped between calls.
+// From the default pool (release threshold 0) every call mapped its buffers afresh once
+// the previous call's stream had synchronised.  If the pool cannot be made, the default
+// pool is used.
+constexpr uint64_t kHostPoolKeep = 1ull << 30;
+cudaMemPool_t host_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  static bool tried[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!tried[dev]) {
+    tried[dev] = true;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+      uint64_t keep = kHostPoolKeep;
+      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess) pools[dev] = pool;
+      else cudaMemPoolDestroy(pool);
+    }
+    cudaGetLastError();  // a failed attempt leaves no sticky error behind
+  }
+  return pools[dev];
+}
+
 struct DevBuf {
   void *p = nullptr;
   cudaStream_t st = nullptr;
@@ -412,7 +443,8 @@ struct DevBuf {
   }
   cudaError_t alloc(size_t bytes, cudaStream_t s) {
     st = s;
-    return cudaMallocAsync(&p, bytes ? bytes : 1, s);
+    cudaMemPool_t pool = host_pool();
+    return pool ? cudaMallocFromPoolAsync(&p, bytes ? bytes : 1, pool, s) : cudaMallocAsync(&p, bytes ? bytes : 1, s);
   }
 };
 
