@@ -92,11 +92,16 @@ class ClockSampler:
         self.idx, self.period = gpu_index, period_s
         self.sm, self.reasons, self.max_mhz = [], set(), None
         self._stop = threading.Event()
+        self._live = threading.Event()  # set once the first sample is taken
 
     def _run(self):
         import pynvml
 
-        pynvml.nvmlInit()
+        try:
+            pynvml.nvmlInit()
+        except Exception:
+            self._live.set()
+            return
         try:
             uuid = os.environ.get("CUDA_VISIBLE_DEVICES", "")
             h = pynvml.nvmlDeviceGetHandleByIndex(self.idx if not uuid or "," in uuid or not uuid.isdigit() else 0)
@@ -107,14 +112,18 @@ class ClockSampler:
                 for name, bit in self.REASONS.items():
                     if r & bit:
                         self.reasons.add(name)
+                self._live.set()
                 time.sleep(self.period)
         finally:
+            self._live.set()
             pynvml.nvmlShutdown()
 
     def __enter__(self):
+        # the timed region starts only once sampling runs (NVML's start-up can take
+        # longer than a short timed region)
         self.t = threading.Thread(target=self._run, daemon=True)
         self.t.start()
-        time.sleep(0.02)
+        self._live.wait(timeout=5.0)
         return self
 
     def __exit__(self, *a):

@@ -260,7 +260,8 @@ int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_s
                        uint32_t max_segment_len, int fit_mode,
                        uint8_t *d_payload, uint64_t payload_cap, uint64_t *d_offsets, void *d_workspace,
                        uint64_t workspace_bytes, leco_stream_t stream);
-/* decodeArray8 over all segments (:573-626); a raw segment yields its own values. */
+/* decodeArray8 over all segments (:573-626); a raw segment yields its own values.
+ * d_out: 8-byte aligned. */
 int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
                        uint64_t n, uint64_t *d_out, leco_stream_t stream);
 /* randomdecodeArray8 for each index (:636-698): binary search of the device start array. */
@@ -308,7 +309,8 @@ uint64_t leco_batch_total_blocks(const leco_batch *b);
  * (column, block) items from an atomic work queue (plus the sequential-fit pass
  * for reference-fit columns that need it). */
 int leco_batch_encode(leco_batch *b, leco_stream_t stream);
-/* Decodes every column into its d_out with one persistent launch. */
+/* Decodes every column into its d_out (aligned to the column's value size) with one
+ * persistent launch. */
 int leco_batch_decode(leco_batch *b, leco_stream_t stream);
 /* Captures the pass(es) (1 encode, 2 decode, 3 both) into a CUDA graph on the
  * first call and replays the graph on every call. */

@@ -312,8 +312,11 @@ int leco_batch_encode(leco_batch *b, leco_stream_t stream) {
 
 int leco_batch_decode(leco_batch *b, leco_stream_t stream) {
   if (!b) return berr(LECO_ERR_ARG, "leco_batch_decode: null batch");
-  for (const auto &c : b->cols)
+  for (const auto &c : b->cols) {
     if (!c.d_out) return berr(LECO_ERR_ARG, "leco_batch_decode: a column has no output buffer");
+    if (reinterpret_cast<uintptr_t>(c.d_out) & (uint64_t)(c.dtype - 1))  // values are stored as 16/32-byte vectors
+      return berr(LECO_ERR_ARG, "leco_batch_decode: a column's output buffer is not aligned to its value size");
+  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const BatchArgs B = args_of(b, b->err);
   cudaError_t e = cudaMemsetAsync(b->d_ws + b->status_bytes, 0, 256, st);  // ticket

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) decode_staged_kernel(DecodeLaunch a, uint
         h.body_bit = (uint64_t)(m.hoff + (raw ? 1u : Hdr<CODEC, S>::bytes)) * 8;
         const uint32_t *w32 = reinterpret_cast<const uint32_t *>(sb);
         const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + base);
-        const int32_t kstart = -(int32_t)((oaddr & 15) / S);
+        const int32_t kstart = -(int32_t)((oaddr & 31) / S);  // groups start on 32 bytes
         const bool fast = (CODEC == kFor) || raw || pred_in_range<CODEC>(h, len);
         if (!raw) mark_nonneg<CODEC>(h, len);
         if (fast) acc += decode_narrow<T, CODEC, true, true, 256, SUM>(h, raw, w32, out, base, 0, len, kstart);

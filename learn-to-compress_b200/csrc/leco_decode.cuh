@@ -102,6 +102,31 @@ __device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *
              make_uint4((uint32_t)v[4 * c], (uint32_t)v[4 * c + 1], (uint32_t)v[4 * c + 2], (uint32_t)v[4 * c + 3]));
   }
 }
+// The same for a group whose start is 32-byte aligned when CNT values make whole
+// 32-byte pieces (the narrow decoders start every thread's group on a 32-byte boundary
+// of the output): each piece goes out as one 256-bit store.  Other sizes as store_vals.
+template <typename T, int CNT>
+__device__ __forceinline__ void store_vals32(T *out, uint64_t o0, const uint64_t *v) {
+  if constexpr (sizeof(T) * CNT % 32 == 0) {
+#pragma unroll
+    for (int c = 0; c < (int)(sizeof(T) * CNT / 32); ++c) {
+      T *p = out + o0 + c * (32 / sizeof(T));
+      if constexpr (sizeof(T) == 8) {
+        asm volatile("st.global.cs.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(v[4 * c]), "l"(v[4 * c + 1]),
+                     "l"(v[4 * c + 2]), "l"(v[4 * c + 3])
+                     : "memory");
+      } else {
+        asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"((uint32_t)v[8 * c]),
+                     "r"((uint32_t)v[8 * c + 1]), "r"((uint32_t)v[8 * c + 2]), "r"((uint32_t)v[8 * c + 3]),
+                     "r"((uint32_t)v[8 * c + 4]), "r"((uint32_t)v[8 * c + 5]), "r"((uint32_t)v[8 * c + 6]),
+                     "r"((uint32_t)v[8 * c + 7])
+                     : "memory");
+      }
+    }
+  } else {
+    store_vals<T, CNT>(out, o0, v);
+  }
+}
 
 // Scratch of the Delta scan: two halves of 8 warp totals for each of up to four
 // groups of a CTA.  One non-template function, so every kernel holds a single copy
@@ -266,11 +291,15 @@ __device__ __forceinline__ bool pred_in_range(const BlockHdr &h, uint32_t len) {
 
 // Decodes values [lo, hi) of one block whose fields are at most 32 bits wide
 // (raw u32 blocks included).  Each thread produces VEC consecutive values per
-// step and writes them with U 16-byte stores (U: the unroll depth).
+// step (U 16-byte chunks, U: the unroll depth; kstart puts every thread's group on
+// a 32-byte boundary of the output) and writes them with 256-bit stores.
 // SUM: instead of storing, returns this thread's sum of the values (as T).
 // The block's case is chosen once, outside the value loop: raw, FOR, a linear block
 // whose predictions all lie in [0, 2^51) (both conversions exact on the FP64 pipe),
-// or the general prediction (FAST: plain truncation, else the x86 rule).
+// or the general prediction (FAST: plain truncation, else the x86 rule).  (With the
+// case tested per value and 16-byte stores the storing u64 decoder was 2 % faster
+// than this loop with 16-byte stores -- which stalled on the memory-instruction
+// queue -- and 1.5 % slower than this loop with 256-bit stores.)
 enum : int { kNarrowRaw = 0, kNarrowFor = 1, kNarrowNonneg = 2, kNarrowPred = 3 };
 template <typename T, int CODEC, int MODE, bool FAST, bool SMEM, int G, bool SUM, int U>
 __device__ __forceinline__ uint64_t decode_narrow_mode(const BlockHdr &h, const uint32_t *__restrict__ words32, T *out,
@@ -324,7 +353,7 @@ __device__ __forceinline__ uint64_t decode_narrow_mode(const BlockHdr &h, const 
     }
     const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
     if (full) {
-      store_vals<T, VEC>(out, obase + kv, v);
+      store_vals32<T, VEC>(out, obase + kv, v);
     } else {
 #pragma unroll
       for (int j = 0; j < VEC; ++j)
@@ -333,74 +362,9 @@ __device__ __forceinline__ uint64_t decode_narrow_mode(const BlockHdr &h, const 
   }
   return acc;
 }
-// The same loop with the block's case tested per value (uniform branches).  The u64
-// decoders that store their values keep it: with the case hoisted they issue ~28 %
-// fewer instructions, but their shared-memory loads and 16-byte stores then come in
-// bursts that stall on the memory-instruction queue, and a 200M-key decode took
-// 0.375 ms instead of 0.353 ms.  The sums and the u32 decoders gain from the hoisting.
-template <typename T, int CODEC, bool FAST, bool SMEM, int G, bool SUM, int U>
-__device__ __forceinline__ uint64_t decode_narrow_per_value(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32,
-                                                  T *out, uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
-  uint64_t acc = 0;
-  constexpr int S = sizeof(T);
-  constexpr int VEC = U * 16 / S;  // U 16-byte stores per step
-  const uint32_t l = raw ? 32u : h.l;
-  // words32 + body_bit/32: the body's first word (global payload or a staged copy in shared memory)
-  const uint32_t *bp = words32 + (h.body_bit >> 5);
-  const uint32_t bsh = (uint32_t)(h.body_bit & 31);
-  const uint32_t mask = l >= 32 ? 0xffffffffu : ((1u << l) - 1u);
-  const uint32_t sb = l ? l - 1 : 0, m1 = mask >> 1;
-  for (int32_t kv = kstart + (int32_t)group_rank<G>() * VEC; kv < (int32_t)hi; kv += (int32_t)group_size<G>() * VEC) {
-    uint64_t v[VEC];
-#pragma unroll
-    for (int j = 0; j < VEC; ++j) {
-      const int32_t k = kv + j;
-      const uint32_t kk = k < (int32_t)lo ? lo : (uint32_t)k;  // values before lo are not stored
-      const uint32_t r = bsh + kk * l;
-      const uint32_t *p = bp + (r >> 5);
-      const uint32_t w0 = SMEM ? p[0] : __ldg(p), w1 = SMEM ? p[1] : __ldg(p + 1);
-      const uint32_t f = l ? (__funnelshift_r(w0, w1, r) & mask) : 0u;
-      if (raw) {
-        v[j] = f;
-      } else if (CODEC == kFor) {
-        v[j] = h.base + f;
-      } else {
-        int64_t pred;
-        if (FAST && (CODEC == kLinear || CODEC == kLegacy) && h.nonneg) {
-          pred = trunc_nonneg_fp64(pred_linear_fp64(h.a0, h.a1, kk));  // no conversion-unit work
-        } else {
-          const double pd = (CODEC == kLinear || CODEC == kLegacy) ? pred_linear(h.a0, h.a1, kk)
-                                                                   : pred_poly2(h.a0, h.a1, h.a2, __uint2double_rn(kk));
-          pred = FAST ? __double2ll_rz(pd) : f2i_x86(pd);
-        }
-        const uint32_t mag = f & m1;
-        const int64_t d = ((f >> sb) & 1u) ? (int64_t)mag : -(int64_t)mag;
-        v[j] = (uint64_t)(pred + d);
-      }
-    }
-    if (SUM) {
-#pragma unroll
-      for (int j = 0; j < VEC; ++j)
-        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) acc += (uint64_t)(T)v[j];
-      continue;
-    }
-    const bool full = kv >= (int32_t)lo && kv + VEC <= (int32_t)hi;
-    if (full) {
-      store_vals<T, VEC>(out, obase + kv, v);
-    } else {
-#pragma unroll
-      for (int j = 0; j < VEC; ++j)
-        if (kv + j >= (int32_t)lo && kv + j < (int32_t)hi) out[obase + kv + j] = (T)v[j];
-    }
-  }
-  return acc;
-}
-
 template <typename T, int CODEC, bool FAST, bool SMEM = false, int G = 256, bool SUM = false, int U = 2>
 __device__ __forceinline__ uint64_t decode_narrow(const BlockHdr &h, bool raw, const uint32_t *__restrict__ words32,
                                                   T *out, uint64_t obase, uint32_t lo, uint32_t hi, int32_t kstart) {
-  if constexpr (sizeof(T) == 8 && !SUM)
-    return decode_narrow_per_value<T, CODEC, FAST, SMEM, G, SUM, U>(h, raw, words32, out, obase, lo, hi, kstart);
   if (raw) return decode_narrow_mode<T, CODEC, kNarrowRaw, FAST, SMEM, G, SUM, U>(h, words32, out, obase, lo, hi, kstart);
   if constexpr (CODEC == kFor) {
     return decode_narrow_mode<T, CODEC, kNarrowFor, FAST, SMEM, G, SUM, U>(h, words32, out, obase, lo, hi, kstart);
@@ -459,7 +423,7 @@ __device__ __forceinline__ void decode_block(const DecodeLaunch &a, uint64_t b) 
   // First vector start so that out[obase + kv] is 16-byte aligned (out must be
   // sizeof(T)-aligned); kv may start up to VEC-1 values before lo.
   const uintptr_t oaddr = reinterpret_cast<uintptr_t>(out + obase + lo);
-  const int32_t kstart = (int32_t)lo - (int32_t)((oaddr & 15) / S);
+  const int32_t kstart = (int32_t)lo - (int32_t)((oaddr & 31) / S);  // groups start on 32 bytes
   const uint32_t l = raw ? TB : h.l;
   if (l <= 32) {
     // Narrow fields (every u32 block, u64 blocks with l <= 32): 32-bit field

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(256) varlen_decode_kernel(const uint8_t *paylo
             h.body_bit = (uint64_t)(hoff + 17) * 8;
             if (fabs(h.a0) + fabs(h.a1) * __uint2double_rn(len) < 4611686018427387904.0) {
               mark_nonneg<kLinear>(h, len);
-              const int32_t kstart = -(int32_t)((reinterpret_cast<uintptr_t>(out + st) & 15) / 8);
+              const int32_t kstart = -(int32_t)((reinterpret_cast<uintptr_t>(out + st) & 31) / 8);
               acc += decode_narrow<uint64_t, kLinear, true, true, 32, SUM>(h, false, reinterpret_cast<const uint32_t *>(sb),
                                                                            out, st, 0, len, kstart);
               staged = true;
@@ -556,6 +556,8 @@ int leco_varlen_encode(const uint64_t *d_values, uint64_t n, const uint64_t *d_s
 int leco_varlen_decode(const uint8_t *d_payload, const uint64_t *d_offsets, const uint64_t *d_starts, uint64_t nseg,
                        uint64_t n, uint64_t *d_out, leco_stream_t stream) {
   if (!d_payload || !d_offsets || !d_starts || !d_out || !nseg) return verr(LECO_ERR_ARG, "leco_varlen_decode: null pointer");
+  if (reinterpret_cast<uintptr_t>(d_out) & 7)  // values are stored as 32-byte vectors
+    return verr(LECO_ERR_ARG, "leco_varlen_decode: d_out must be 8-byte aligned");
   uint32_t *err = nullptr;
   int rc = leco::device_error_word(&err);
   if (rc) return rc;
