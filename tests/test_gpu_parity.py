@@ -189,12 +189,16 @@ def test_corrupt_header_sets_error_word(lc, orc, dev):
 
 
 @pytest.mark.parametrize("s,codec,bs,shift", [(8, 0, 4096, 0), (8, 3, 4096, 0), (4, 0, 4096, 0), (4, 5, 4096, 0),
-                                              (8, 0, 4096, 1), (8, 0, 4099, 0), (4, 0, 2050, 0)])
+                                              (8, 0, 4096, 1), (8, 0, 4099, 0), (4, 0, 2050, 0), (8, 3, 4096, 1),
+                                              (4, 3, 2050, 0)])
 def test_reference_fit_large_columns(lc, orc, dev, s, codec, bs, shift):
     """Columns of >= 4096 blocks under the reference fit (the sequential-fit
     kernel, then the encoder), with values 8 bytes off 16-byte alignment and block
-    sizes whose rows are not a multiple of 16 bytes among them.  Every image equals
-    the oracle's; large values make the reference's sequential FP64 sums round."""
+    sizes whose rows are not a multiple of 16 bytes among them: aligned columns take
+    the cp.async ring fit, the others the register-tiled fit (which also serves
+    columns of more than one wave of the ring kernel), for linear and degree-2 fits.
+    Every image equals the oracle's; large values make the reference's sequential
+    FP64 sums round."""
     import torch
     rng = np.random.default_rng(7 * s + codec + bs + shift)
     dt = np.uint64 if s == 8 else np.uint32
