@@ -254,8 +254,9 @@ __device__ __forceinline__ void delta_tiles(const uint64_t *__restrict__ words, 
   if (SMEM || h.l <= 32) delta_tiles_w<T, G, false, SMEM>(words, h, len, lo, hi, emit);
   else delta_tiles_w<T, G, true, false>(words, h, len, lo, hi, emit);
 }
-// Emitter of delta_tiles that stores the values of [lo, hi) to out[obase + k]:
-// 16-byte stores for a span wholly inside and aligned, else one value at a time.
+// Emitter of delta_tiles that stores the values of [lo, hi) to out[obase + k]: for
+// a span wholly inside, 256-bit stores when it starts on 32 bytes, 16-byte stores
+// when on 16, else one value at a time.
 template <typename T>
 struct DeltaStore {
   T *out;
@@ -264,11 +265,13 @@ struct DeltaStore {
   template <typename A>
   __device__ __forceinline__ void operator()(uint32_t k0, const A *v) const {
     T *o = out + obase + k0;
-    if (k0 >= lo && k0 + kDeltaSpan <= hi && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+    const uintptr_t oa = reinterpret_cast<uintptr_t>(o);
+    if (k0 >= lo && k0 + kDeltaSpan <= hi && (oa & 15) == 0) {
       uint64_t w[kDeltaSpan];
 #pragma unroll
       for (int j = 0; j < kDeltaSpan; ++j) w[j] = (uint64_t)v[j];
-      store_vals<T, kDeltaSpan>(out, obase + k0, w);
+      if ((oa & 31) == 0) store_vals32<T, kDeltaSpan>(out, obase + k0, w);
+      else store_vals<T, kDeltaSpan>(out, obase + k0, w);
     } else {
 #pragma unroll
       for (int j = 0; j < kDeltaSpan; ++j)
