@@ -24,6 +24,7 @@ __device__ __forceinline__ void batch_encode_one(const BatchArgs &B, const DevCo
   a.status = B.status + p0;
   a.ticket = nullptr;
   a.error = B.error;
+  a.rows_area = 0;  // the batch's per-group slices hold the values only
   encode_block<T, CODEC, G, U>(a, b, smem);
 }
 // The unroll depth changes only the u64 LeCo encoder; other codecs take one instance.

@@ -243,6 +243,9 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
   a.values = L.values; a.n = L.n; a.bs = L.bs; a.nb = L.nb;
   a.payload = L.payload; a.payload_cap = L.payload_cap; a.offsets = L.offsets; a.dir = L.dir;
   a.seq_models = nullptr; a.status = L.status; a.ticket = L.ticket; a.error = L.error;
+  // u32 LeCo / degree-2 blocks of 513..4096 values pack their residual rows in an area of
+  // shared memory after the values (six CTAs per SM are set by registers there anyway)
+  a.rows_area = sizeof(T) == 4 && (CODEC == kLinear || CODEC == kPoly2) && L.bs > kWarpBlock && L.bs <= 4096;
   PolyX px;
   for (int i = 0; i < 10; ++i) a.polyX[i] = px.x[i] = L.polyX[i];
   if (L.seq_models && (CODEC == kLinear || CODEC == kPoly2 || CODEC == kLegacy)) {
@@ -265,7 +268,7 @@ static int launch_encode_t(const EncodeLaunch &L, cudaStream_t st) {
     }
     a.seq_models = L.seq_models;
   }
-  const uint32_t smem = enc_smem_bytes(L.bs, sizeof(T));
+  const uint32_t smem = enc_smem_bytes(L.bs, sizeof(T)) + (a.rows_area ? enc_rows_bytes(L.bs) : 0u);
   if (L.bs <= kWarpBlock) {
     const uint32_t slice = (smem + 15) / 16 * 16;
     encode_kernel_warp<T, CODEC><<<(unsigned)((L.nb + 7) / 8), 256, 8 * slice, st>>>(a, slice);

@@ -32,6 +32,8 @@ struct EncodeArgs {
   uint64_t *status;          // [nb] look-back words, zeroed
   uint32_t *ticket;          // zeroed
   uint32_t *error;           // error word
+  uint32_t rows_area;        // 1: the group's shared memory holds enc_rows_bytes(bs) more bytes after the
+                             // values, where u32 LeCo / degree-2 residual rows are packed
 };
 
 // Shared-memory layout helper.
@@ -60,6 +62,9 @@ __device__ __forceinline__ EncSmem<T> enc_smem(uint8_t *base, uint32_t bs) {
 __host__ __device__ inline uint32_t enc_smem_bytes(uint32_t bs, uint32_t s) {
   return 1152 + ((bs / 32 + 9) * 4 + 15) / 16 * 16 + (bs + 31) / 32 * 32 * s + 16;
 }
+// The packed-rows area of the u32 LeCo / degree-2 encoder: a packed body of at most
+// round32(bs) words plus the four zero words after it.
+__host__ __device__ inline uint32_t enc_rows_bytes(uint32_t bs) { return (bs + 31) / 32 * 32 * 4 + 16; }
 
 // Decoupled look-back (single-pass prefix sum over per-block totals), run by one
 // full warp.  lookback_excl walks back over the predecessors of block b 32 at a
@@ -922,6 +927,13 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   const uint64_t base = b * a.bs;
   const uint32_t len = (uint32_t)umin64((uint64_t)a.bs, a.n - base);
   const T *src = reinterpret_cast<const T *>(a.values) + base;
+  // u32 LeCo / degree-2 blocks with a packed-rows area: residuals are kept row-swizzled
+  // (residual i of a row of 32 at column i ^ row) and packed by rows of 32 fields with
+  // pack_rows, the image then written from the packed words (write_image_packed)
+  // instead of gathering each 16-byte chunk field by field.
+  constexpr bool kRowsCodec = S == 4 && (CODEC == kLinear || CODEC == kPoly2) && G != 32;
+  const bool rows = kRowsCodec && a.rows_area;
+  uint32_t *pk = reinterpret_cast<uint32_t *>(sm.vals) + (a.bs + 31) / 32 * 32;
 
   // ---- stage the block ------------------------------------------------------
   constexpr uint32_t V = 16 / S;
@@ -1032,9 +1044,9 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
           for (uint32_t i0 = 0; i0 < len; i0 += nt) {
             const uint32_t i = i0 + tid;
             bool pos = false;
+            uint64_t r = 0;
             if (i < len) {
               const uint64_t y = (uint64_t)sm.vals[i];
-              uint64_t r;
               if (CODEC == kLinear) {
                 const int64_t pred = lin_pred<decltype(rule)::value>(m0, m1, i);
                 pos = S == 8 ? (y > (uint64_t)pred) : ((int64_t)y > pred);
@@ -1046,10 +1058,12 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
                 r = pos ? y - (uint64_t)pred : (uint64_t)pred - y;
               }
               r &= (S == 8 ? ~0ull : 0xffffffffull);
-              sm.vals[i] = (T)r;
               rmax = r > rmax ? r : rmax;
             }
+            // every lane of the warp (one row of 32) has read its value before any lane
+            // writes its residual: the swizzled write lands in another lane's slot
             const uint32_t ballot = __ballot_sync(0xffffffffu, pos);
+            if (i < len) sm.vals[kRowsCodec && rows ? swz32(i) : i] = (T)r;
             if ((tid & 31) == 0) sm.signs[i0 / 32 + tid / 32] = ballot;
           }
         };
@@ -1100,6 +1114,8 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
     for (uint32_t i = tid; i < len; i += nt) sm.vals[i] = __ldg(src + i);
   }
   const uint64_t size = block_bytes<CODEC, S>(l, len);
+  // residuals and signs are complete (the width reduction ended with a barrier)
+  if (rows && !raw && l > 0) pack_rows(reinterpret_cast<const uint32_t *>(sm.vals), sm.signs, pk, len, l, tid, nt);
 
   // ---- offset by look-back ----------------------------------------------------
   if (tid < 32) {
@@ -1148,6 +1164,8 @@ __device__ __forceinline__ void encode_block(const EncodeArgs &a, uint64_t b, ui
   const uint32_t *signs = sm.signs;
   if (raw) {
     write_image(a.payload, goff, size, H, sm.hdr, TB, len, [&](uint32_t k) -> uint64_t { return (uint64_t)vals[k]; }, tid, nt);
+  } else if (rows && l > 0) {
+    write_image_packed(a.payload, goff, size, H, sm.hdr, pk, tid, nt);
   } else if (CODEC == kLegacy) {  // write_delta_T (bit_write.h:186-245): |r| below the sign bit
     const uint32_t sb = l ? l - 1 : 0;
     const uint32_t mm = (1u << sb) - 1u;
