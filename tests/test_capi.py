@@ -87,6 +87,11 @@ def test_argument_errors_need_no_gpu(lc):
     assert L.leco_decode(0, 8, None, dummy, 10, 16, dummy, None) == -1
     assert L.leco_decode(0, 8, P(17), dummy, 10, 16, dummy, None) == -1  # misaligned payload
     assert b"block_size" in L.leco_last_error() or b"aligned" in L.leco_last_error()
+    # outputs not aligned to the value size (the decoders store 16/32-byte vectors)
+    assert L.leco_decode(0, 8, dummy, dummy, 10, 16, P(20), None) == -1
+    assert b"misaligned" in L.leco_last_error()
+    assert L.leco_varlen_decode(dummy, dummy, dummy, 1, 10, P(20), None) == -1
+    assert b"aligned" in L.leco_last_error()
     assert L.leco_num_blocks(10, 4) == 3 and L.leco_num_blocks(0, 4) == 0
 
 
