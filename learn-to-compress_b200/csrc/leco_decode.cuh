@@ -104,7 +104,9 @@ __device__ __forceinline__ void store_vals(T *out, uint64_t o0, const uint64_t *
 }
 // The same for a group whose start is 32-byte aligned when CNT values make whole
 // 32-byte pieces (the narrow decoders start every thread's group on a 32-byte boundary
-// of the output): each piece goes out as one 256-bit store.  Other sizes as store_vals.
+// of the output): each piece goes out as one 256-bit store (sm_100).  Other sizes as
+// store_vals.  `out` is a generic pointer to global memory, which st.global takes as is:
+// a generic address of global memory is its global address.
 template <typename T, int CNT>
 __device__ __forceinline__ void store_vals32(T *out, uint64_t o0, const uint64_t *v) {
   if constexpr (sizeof(T) * CNT % 32 == 0) {
